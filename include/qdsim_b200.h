@@ -1,0 +1,193 @@
+/*
+ * qdsim_b200 -- C ABI of the B200 (sm_100a) finite-element quantum-dot hot path.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: QD_OK (0) or a negative QD_ERR_*.
+ *  - Pointers named d_* are device pointers (any allocator; the caller owns
+ *    them), h_* are host pointers.  The library never allocates device
+ *    memory: scratch comes from a caller-provided workspace whose size is
+ *    returned by the matching *_workspace_size query.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *  - Units are whatever the caller uses consistently; the Python layer passes
+ *    nm and eV (kinetic coefficient c = hbar^2/(2 m*) in eV nm^2).
+ *  - Matrices are CSR with int32 row pointers / column indices and FP64 values.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the QDSim source tree).
+ */
+#ifndef QDSIM_B200_H
+#define QDSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  QD_OK = 0,
+  QD_ERR_INVALID = -1,        /* bad argument (sizes, null pointers, order)      */
+  QD_ERR_CUDA = -2,           /* a CUDA runtime call failed                       */
+  QD_ERR_NOT_CONVERGED = -3,  /* iteration cap reached; residuals are returned   */
+  QD_ERR_BREAKDOWN = -4,      /* Gram matrix not positive definite / NaN input   */
+  QD_ERR_WORKSPACE = -5,      /* workspace too small or misaligned               */
+  QD_ERR_DEGENERATE = -6,     /* zero-area element or non-finite coefficient     */
+  QD_ERR_LIMIT = -7           /* a size exceeds a compiled-in limit              */
+};
+
+/* assembly modes */
+enum {
+  QD_ASM_FEM = 0,             /* fem.cpp weak form, nodal V/W interpolated        */
+  QD_ASM_REF_CYTHON = 1,      /* schrodinger_solver.pyx:201-251 element formulas  */
+  QD_ASM_REF_FIXED = 2        /* fixed_open_system_solver.pyx:197-271 formulas    */
+};
+
+/* eigensolver precision modes */
+enum {
+  QD_PREC_FP64 = 0,           /* FP64 vectors throughout (the plain form)         */
+  QD_PREC_MIXED = 1           /* FP32 vector phase, then FP64 finishing phase     */
+};
+
+const char *qd_version(void);
+const char *qd_status_string(int status);
+/* Number of kernels this library launched since load (all entry points). */
+uint64_t qd_kernel_launch_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Sparsity pattern (host, C++).  Replaces the triplet build + setFromTriplets
+ * of FEMSolver::assemble_matrices_serial (backend/src/fem.cpp:116-151) and the
+ * triplet lists of CythonSchrodingerSolver._assemble_matrices
+ * (qdsim_cython/solvers/schrodinger_solver.pyx:131-190).
+ *
+ * Rows/cols are reduced DOFs: h_dof_map[node] in [0, n_dofs) or -1 for an
+ * eliminated (Dirichlet) node.  Call once with all output pointers NULL to get
+ * the sizes, then again with buffers of those sizes.
+ *   rowptr  int32[n_dofs+1]      col     int32[nnz]   (sorted per row)
+ *   adjptr  int32[n_dofs+1]      adj     int32[n_adj]   (elem << 4 | local)
+ *   cptr    int32[n_dofs+1]      contrib uint8[n_contrib] (t*k+b, slot order)
+ *   slotcnt uint8[nnz]  (contributions per slot)
+ * ------------------------------------------------------------------------- */
+int qd_pattern_build(int64_t num_nodes, int64_t num_elems, int k,
+                     const int32_t *h_elems, const int32_t *h_dof_map, int32_t n_dofs,
+                     int64_t *nnz, int64_t *n_adj, int64_t *n_contrib,
+                     int32_t *h_rowptr, int32_t *h_col,
+                     int32_t *h_adjptr, int32_t *h_adj,
+                     int32_t *h_cptr, uint8_t *h_contrib, uint8_t *h_slotcnt);
+
+/* Node -> incident (element, local index) lists over ALL nodes (used by the
+ * adjoint's nodal gather).  Same two-call protocol. */
+int qd_node_adjacency(int64_t num_nodes, int64_t num_elems, int k, const int32_t *h_elems,
+                      int64_t *n_adj, int32_t *h_adjptr, int32_t *h_adj);
+
+/* ---------------------------------------------------------------------------
+ * Element-parallel assembly into the precomputed CSR pattern (GPU).
+ * Replaces FEMSolver::assemble_element_matrix (backend/src/fem.cpp:736-990),
+ * the GPU element kernels (backend/src/gpu_kernels.cu:46-336, 442-745) and the
+ * host triplet scatter of GPUAccelerator::assemble_matrices
+ * (backend/src/gpu_accelerator.cpp:439-642).
+ *
+ * One warp per CSR row; each row's slots are summed in a fixed order over the
+ * row's contribution list (deterministic, no atomics).
+ *   order        1, 2 or 3 (k = 3, 6, 10 nodes per element)
+ *   d_nodes      double[num_nodes*2] (x, y)
+ *   d_elems      int32[num_elems*k]
+ *   d_c          double[num_elems]   kinetic coefficient per element
+ *   d_V          FEM mode: double[num_nodes] nodal V; REF modes: double[num_elems]
+ *   d_W          FEM mode: double[num_nodes] nodal CAP amplitude or NULL
+ *   outputs      d_H[nnz] (real part K + V), d_M[nnz], d_Himag[nnz] (= -W term,
+ *                may be NULL)
+ * The call is asynchronous.  `d_status` (int32[1], device, zeroed by the
+ * caller) receives bit 1 for a zero-area element or non-finite c and bit 2
+ * for a non-finite V; callers read it after synchronising and map a nonzero
+ * value to QD_ERR_DEGENERATE.  Limits: at most 16 incident elements and 128
+ * slots per row (QD_ERR_LIMIT from qd_pattern_build otherwise).
+ * ------------------------------------------------------------------------- */
+int qd_assemble(int order, int mode, int64_t num_nodes, int64_t num_elems, int32_t n_dofs,
+                const double *d_nodes, const int32_t *d_elems,
+                const double *d_c, const double *d_V, const double *d_W,
+                const int32_t *d_rowptr, const int32_t *d_adjptr, const int32_t *d_adj,
+                const int32_t *d_cptr, const uint8_t *d_contrib, const uint8_t *d_slotcnt,
+                double *d_H, double *d_M, double *d_Himag, int32_t *d_status, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Fused dual SpMM over the shared H/M pattern: HX = H X, MX = M X for a block
+ * of b vectors stored row-major (X[row*b + j]).  FP64 accumulation; vec_fp32
+ * selects float (1) or double (0) vector storage.  Supersedes fusedSpMV
+ * (backend/src/fused_gpu_kernels.cu:97-125).  Either output may be NULL.
+ * ------------------------------------------------------------------------- */
+int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32,
+                 const int32_t *d_rowptr, const int32_t *d_col,
+                 const double *d_H, const double *d_M,
+                 const void *d_X, void *d_HX, void *d_MX, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched LOBPCG for the k lowest eigenpairs of H x = E M x on a
+ * block-diagonal batch of n_dots independent problems (rows of dot d are
+ * [h_row_off[d], h_row_off[d+1]) with global column indices).  Replaces the
+ * eigsh(H, k, M, which='SM') call of CythonSchrodingerSolver.solve
+ * (qdsim_cython/solvers/schrodinger_solver.pyx:447-453) and the dense
+ * EigenSolver::solve (backend/src/solver.cpp:59-200).
+ *   b            block size (k <= b <= 32; b - k guard vectors)
+ *   prec_mode    QD_PREC_FP64 or QD_PREC_MIXED
+ *   tol          converged when ||H x - t M x|| <= tol |t| ||M x|| for all k
+ *   d_X_out      double[n_rows_total * k] row-major per row (X[row*k + j]),
+ *                M-orthonormal per dot
+ *   d_E_out      double[n_dots * k]; d_res_out double[n_dots * k] relative
+ *                residuals; d_iters_out int32[n_dots] (FP32 + FP64 iterations)
+ *   h_info       int32[4] (host): total iterations, FP32 iterations, FP64
+ *                iterations, number of converged dots
+ * The initial block is drawn from `seed` (deterministic).  Returns
+ * QD_ERR_NOT_CONVERGED if any dot hits max_iter (results still written).
+ * ------------------------------------------------------------------------- */
+int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b, int prec_mode,
+                             size_t *bytes);
+int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
+                    const int32_t *d_rowptr, const int32_t *d_col,
+                    const double *d_H, const double *d_M,
+                    int k, int b, int prec_mode, double tol, int max_iter, uint64_t seed,
+                    double *d_X_out, double *d_E_out, double *d_res_out, int32_t *d_iters_out,
+                    int32_t *h_info, void *d_work, size_t work_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Jacobi-preconditioned CG, FP64, for nrhs right-hand sides sharing one SPD
+ * matrix (row-major X[row*nrhs + j]).  Rows with d_fixed[row] != 0 are
+ * Dirichlet rows: X keeps its input value there and the row/column are
+ * eliminated (equivalent to the row replacement of
+ * qdsim_cython/solvers/poisson_solver.pyx:276-308, which the reference then
+ * hands to spsolve at :240).  Replaces PoissonSolver::solve's SimplicialLDLT
+ * (backend/src/poisson.cpp:320-334) and fusedPoissonSolver
+ * (backend/src/fused_gpu_kernels.cu:159-206).
+ *   tol          relative residual ||b - A x|| / ||b|| per column
+ *   h_iters/h_relres  host outputs: iterations used, final max relative residual
+ * ------------------------------------------------------------------------- */
+int qd_pcg_workspace_size(int32_t n, int nrhs, size_t *bytes);
+int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_col,
+                 const double *d_A, const double *d_B, double *d_X, const int32_t *d_fixed,
+                 double tol, int max_iter, int32_t *h_iters, double *h_relres,
+                 void *d_work, size_t work_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Adjoint (Hellmann-Feynman) gradients of L = sum_s w_s E_s with respect to
+ * nodal V and the per-element kinetic coefficient c.  With M-normalised
+ * eigenvectors, dE_s/dV_l = psi_s^T (dH/dV_l) psi_s and
+ * dE_s/dc_e = psi_s^T K_e psi_s / c_e (M depends on neither).  No reference
+ * counterpart: the reference has no derivatives; the checker is central finite
+ * differences of the FP64 eigenvalues.
+ *   d_psi        double[n_dofs * n_states] row-major (psi[dof*n_states + s])
+ *   d_w          double[n_states] weights
+ *   d_nadjptr/d_nadj  node adjacency from qd_node_adjacency
+ *   d_dofmap     int32[num_nodes]
+ *   outputs      d_dLdV[num_nodes], d_dLdc[num_elems]
+ * ------------------------------------------------------------------------- */
+int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states,
+               const double *d_nodes, const int32_t *d_elems, const int32_t *d_dofmap,
+               const double *d_c, const double *d_psi, const double *d_w,
+               const int32_t *d_nadjptr, const int32_t *d_nadj,
+               double *d_dLdV, double *d_dLdc, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QDSIM_B200_H */
