@@ -121,6 +121,22 @@ int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32,
                  const double *d_H, const double *d_M,
                  const void *d_X, void *d_HX, void *d_MX, void *stream);
 
+/* Fast-sine-transform preconditioner of one dot (see qd_lobpcg_solve).  The
+ * dot's reduced DOFs must be the interior points of an nx x ny lattice in
+ * row-major order (structured rectangle, homogeneous Dirichlet boundary).
+ * T = (cx Kx + cy Ky + shift I)^-1 with Kx, Ky the 1-D second differences,
+ * applied as DST-I transforms; nx = 0 disables preconditioning for the dot.
+ * d_prec_mats holds the orthonormal DST-I matrices
+ * S[i][j] = sqrt(2/(N+1)) sin(pi (i+1)(j+1)/(N+1)) (double, row-major) at
+ * sx_off (N = nx) and sy_off (N = ny).  The transforms run in the precision
+ * of the vectors they act on. */
+typedef struct {
+  int32_t nx, ny;
+  int64_t sx_off, sy_off;
+  float cx, cy, shift;
+  int32_t pad;
+} qd_dst_prec;
+
 /* ---------------------------------------------------------------------------
  * Batched LOBPCG for the k lowest eigenpairs of H x = E M x on a
  * block-diagonal batch of n_dots independent problems (rows of dot d are
@@ -130,24 +146,44 @@ int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32,
  * EigenSolver::solve (backend/src/solver.cpp:59-200).
  *   b            block size (k <= b <= 32; b - k guard vectors)
  *   prec_mode    QD_PREC_FP64 or QD_PREC_MIXED
- *   tol          converged when ||H x - t M x|| <= tol |t| ||M x|| for all k
+ *   tol          target relative eigenvalue error: converged when, for all k
+ *                pairs, 20 (||r||/||Mx||)^2 / ((t_{b-1} - t) |t|) <= tol with
+ *                r = H x - t M x (quadratic residual estimate, gap to the block
+ *                edge) and ||r|| <= 1e-2 |t| ||Mx||
  *   d_X_out      double[n_rows_total * k] row-major per row (X[row*k + j]),
  *                M-orthonormal per dot
  *   d_E_out      double[n_dots * k]; d_res_out double[n_dots * k] relative
- *                residuals; d_iters_out int32[n_dots] (FP32 + FP64 iterations)
+ *                residuals ||r|| / (|t| ||Mx||); d_iters_out int32[n_dots] (FP32 + FP64 iterations)
  *   h_info       int32[4] (host): total iterations, FP32 iterations, FP64
  *                iterations, number of converged dots
+ *   h_counts     int32[n_dots*6] (host, may be NULL): per dot, the launches of
+ *                SpMM, Gram and update that did work in the FP32 and the FP64
+ *                phase (for algorithmic-byte accounting)
+ *   h_prec/d_prec_mats  optional per-dot DST preconditioner (host descriptor
+ *                array, device matrices); NULL = unpreconditioned
  * The initial block is drawn from `seed` (deterministic).  Returns
  * QD_ERR_NOT_CONVERGED if any dot hits max_iter (results still written).
  * ------------------------------------------------------------------------- */
 int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b, int prec_mode,
-                             size_t *bytes);
+                             const qd_dst_prec *h_prec, size_t *bytes);
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
                     const int32_t *d_rowptr, const int32_t *d_col,
                     const double *d_H, const double *d_M,
+                    const qd_dst_prec *h_prec, const double *d_prec_mats,
                     int k, int b, int prec_mode, double tol, int max_iter, uint64_t seed,
                     double *d_X_out, double *d_E_out, double *d_res_out, int32_t *d_iters_out,
-                    int32_t *h_info, void *d_work, size_t work_bytes, void *stream);
+                    int32_t *h_info, int32_t *h_counts, void *d_work, size_t work_bytes,
+                    void *stream);
+
+/* Apply the DST preconditioner W = T R to a batch of b-column blocks
+ * (row-major, float if vec_fp32 else double; in-place allowed).  Same
+ * descriptors as qd_lobpcg_solve; exposed for testing and reuse. */
+int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int b,
+                                  const qd_dst_prec *h_prec, size_t *bytes);
+int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, int b, int vec_fp32,
+                         const qd_dst_prec *h_prec, const double *d_prec_mats,
+                         const void *d_in, void *d_out, void *d_work, size_t work_bytes,
+                         void *stream);
 
 /* ---------------------------------------------------------------------------
  * Jacobi-preconditioned CG, FP64, for nrhs right-hand sides sharing one SPD
@@ -185,6 +221,17 @@ int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states,
                const double *d_c, const double *d_psi, const double *d_w,
                const int32_t *d_nadjptr, const int32_t *d_nadj,
                double *d_dLdV, double *d_dLdc, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Per-kernel-kind timing with CUDA events, recorded on the stream of each
+ * launch (off by default).  Kinds: 0 SpMM, 1 Gram, 2 Rayleigh-Ritz, 3 update,
+ * 4 assembly, 5 PCG, 6 adjoint, 7 DST preconditioner, 8 other.  qd_prof_read
+ * synchronises the recorded events and returns cumulative milliseconds and
+ * launch counts (arrays of 9); reset != 0 clears the totals.  Benchmark instrumentation with
+ * no reference counterpart.
+ * ------------------------------------------------------------------------- */
+int qd_prof_enable(int on);
+int qd_prof_read(double *ms, int64_t *launches, int reset);
 
 #ifdef __cplusplus
 }

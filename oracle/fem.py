@@ -463,25 +463,27 @@ def dot_config_c1(seed=0, nx=100, ny=50, Lx=100.0, Ly=50.0):
     return mesh, c, Vn
 
 
-def dot_config_sweep(seed, order=2, nx=None):
-    """One dot of the batched sweep: P2, nx ~ U{40..240}, ny = nx/2, 1 nm cells,
-    radius U[5,20] nm, depth U[0.1,0.5] eV, m* 0.041 inside / 0.067 outside."""
-    rng = np.random.default_rng(seed)
-    if nx is None:
-        nx = int(rng.integers(40, 241))
-    ny = nx // 2
-    Lx, Ly = float(nx), float(ny)
-    R = rng.uniform(5, 20)
+SWEEP_SEED = 20261203
+
+
+def dot_config_sweep(i, base_seed=SWEEP_SEED, order=2, nx=None):
+    """Dot i of the batched sweep: P2, nx ~ U{40..240}, ny = nx // 2, 1 nm cells,
+    circular well of radius U[5,20] nm and depth U[0.1,0.5] eV centred within
+    +-5 nm of the middle, m* 0.041 m0 inside (element centroid) / 0.067 outside."""
+    rng = np.random.default_rng([base_seed, i])
+    n = int(rng.integers(40, 241))
+    if nx is not None:
+        n = int(nx)
+    ny = n // 2
+    Lx, Ly = float(n), float(ny)
+    R = rng.uniform(5.0, 20.0)
     depth = rng.uniform(0.1, 0.5)
-    cx = Lx / 2 + rng.uniform(-0.1, 0.1) * Lx
-    cy = Ly / 2 + rng.uniform(-0.1, 0.1) * Ly
-    mesh = structured_mesh(order, nx, ny, Lx, Ly)
-
-    def V(x, y):
-        return -depth * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * R ** 2))
-
-    Vn = V(mesh.nodes[:, 0], mesh.nodes[:, 1])
+    cx = Lx / 2 + rng.uniform(-5.0, 5.0)
+    cy = Ly / 2 + rng.uniform(-5.0, 5.0)
+    mesh = structured_mesh(order, n, ny, Lx, Ly)
+    x, y = mesh.nodes[:, 0], mesh.nodes[:, 1]
+    Vn = np.where((x - cx) ** 2 + (y - cy) ** 2 < R * R, -depth, 0.0)
     cen = centroids(mesh)
-    inside = ((cen[:, 0] - cx) ** 2 + (cen[:, 1] - cy) ** 2) < R * R
+    inside = (cen[:, 0] - cx) ** 2 + (cen[:, 1] - cy) ** 2 < R * R
     mstar = np.where(inside, 0.041, 0.067)
     return mesh, C0_EV_NM2 / mstar, Vn

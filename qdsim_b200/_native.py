@@ -45,15 +45,27 @@ SIGNATURES = {
     "qd_assemble": (_int, [_int, _int, _i64, _i64, _i32, _p, _p, _p, _p, _p,
                            _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_spmm_dual": (_int, [_i32, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p]),
-    "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _int, _int, _p]),
-    "qd_lobpcg_solve": (_int, [_i32, _p, _p, _p, _p, _p, _p, _int, _int, _int, _dbl,
-                               _int, _u64, _p, _p, _p, _p, _p, _p, _sz, _p]),
+    "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _int, _int, _p, _p]),
+    "qd_lobpcg_solve": (_int, [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _int, _int, _int, _dbl,
+                               _int, _u64, _p, _p, _p, _p, _p, _p, _p, _sz, _p]),
+    "qd_dst_precond_workspace_size": (_int, [_i32, _p, _int, _p, _p]),
+    "qd_dst_precond_apply": (_int, [_i32, _p, _int, _int, _p, _p, _p, _p, _p, _sz, _p]),
     "qd_pcg_workspace_size": (_int, [_i32, _int, _p]),
     "qd_pcg_solve": (_int, [_i32, _int, _p, _p, _p, _p, _p, _p, _dbl, _int, _p, _p,
                             _p, _sz, _p]),
+    "qd_prof_enable": (_int, [_int]),
+    "qd_prof_read": (_int, [_p, _p, _int]),
     "qd_adjoint": (_int, [_int, _i64, _i64, _int, _p, _p, _p, _p, _p, _p, _p, _p,
                           _p, _p, _p]),
 }
+
+
+# struct qd_dst_prec (include/qdsim_b200.h)
+import numpy as _np  # noqa: E402
+DST_PREC_DTYPE = _np.dtype([("nx", _np.int32), ("ny", _np.int32), ("sx_off", _np.int64),
+                            ("sy_off", _np.int64), ("cx", _np.float32), ("cy", _np.float32),
+                            ("shift", _np.float32), ("pad", _np.int32)], align=True)
+assert DST_PREC_DTYPE.itemsize == 40
 
 
 class QDError(RuntimeError):

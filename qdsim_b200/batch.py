@@ -1,0 +1,155 @@
+"""Batches of independent dots packed as one disjoint-union mesh.
+
+The union's reduced DOFs are numbered dot by dot, so its CSR pattern is block
+diagonal: one assembly launch fills every dot's H and M, and one batched
+LOBPCG call solves them all.  Per-shape CSR patterns (and assembly plans) are
+built once on the host and replicated with offsets.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .eigen import DSTPreconditioner, EigResult, Workspace, lobpcg_packed
+from .fem import FEMProblem, build_pattern, dof_map_for, stream_ptr
+
+_SHAPE_CACHE: dict = {}
+
+
+def _shape_pattern(mesh, dirichlet=True):
+    key = (mesh.shape_key(), dirichlet)
+    if key not in _SHAPE_CACHE:
+        dm, n = dof_map_for(mesh, dirichlet)
+        _SHAPE_CACHE[key] = (dm, n, build_pattern(mesh.elems, dm, n, mesh.num_nodes))
+    return _SHAPE_CACHE[key]
+
+
+class HostBatch:
+    """Host (numpy) arrays of the union mesh, its pattern and coefficients."""
+
+    def __init__(self, dots, dirichlet=True, precondition=True):
+        if not dots:
+            raise ValueError("empty batch")
+        order = dots[0].mesh.order
+        if any(d.mesh.order != order for d in dots):
+            raise ValueError("all dots in a batch must share the element order")
+        self.order = order
+        self.n_dots = len(dots)
+        nodes, elems, dmaps, cs, Vs = [], [], [], [], []
+        rowptr, col, adjptr, adj, cptr, contrib, slotcnt = [], [], [], [], [], [], []
+        node_off = elem_off = row_off = nnz_off = adj_off = con_off = 0
+        self.row_off = [0]
+        self.nnz_per_dot = []
+        self.rows_per_dot = []
+        for d in dots:
+            m = d.mesh
+            dm, n, P = _shape_pattern(m, dirichlet)
+            nodes.append(m.nodes)
+            elems.append(m.elems + node_off)
+            dmaps.append(np.where(dm >= 0, dm + row_off, -1))
+            cs.append(np.asarray(d.c, np.float64))
+            Vs.append(np.asarray(d.V, np.float64))
+            rowptr.append(P.rowptr[:-1] + nnz_off)
+            col.append(P.col + row_off)
+            adjptr.append(P.adjptr[:-1] + adj_off)
+            adj.append(P.adj + (elem_off << 4))
+            cptr.append(P.cptr[:-1] + con_off)
+            contrib.append(P.contrib)
+            slotcnt.append(P.slotcnt)
+            node_off += m.num_nodes
+            elem_off += m.num_elements
+            row_off += n
+            nnz_off += P.nnz
+            adj_off += P.adj.size
+            con_off += P.contrib.size
+            self.row_off.append(row_off)
+            self.nnz_per_dot.append(P.nnz)
+            self.rows_per_dot.append(n)
+        if nnz_off >= 2**31 or con_off >= 2**31 or elem_off >= 2**27:
+            raise ValueError("batch too large for the int32 CSR / plan indices")
+        i32 = lambda parts, last: np.ascontiguousarray(  # noqa: E731
+            np.concatenate(parts + [np.array([last], np.int64)]).astype(np.int32))
+        self.arrays = {
+            "nodes": np.ascontiguousarray(np.concatenate(nodes).astype(np.float64)),
+            "elems": np.ascontiguousarray(np.concatenate(elems).astype(np.int32)),
+            "c": np.ascontiguousarray(np.concatenate(cs)),
+            "V": np.ascontiguousarray(np.concatenate(Vs)),
+            "rowptr": i32(rowptr, nnz_off),
+            "col": np.ascontiguousarray(np.concatenate(col).astype(np.int32)),
+            "adjptr": i32(adjptr, adj_off),
+            "adj": np.ascontiguousarray(np.concatenate(adj).astype(np.int32)),
+            "cptr": i32(cptr, con_off),
+            "contrib": np.ascontiguousarray(np.concatenate(contrib)),
+            "slotcnt": np.ascontiguousarray(np.concatenate(slotcnt)),
+        }
+        self.dof_map = np.concatenate(dmaps).astype(np.int32)
+        self.num_nodes = node_off
+        self.num_elems = elem_off
+        self.n = row_off
+        self.nnz = nnz_off
+        self.row_off = np.asarray(self.row_off, dtype=np.int32)
+        self.prec_specs = ([DSTPreconditioner.spec_for(d.mesh, d.c, d.V) for d in dots]
+                           if (precondition and dirichlet) else None)
+
+    def pin(self):
+        """Page-locked copies of the input arrays (for timed host->device copies)."""
+        return {k: torch.from_numpy(v).pin_memory() for k, v in self.arrays.items()}
+
+    def input_bytes(self) -> int:
+        return int(sum(v.nbytes for v in self.arrays.values()))
+
+
+class DeviceBatch:
+    """Device-resident union mesh; ``assemble`` + ``solve`` are the hot path."""
+
+    def __init__(self, host: HostBatch, device="cuda"):
+        self.host = host
+        self.device = torch.device(device)
+        self.d = {k: torch.empty(v.shape, dtype=torch.from_numpy(v[:0]).dtype, device=self.device)
+                  for k, v in host.arrays.items()}
+        self.H = torch.empty(host.nnz, dtype=torch.float64, device=self.device)
+        self.M = torch.empty(host.nnz, dtype=torch.float64, device=self.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.ws = Workspace(self.device)
+        self.precond = (DSTPreconditioner(host.prec_specs, self.device)
+                        if host.prec_specs is not None else None)
+
+    def upload(self, pinned=None, non_blocking=True):
+        src = pinned if pinned is not None else {k: torch.from_numpy(v) for k, v in self.host.arrays.items()}
+        for k, t in src.items():
+            self.d[k].copy_(t, non_blocking=non_blocking)
+
+    def assemble(self, stream=None):
+        h, d = self.host, self.d
+        self.status.zero_()
+        N.check(N.lib().qd_assemble(
+            h.order, N.QD_ASM_FEM, h.num_nodes, h.num_elems, h.n, N.ptr(d["nodes"]),
+            N.ptr(d["elems"]), N.ptr(d["c"]), N.ptr(d["V"]), None, N.ptr(d["rowptr"]),
+            N.ptr(d["adjptr"]), N.ptr(d["adj"]), N.ptr(d["cptr"]), N.ptr(d["contrib"]),
+            N.ptr(d["slotcnt"]), N.ptr(self.H), N.ptr(self.M), None, N.ptr(self.status),
+            stream_ptr(stream)), "qd_assemble")
+
+    def solve(self, k, **kw):
+        h = self.host
+        kw.setdefault("precond", self.precond)
+        return lobpcg_packed(h.row_off, self.d["rowptr"], self.d["col"], self.H, self.M, k,
+                             workspace=self.ws, **kw)
+
+    def check_status(self):
+        flag = int(self.status.item())
+        if flag:
+            raise N.QDError(N.QD_ERR_DEGENERATE, f"qd_assemble (flag {flag})")
+
+
+def solve_dots(dots, k, device="cuda", **kw) -> EigResult:
+    """Assemble and solve a list of ``workloads.Dot`` on the GPU."""
+    hb = HostBatch(dots)
+    db = DeviceBatch(hb, device)
+    db.upload(non_blocking=False)
+    db.assemble()
+    db.check_status()
+    E, X, R, it, info, st = db.solve(k, **kw)
+    ro = hb.row_off
+    return EigResult(E.cpu().numpy(), [X[ro[i]:ro[i + 1]] for i in range(hb.n_dots)],
+                     R.cpu().numpy(), it.cpu().numpy(), info, st)

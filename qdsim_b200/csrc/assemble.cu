@@ -165,9 +165,11 @@ int launch_assemble(int mode, int32_t n, const double *nodes, const int32_t *ele
   if (n == 0) return QD_OK;
   int64_t blocks = (int64_t(n) + kWarps - 1) / kWarps;
   if (blocks > 148 * 64) blocks = 148 * 64;
+  qd::prof_begin(qd::PK_ASSEMBLE, s);
   assemble_rows_kernel<K><<<int(blocks), kWarps * 32, 0, s>>>(
       mode, n, reinterpret_cast<const double2 *>(nodes), elems, c, V, W, rowptr, adjptr, adj,
       cptr, contrib, slotcnt, H, M, Him, status);
+  qd::prof_end(qd::PK_ASSEMBLE, s);
   QD_CHECK_LAUNCH();
   return QD_OK;
 }

@@ -14,6 +14,16 @@ namespace qd {
 // counts kernels launched by this library (reported by qd_kernel_launch_count)
 extern std::atomic<uint64_t> g_launches;
 
+// Optional per-kernel-kind timing with CUDA events (qd_prof_*).  Disabled by
+// default; when enabled every instrumented launch records an event pair on its
+// own stream, resolved by qd_prof_read.
+enum ProfKind { PK_SPMM = 0, PK_GRAM, PK_RR, PK_UPDATE, PK_ASSEMBLE, PK_PCG, PK_ADJOINT, PK_PRECOND,
+                PK_OTHER, PK_COUNT };
+#ifdef __CUDACC__
+void prof_begin(int kind, cudaStream_t s);
+void prof_end(int kind, cudaStream_t s);
+#endif
+
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Bump allocator over a caller-provided workspace.

@@ -13,15 +13,19 @@
 // once for a dot that has converged, so one launch serves the whole batch and
 // the work of uneven dots is balanced by the hardware scheduler.
 //
-// Per iteration (S = [X W P], products kept in HS = [HX HW HP], MS = [MX MW MP]):
-//   gram   : per chunk, A_c = S^T HS and B_c = S^T MS (3B x 3B), FP64 accumulation
-//   rr     : per dot (one CTA), A = sum_c A_c, B = sum_c B_c; Cholesky of the
-//            column-scaled B, C = L^-1 A L^-T, cyclic Jacobi eigensolve of C,
-//            Ritz coefficients Y -- all FP64 in shared memory
-//   update : per chunk, X = S Y, P = [W P] Y_wp, same for HS/MS, residual
+// Per iteration (S = [X W P], HS = [HX HW HP], MS = [MX MW MP]):
+//   spmm_xp: explicit HX, MX, HP, MP (FP64 accumulation), residual
 //            W = HX - MX Theta and its per-column norms
-//   spmm   : HW = H W, MW = M W (FP64 accumulation)
-// Every kRefresh iterations HX, MX, HP, MP are recomputed from X and P.
+//   precond: W = T W (DST preconditioner, when the dot has a lattice)
+//   spmm   : HW = H W, MW = M W
+//   gram   : per chunk, A_c = S^T HS and B_c = S^T MS (3B x 3B)
+//   rr     : per dot (one CTA): convergence test, A = sum_c A_c, B = sum_c B_c,
+//            SVQB orthonormalisation of the basis and a cyclic Jacobi
+//            eigensolve, Ritz coefficients Y -- all FP64 in shared memory
+//   update : X = S Y, P = [W P] Y_wp
+// Recomputing the products of X and P every iteration (instead of updating
+// them with the Ritz coefficients) keeps the residual consistent with X even
+// when the basis is nearly dependent and the coefficients are large.
 //
 // Precision: QD_PREC_FP64 stores vectors in FP64.  QD_PREC_MIXED runs the
 // same iteration with FP32 vector storage and FP32 update arithmetic (matrix
@@ -34,16 +38,17 @@
 #include <vector>
 #include "common.h"
 #include "spmm.cuh"
+#include "dstprec.cuh"
 
 namespace {
 
 constexpr int kChunkRows = 2048;
 constexpr int kMaxB = 16;
 constexpr int kMaxM = 3 * kMaxB;
-constexpr int kRefresh32 = 20;
-constexpr int kRefresh64 = 40;
-constexpr int kStagWindow = 40;
-constexpr double kTol32 = 5e-5;
+constexpr int kStagWindow = 30;     // FP32 iterations without halving the estimate
+constexpr double kTol32Floor = 1e-7; // FP32 phase target (estimated rel. eigenvalue error)
+constexpr double kSafety = 1.0;
+constexpr double kRelCap = 1e-2;     // never stop while the relative residual exceeds this
 
 struct Chunk {
   int dot, begin, end, pad;
@@ -60,6 +65,8 @@ struct DotState {
   int have_res;     // residual norms of the current X are available
   int chunk0, chunk1;
   double best;      // best max relative residual in this phase
+  int launches[2][3];   // [FP32, FP64 phase][spmm, gram, update] launches that did work
+  int pad2;
 };
 
 // ---------------------------------------------------------------------------
@@ -115,10 +122,101 @@ __global__ void spmm_chunk_kernel(const Chunk *chunks, const DotState *st,
   constexpr int G = B / 4;
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].active) return;
+  if (threadIdx.x == 0 && blockIdx.x == st[ch.dot].chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][0]++;
   const int sub = threadIdx.x / G, g = threadIdx.x % G;
   const int rpp = blockDim.x / G;
   for (int r = ch.begin + sub; r < ch.end; r += rpp)
     qd::spmm_row<TV, B, true>(r, g, rowptr, col, H, M, X, HX, MX);
+}
+
+// Explicit products of the current X and P (no drift from implicit updates):
+// HX, MX, HP, MP, the residual W = HX - MX Theta and per-chunk column norms
+// sum r^2 and sum (Mx)^2.  2G threads per row: g < G own X columns, the rest P.
+template <typename TV, int B>
+__global__ void __launch_bounds__(128 * (B / 4))
+spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
+               const int32_t *__restrict__ col, const double *__restrict__ H,
+               const double *__restrict__ M, const double *__restrict__ theta,
+               const TV *__restrict__ X, const TV *__restrict__ P, TV *__restrict__ HX,
+               TV *__restrict__ MX, TV *__restrict__ HP, TV *__restrict__ MP,
+               TV *__restrict__ W, double *__restrict__ norms) {
+  constexpr int G = B / 4;
+  constexpr int G2 = 2 * G;
+  constexpr int RPP = 64;   // rows per pass (blockDim = 64 * G2)
+  __shared__ double s_th[B];
+  __shared__ double s_red[RPP * G2 * 8];
+  const Chunk ch = chunks[blockIdx.x];
+  const DotState &sd = st[ch.dot];
+  if (!sd.active) return;
+  const bool with_p = sd.has_p != 0;
+  if (threadIdx.x == 0 && blockIdx.x == sd.chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][0]++;
+  if (threadIdx.x < B) s_th[threadIdx.x] = theta[size_t(ch.dot) * B + threadIdx.x];
+  __syncthreads();
+  const int sub = threadIdx.x / G2, gg = threadIdx.x % G2;
+  const bool isx = gg < G;
+  const int g = isx ? gg : gg - G;
+  double rr[4] = {0, 0, 0, 0}, mm[4] = {0, 0, 0, 0};
+  for (int r = ch.begin + sub; r < ch.end; r += RPP) {
+    if (!isx && !with_p) {
+      double z[4] = {0, 0, 0, 0};
+      qd::V4<TV>::store(HP + size_t(r) * B + 4 * g, z);
+      qd::V4<TV>::store(MP + size_t(r) * B + 4 * g, z);
+      continue;
+    }
+    double h[4] = {0, 0, 0, 0}, m[4] = {0, 0, 0, 0};
+    const TV *src = isx ? X : P;
+    const int p0 = __ldg(rowptr + r), p1 = __ldg(rowptr + r + 1);
+#pragma unroll 4
+    for (int p = p0; p < p1; ++p) {
+      const int j = __ldg(col + p);
+      const double hv = __ldg(H + p), mv = __ldg(M + p);
+      double x[4];
+      qd::V4<TV>::load(src + size_t(j) * B + 4 * g, x);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        h[c] = fma(hv, x[c], h[c]);
+        m[c] = fma(mv, x[c], m[c]);
+      }
+    }
+    const size_t o = size_t(r) * B + 4 * g;
+    if (isx) {
+      double res[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        // residual from the stored (rounded) products, as the iteration sees them
+        const double hq = double(TV(h[c])), mq = double(TV(m[c]));
+        res[c] = hq - s_th[4 * g + c] * mq;
+        rr[c] += res[c] * res[c];
+        mm[c] += mq * mq;
+      }
+      qd::V4<TV>::store(HX + o, h);
+      qd::V4<TV>::store(MX + o, m);
+      qd::V4<TV>::store(W + o, res);
+    } else {
+      qd::V4<TV>::store(HP + o, h);
+      qd::V4<TV>::store(MP + o, m);
+    }
+  }
+  // per-chunk column norms (fixed-order reduction over the CTA's rows)
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    s_red[(threadIdx.x * 4 + c) * 2] = rr[c];
+    s_red[(threadIdx.x * 4 + c) * 2 + 1] = mm[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < B) {
+    const int j = threadIdx.x, gj = j / 4, cj = j % 4;
+    double a = 0.0, b = 0.0;
+    for (int sr = 0; sr < RPP; ++sr) {
+      const int t = sr * G2 + gj;
+      a += s_red[(t * 4 + cj) * 2];
+      b += s_red[(t * 4 + cj) * 2 + 1];
+    }
+    norms[size_t(blockIdx.x) * 2 * B + j] = a;
+    norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -152,6 +250,8 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].active) return;
   const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][1]++;
   const bool worker = tid < NBLK * RG;
   const int blk = tid % NBLK, rg = tid / NBLK;
   const int bi = blk / NB, bj = blk % NB;
@@ -265,6 +365,112 @@ struct RRParams {
   int max_iter;    // total iteration cap per dot
 };
 
+__device__ inline double cta_sum(double v, double *s_red) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  __syncthreads();
+  s_red[tid] = v;
+  __syncthreads();
+  for (int w = nt / 2; w > 0; w >>= 1) {
+    if (tid < w) s_red[tid] += s_red[tid + w];
+    __syncthreads();
+  }
+  const double r = s_red[0];
+  __syncthreads();
+  return r;
+}
+
+// Cyclic Jacobi eigensolver for a symmetric n x n matrix A (leading dimension
+// ld, shared memory) with round-robin pairing; V (ld) receives the
+// eigenvectors as columns, A's diagonal the eigenvalues.  A pair is rotated
+// only while |a_pq| > eps sqrt(|a_pp a_qq|) (the relative threshold of
+// Demmel and Veselic), so tiny eigenvalues of a scaled SPD Gram matrix come out
+// with high relative accuracy; the sweeps stop when a sweep rotates nothing.
+// Odd n uses a dummy index that is never rotated.  All threads must call it.
+__device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, double *s_c,
+                           double *s_s, int *s_p, int *s_q) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  __shared__ int s_rot;
+  for (int idx = tid; idx < n * n; idx += nt) {
+    const int i = idx / n, j = idx % n;
+    V[i * ld + j] = (i == j) ? 1.0 : 0.0;
+  }
+  (void)s_red;
+  const int ne = (n + 1) & ~1;   // even count including the dummy
+  if (ne < 2) return;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    __syncthreads();
+    if (tid == 0) s_rot = 0;
+    __syncthreads();
+    for (int round = 0; round < ne - 1; ++round) {
+      if (tid < ne / 2) {
+        int p, q;
+        if (tid == 0) {
+          p = 0;
+          q = 1 + (round % (ne - 1));
+        } else {
+          p = 1 + ((tid + round) % (ne - 1));
+          q = 1 + ((ne - 1 - tid + round) % (ne - 1));
+        }
+        if (p > q) {
+          const int t = p; p = q; q = t;
+        }
+        double c = 1.0, sn = 0.0;
+        if (q < n) {
+          const double apq = A[p * ld + q];
+          const double app = A[p * ld + p], aqq = A[q * ld + q];
+          if (fabs(apq) > 1e-300 && fabs(apq) > 1e-16 * sqrt(fabs(app * aqq))) {
+            const double tau = (aqq - app) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = rsqrt(1.0 + t * t);
+            sn = t * c;
+            s_rot = 1;
+          } else {
+            q = -1;
+          }
+        } else {
+          q = -1;   // pair with the dummy: no rotation
+        }
+        s_c[tid] = c;
+        s_s[tid] = sn;
+        s_p[tid] = p;
+        s_q[tid] = q;
+      }
+      __syncthreads();
+      const int np = ne / 2;
+      for (int idx = tid; idx < np * n; idx += nt) {   // rows
+        const int t = idx / n, j = idx % n;
+        const int p = s_p[t], q = s_q[t];
+        if (q < 0) continue;
+        const double c = s_c[t], sn = s_s[t];
+        const double a = A[p * ld + j], b = A[q * ld + j];
+        A[p * ld + j] = c * a - sn * b;
+        A[q * ld + j] = sn * a + c * b;
+      }
+      __syncthreads();
+      for (int idx = tid; idx < np * n; idx += nt) {   // columns (and V)
+        const int t = idx / n, i = idx % n;
+        const int p = s_p[t], q = s_q[t];
+        if (q < 0) continue;
+        const double c = s_c[t], sn = s_s[t];
+        const double a = A[i * ld + p], b = A[i * ld + q];
+        A[i * ld + p] = c * a - sn * b;
+        A[i * ld + q] = sn * a + c * b;
+        const double va = V[i * ld + p], vb = V[i * ld + q];
+        V[i * ld + p] = c * va - sn * vb;
+        V[i * ld + q] = sn * va + c * vb;
+      }
+      __syncthreads();
+    }
+    if (!s_rot) break;
+  }
+  __syncthreads();
+}
+
+// Rayleigh-Ritz on span[X W P] by SVQB: with D the diagonal scaling of the
+// basis Gram B, eigendecompose D B D = U S U^T, drop directions with
+// S < tau max(S) (near-dependent or null columns, e.g. a preconditioned
+// residual that is almost parallel to X), Q = U_keep S_keep^-1/2, then solve
+// the standard problem (Q^T D A D Q) z = theta z and return Y = D Q Z.
 template <int B>
 __global__ void __launch_bounds__(256)
 rr_kernel(DotState *st, const double *partial, const double *norms, double *theta,
@@ -272,14 +478,16 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   constexpr int m = 3 * B;
   extern __shared__ double sm[];
   double *sA = sm;             // m*m
-  double *sB = sA + m * m;     // m*m  (B, then its Cholesky factor L)
-  double *sT = sB + m * m;     // m*m  (L^-1)
-  double *sZ = sT + m * m;     // m*m  (temp, then eigenvectors)
+  double *sB = sA + m * m;     // m*m
+  double *sT = sB + m * m;     // m*m
+  double *sZ = sT + m * m;     // m*m
   double *sD = sZ + m * m;     // m    column scaling
   double *sE = sD + m;         // m    eigenvalues
   double *sR = sE + m;         // B    relative residuals
-  __shared__ int s_flag, s_fail, s_sel[kMaxM];
+  __shared__ int s_flag, s_r, s_keep[kMaxM], s_sel[kMaxM];
   __shared__ double s_red[256];
+  __shared__ double s_c[kMaxM / 2 + 1], s_s[kMaxM / 2 + 1];
+  __shared__ int s_p[kMaxM / 2 + 1], s_q[kMaxM / 2 + 1];
 
   const int d = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   DotState &s = st[d];
@@ -288,7 +496,13 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   if (tid == 0) s_flag = 0;
   __syncthreads();
 
-  // 1. convergence test on the residual norms of the current X
+  // 1. convergence test on the residual norms of the current X.
+  // rel_j = ||r_j|| / (|theta_j| ||M x_j||) is reported; the stopping rule is
+  // the quadratic eigenvalue-error estimate
+  //   est_j = kSafety (||r_j|| / ||M x_j||)^2 / ((theta_{B-1} - theta_j) |theta_j|)
+  // (residual squared over the gap to the block edge, relative to |theta_j|;
+  // kSafety covers ||r||_{M^-1} exceeding ||r|| / ||M x|| for residuals in the
+  // high modes of M).
   if (s.have_res) {
     if (tid < B) {
       double rr = 0.0, mx = 0.0;
@@ -296,24 +510,30 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
         rr += norms[size_t(c) * 2 * B + tid];
         mx += norms[size_t(c) * 2 * B + B + tid];
       }
-      double scale = fabs(th[tid]);
-      if (prm.phase32) scale = fmax(scale, fabs(th[B - 1] - th[0]));
-      scale = fmax(scale, 1e-300);
-      const double rel = sqrt(rr / fmax(mx, 1e-300)) / scale;
-      sR[tid] = rel;
+      const double at = fmax(fabs(th[tid]), 1e-300);
+      const double ares = sqrt(rr / fmax(mx, 1e-300));
+      const double gap = fmax(th[B - 1] - th[tid], 1e-300);
+      const double rel = ares / at;
+      double est = kSafety * ares * ares / (gap * at);
+      if (!isfinite(est)) est = 1e300;
+      sE[tid] = est;                               // uncapped, for the stagnation test
+      sR[tid] = (rel <= kRelCap) ? est : 1e300;
       relres[size_t(d) * B + tid] = rel;
     }
     __syncthreads();
     if (tid == 0) {
-      double worst = 0.0;
-      for (int j = 0; j < prm.k; ++j) worst = fmax(worst, isfinite(sR[j]) ? sR[j] : 1e300);
+      double worst = 0.0, worst_raw = 0.0;
+      for (int j = 0; j < prm.k; ++j) {
+        worst = fmax(worst, sR[j]);
+        worst_raw = fmax(worst_raw, sE[j]);
+      }
       int stop = 0;
       if (worst <= prm.tol) {
         stop = 1;
         if (!prm.phase32) s.status = 1;
       } else if (prm.phase32) {
-        if (worst < 0.8 * s.best) {
-          s.best = worst;
+        if (worst_raw < 0.5 * s.best) {
+          s.best = worst_raw;
           s.stag = 0;
         } else if (++s.stag >= kStagWindow) {
           stop = 1;
@@ -332,218 +552,107 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     if (s_flag) return;
   }
 
-  // 2. Gram matrices summed over the dot's chunks (fixed order)
+  // 2. Gram matrices summed over the dot's chunks (fixed order), symmetrised
   for (int idx = tid; idx < m * m; idx += nt) {
     double a = 0.0, b = 0.0;
     for (int c = s.chunk0; c < s.chunk1; ++c) {
       a += partial[size_t(c) * 2 * m * m + idx];
       b += partial[size_t(c) * 2 * m * m + m * m + idx];
     }
-    sA[idx] = a;
-    sZ[idx] = b;   // keep the raw B for a retry without P
+    sT[idx] = a;
+    sZ[idx] = b;
   }
   __syncthreads();
-  int has_p = s.has_p;
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    // symmetrise, drop P if requested, scale columns
-    for (int idx = tid; idx < m * m; idx += nt) {
-      const int i = idx / m, j = idx % m;
-      double a = 0.5 * (sA[i * m + j] + sA[j * m + i]);
-      double b = 0.5 * (sZ[i * m + j] + sZ[j * m + i]);
-      if (!has_p && (i >= 2 * B || j >= 2 * B)) a = b = 0.0;
-      sT[idx] = a;        // temporarily the symmetric A
-      sB[idx] = b;
-    }
-    __syncthreads();
-    // column scaling from the diagonal of B
-    double dmax = 0.0;
-    for (int i = 0; i < m; ++i) dmax = fmax(dmax, sB[i * m + i]);
-    if (tid < m) {
-      const double bii = sB[tid * m + tid];
-      sD[tid] = (bii > 1e-26 * dmax && isfinite(bii)) ? rsqrt(bii) : 0.0;
-    }
-    __syncthreads();
-    double amax = 0.0;
-    for (int i = 0; i < m; ++i) amax = fmax(amax, fabs(sT[i * m + i]) * sD[i] * sD[i]);
-    __syncthreads();   // every thread has read the unscaled diagonal
-    for (int idx = tid; idx < m * m; idx += nt) {
-      const int i = idx / m, j = idx % m;
-      double a = sT[idx] * sD[i] * sD[j];
-      double b = sB[idx] * sD[i] * sD[j];
-      if (i == j && sD[i] == 0.0) {
-        b = 1.0;
-        a = 1e6 * (amax + 1.0);   // decoupled (null) column: far above the spectrum
-      }
-      sT[idx] = a;
-      sB[idx] = b;
-    }
-    if (tid == 0) s_fail = 0;
-    __syncthreads();
-    // Cholesky of B in place (lower)
-    for (int j = 0; j < m; ++j) {
-      if (tid == 0) {
-        const double piv = sB[j * m + j];
-        if (!(piv > 1e-13)) s_fail = 1;
-        else sB[j * m + j] = sqrt(piv);
-      }
-      __syncthreads();
-      if (s_fail) break;
-      const double ljj = sB[j * m + j];
-      for (int i = j + 1 + tid; i < m; i += nt) sB[i * m + j] /= ljj;
-      __syncthreads();
-      const int rem = m - j - 1;
-      for (int idx = tid; idx < rem * rem; idx += nt) {
-        const int i = j + 1 + idx / rem, l = j + 1 + idx % rem;
-        if (l <= i) sB[i * m + l] -= sB[i * m + j] * sB[l * m + j];
-      }
-      __syncthreads();
-    }
-    if (!s_fail) break;
-    if (!has_p) break;
-    has_p = 0;   // retry without the P block
-    __syncthreads();
+  const bool has_p = s.has_p != 0;
+  if (tid < m) {
+    const double bii = sZ[tid * m + tid];
+    const bool use = (has_p || tid < 2 * B) && bii > 0.0 && isfinite(bii);
+    sD[tid] = use ? rsqrt(bii) : 0.0;
   }
-  if (s_fail) {
+  __syncthreads();
+  for (int idx = tid; idx < m * m; idx += nt) {
+    const int i = idx / m, j = idx % m;
+    const double dd = sD[i] * sD[j];
+    sA[idx] = 0.5 * (sT[i * m + j] + sT[j * m + i]) * dd;
+    sB[idx] = 0.5 * (sZ[i * m + j] + sZ[j * m + i]) * dd;
+  }
+  __syncthreads();
+  // 3. SVQB: eigendecompose the scaled basis Gram, keep the well-conditioned span
+  jacobi_cta(sB, sZ, m, m, s_red, s_c, s_s, s_p, s_q);
+  if (tid == 0) {
+    double smax = 0.0;
+    for (int i = 0; i < m; ++i) smax = fmax(smax, sB[i * m + i]);
+    const double tau = prm.phase32 ? 1e-6 : 1e-12;
+    int r = 0;
+    for (int i = 0; i < m; ++i)
+      if (sB[i * m + i] > tau * smax && smax > 0.0) s_keep[r++] = i;
+    s_r = r;
+  }
+  __syncthreads();
+  const int r = s_r;
+  if (r < B || !(r > 0)) {
     if (tid == 0) {
       s.active = 0;
       s.status = 2;
     }
     return;
   }
-  // move A (scaled) to sA; L^-1 into sT
-  for (int idx = tid; idx < m * m; idx += nt) sA[idx] = sT[idx];
-  __syncthreads();
-  if (tid < m) {
-    const int j = tid;
-    for (int i = 0; i < m; ++i) {
-      if (i < j) {
-        sT[i * m + j] = 0.0;
-        continue;
-      }
-      double sum = (i == j) ? 1.0 : 0.0;
-      for (int l = j; l < i; ++l) sum -= sB[i * m + l] * sT[l * m + j];
-      sT[i * m + j] = sum / sB[i * m + i];
+  // Q = U_keep S_keep^-1/2 (m x r) into sT
+  for (int idx = tid; idx < m * m; idx += nt) {
+    const int i = idx / m, c = idx % m;
+    double q = 0.0;
+    if (c < r) {
+      const int kc = s_keep[c];
+      q = sZ[i * m + kc] * rsqrt(sB[kc * m + kc]);
     }
+    sT[idx] = q;
   }
   __syncthreads();
-  // Z = A L^-T ; C = L^-1 Z  (C into sB, which is free now)
-  for (int idx = tid; idx < m * m; idx += nt) {
-    const int i = idx / m, j = idx % m;
+  // sZ = A' Q (m x r);  sB = Q^T sZ (r x r)
+  for (int idx = tid; idx < m * r; idx += nt) {
+    const int i = idx / r, c = idx % r;
     double sum = 0.0;
-    for (int l = 0; l <= j; ++l) sum += sA[i * m + l] * sT[j * m + l];
-    sZ[idx] = sum;
+    for (int l = 0; l < m; ++l) sum += sA[i * m + l] * sT[l * m + c];
+    sZ[i * m + c] = sum;
   }
   __syncthreads();
-  for (int idx = tid; idx < m * m; idx += nt) {
-    const int i = idx / m, j = idx % m;
+  for (int idx = tid; idx < r * r; idx += nt) {
+    const int i = idx / r, j = idx % r;
     double sum = 0.0;
-    for (int l = 0; l <= i; ++l) sum += sT[i * m + l] * sZ[l * m + j];
-    sB[idx] = sum;
+    for (int l = 0; l < m; ++l) sum += sT[l * m + i] * sZ[l * m + j];
+    sB[i * m + j] = sum;
   }
   __syncthreads();
-  for (int idx = tid; idx < m * m; idx += nt) {
-    const int i = idx / m, j = idx % m;
-    sA[idx] = 0.5 * (sB[i * m + j] + sB[j * m + i]);
-    sZ[idx] = (i == j) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  // cyclic Jacobi with round-robin pairing (m even)
-  __shared__ double s_c[kMaxM / 2], s_s[kMaxM / 2];
-  __shared__ int s_p[kMaxM / 2], s_q[kMaxM / 2];
-  for (int sweep = 0; sweep < 40; ++sweep) {
-    double off = 0.0, fro = 0.0;
-    for (int idx = tid; idx < m * m; idx += nt) {
-      const int i = idx / m, j = idx % m;
-      const double v = sA[idx] * sA[idx];
-      fro += v;
-      if (i != j) off += v;
-    }
-    s_red[tid] = off;
-    __syncthreads();
-    for (int w = nt / 2; w > 0; w >>= 1) {
-      if (tid < w) s_red[tid] += s_red[tid + w];
-      __syncthreads();
-    }
-    off = s_red[0];
-    __syncthreads();
-    s_red[tid] = fro;
-    __syncthreads();
-    for (int w = nt / 2; w > 0; w >>= 1) {
-      if (tid < w) s_red[tid] += s_red[tid + w];
-      __syncthreads();
-    }
-    fro = s_red[0];
-    __syncthreads();
-    if (off <= 1e-30 * fro) break;
-    for (int round = 0; round < m - 1; ++round) {
-      if (tid < m / 2) {
-        int p, q;
-        if (tid == 0) {
-          p = 0;
-          q = 1 + (round % (m - 1));
-        } else {
-          p = 1 + ((tid + round) % (m - 1));
-          q = 1 + ((m - 1 - tid + round) % (m - 1));
-        }
-        if (p > q) {
-          const int t = p; p = q; q = t;
-        }
-        const double apq = sA[p * m + q];
-        double c = 1.0, sn = 0.0;
-        if (fabs(apq) > 1e-300) {
-          const double tau = (sA[q * m + q] - sA[p * m + p]) / (2.0 * apq);
-          const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-          c = rsqrt(1.0 + t * t);
-          sn = t * c;
-        }
-        s_c[tid] = c;
-        s_s[tid] = sn;
-        s_p[tid] = p;
-        s_q[tid] = q;
-      }
-      __syncthreads();
-      for (int idx = tid; idx < (m / 2) * m; idx += nt) {   // rows
-        const int t = idx / m, j = idx % m;
-        const int p = s_p[t], q = s_q[t];
-        const double c = s_c[t], sn = s_s[t];
-        const double a = sA[p * m + j], b = sA[q * m + j];
-        sA[p * m + j] = c * a - sn * b;
-        sA[q * m + j] = sn * a + c * b;
-      }
-      __syncthreads();
-      for (int idx = tid; idx < (m / 2) * m; idx += nt) {   // columns (and Z)
-        const int t = idx / m, i = idx % m;
-        const int p = s_p[t], q = s_q[t];
-        const double c = s_c[t], sn = s_s[t];
-        const double a = sA[i * m + p], b = sA[i * m + q];
-        sA[i * m + p] = c * a - sn * b;
-        sA[i * m + q] = sn * a + c * b;
-        const double za = sZ[i * m + p], zb = sZ[i * m + q];
-        sZ[i * m + p] = c * za - sn * zb;
-        sZ[i * m + q] = sn * za + c * zb;
-      }
-      __syncthreads();
+  for (int idx = tid; idx < r * r; idx += nt) {
+    const int i = idx / r, j = idx % r;
+    if (i < j) {
+      const double v = 0.5 * (sB[i * m + j] + sB[j * m + i]);
+      sB[i * m + j] = v;
+      sB[j * m + i] = v;
     }
   }
-  if (tid < m) sE[tid] = sA[tid * m + tid];
   __syncthreads();
-  if (tid < m) {
+  // 4. standard eigenproblem of size r; eigenvectors into sA
+  jacobi_cta(sB, sA, r, m, s_red, s_c, s_s, s_p, s_q);
+  if (tid < r) sE[tid] = sB[tid * m + tid];
+  __syncthreads();
+  if (tid < r) {
     const double e = sE[tid];
     int rank = 0;
-    for (int j = 0; j < m; ++j) {
+    for (int j = 0; j < r; ++j) {
       const double f = sE[j];
       rank += (f < e) || (f == e && j < tid);
     }
     s_sel[rank] = tid;
   }
   __syncthreads();
-  // Y = D L^-T Z[:, sel]  (m x B)
+  // 5. Y = D Q Z[:, sel]  (m x B)
   double *Y = coef + size_t(d) * m * B;
   for (int idx = tid; idx < m * B; idx += nt) {
     const int i = idx / B, c = idx % B;
     const int zc = s_sel[c];
     double sum = 0.0;
-    for (int l = i; l < m; ++l) sum += sT[l * m + i] * sZ[l * m + zc];
+    for (int l = 0; l < r; ++l) sum += sT[i * m + l] * sA[l * m + zc];
     Y[idx] = sD[i] * sum;
   }
   if (tid < B) th[tid] = sE[s_sel[tid]];
@@ -566,80 +675,50 @@ template <int B> struct UpdCfg {
   static constexpr int THREADS = R * B;
 };
 
+// X = S Y, P = [W P] Y_wp  (S = [X W P]); products are recomputed explicitly
+// at the start of the next iteration.
 template <typename TV, int B>
 __global__ void __launch_bounds__(UpdCfg<B>::THREADS)
-update_kernel(const Chunk *chunks, const DotState *st, const double *coef, const double *theta,
-              TV *X, TV *W, TV *P, TV *HX, TV *HW, TV *HP, TV *MX, TV *MW, TV *MP,
-              double *norms) {
+update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X, const TV *W,
+              TV *P) {
   constexpr int m = 3 * B, R = UpdCfg<B>::R;
   using ACC = TV;   // FP32 arithmetic in the FP32 phase, FP64 in the FP64 phase
   __shared__ ACC sY[m * B];
-  __shared__ ACC sTh[B];
-  __shared__ TV sIn[R * 9 * B];
-  __shared__ double sRed[R * B * 2];
+  __shared__ TV sIn[R * 3 * B];
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].active) return;
   const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][2]++;
   const double *Yg = coef + size_t(ch.dot) * m * B;
   for (int i = tid; i < m * B; i += blockDim.x) sY[i] = ACC(Yg[i]);
-  if (tid < B) sTh[tid] = ACC(theta[size_t(ch.dot) * B + tid]);
-  TV *src[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
+  const TV *src[3] = {X, W, P};
   const int row = tid / B, j = tid % B;
-  double rr = 0.0, mm = 0.0;
   for (int r0 = ch.begin; r0 < ch.end; r0 += R) {
     const int nr = min(R, ch.end - r0);
     __syncthreads();
-    for (int idx = tid; idx < 9 * R * B; idx += blockDim.x) {
-      const int a = idx / (R * B), rem = idx % (R * B);
-      const int rr_ = rem / B, cc = rem % B;
-      sIn[rr_ * 9 * B + a * B + cc] = (rr_ < nr) ? src[a][size_t(r0 + rr_) * B + cc] : TV(0);
-    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      for (int idx = tid; idx < R * B; idx += blockDim.x) {
+        const int rr_ = idx / B, cc = idx % B;
+        sIn[rr_ * 3 * B + a * B + cc] = (rr_ < nr) ? src[a][size_t(r0 + rr_) * B + cc] : TV(0);
+      }
     __syncthreads();
     if (row < nr) {
-      const TV *in = sIn + row * 9 * B;
-      ACC x = 0, p = 0, hx = 0, hp = 0, mx = 0, mp = 0;
+      const TV *in = sIn + row * 3 * B;
+      ACC x = 0, p = 0;
 #pragma unroll
-      for (int i = 0; i < B; ++i) {
-        const ACC y = sY[i * B + j];
-        x = fma(ACC(in[i]), y, x);
-        hx = fma(ACC(in[3 * B + i]), y, hx);
-        mx = fma(ACC(in[6 * B + i]), y, mx);
-      }
+      for (int i = 0; i < B; ++i) x = fma(ACC(in[i]), sY[i * B + j], x);
 #pragma unroll
       for (int i = B; i < 3 * B; ++i) {
-        const ACC y = sY[i * B + j];
-        const ACC s0 = ACC(in[i]), h0 = ACC(in[3 * B + i]), m0 = ACC(in[6 * B + i]);
-        x = fma(s0, y, x);
-        hx = fma(h0, y, hx);
-        mx = fma(m0, y, mx);
-        p = fma(s0, y, p);
-        hp = fma(h0, y, hp);
-        mp = fma(m0, y, mp);
+        const ACC v = ACC(in[i]) * sY[i * B + j];
+        x += v;
+        p += v;
       }
-      const ACC res = hx - sTh[j] * mx;
       const size_t o = size_t(r0 + row) * B + j;
       X[o] = TV(x);
       P[o] = TV(p);
-      HX[o] = TV(hx);
-      HP[o] = TV(hp);
-      MX[o] = TV(mx);
-      MP[o] = TV(mp);
-      W[o] = TV(res);
-      rr += double(res) * double(res);
-      mm += double(mx) * double(mx);
     }
-  }
-  sRed[tid] = rr;
-  sRed[R * B + tid] = mm;
-  __syncthreads();
-  if (tid < B) {
-    double a = 0.0, b = 0.0;
-    for (int rr_ = 0; rr_ < R; ++rr_) {
-      a += sRed[rr_ * B + tid];
-      b += sRed[R * B + rr_ * B + tid];
-    }
-    norms[size_t(blockIdx.x) * 2 * B + tid] = a;
-    norms[size_t(blockIdx.x) * 2 * B + B + tid] = b;
   }
 }
 
@@ -699,6 +778,12 @@ struct Layout {
   int *count;
   double *slot[9];
   int nchunks;
+  // DST preconditioner
+  double *tmp1, *tmp2;   // used as float in the FP32 phase
+  qd_dst_prec *desc;
+  qd::GemmTile *tiles_x, *tiles_y;
+  int64_t ntx, nty;
+  const double *mats;
 };
 
 size_t rr_smem_bytes(int B) {
@@ -706,7 +791,8 @@ size_t rr_smem_bytes(int B) {
   return size_t(4 * m * m + 2 * m + B) * sizeof(double);
 }
 
-int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, Layout &L) {
+int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t ntx,
+          int64_t nty, Layout &L) {
   const int m = 3 * B;
   L.chunks = ar.take<Chunk>(nchunks);
   L.row_off = ar.take<int32_t>(n_dots + 1);
@@ -719,6 +805,20 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, Layout 
   L.count = ar.take<int>(4);
   for (int i = 0; i < 9; ++i) L.slot[i] = ar.take<double>(size_t(n_rows) * B);
   L.nchunks = nchunks;
+  L.ntx = ntx;
+  L.nty = nty;
+  L.mats = nullptr;
+  if (ntx > 0) {
+    L.tmp1 = ar.take<double>(size_t(n_rows) * B);
+    L.tmp2 = ar.take<double>(size_t(n_rows) * B);
+    L.desc = ar.take<qd_dst_prec>(n_dots);
+    L.tiles_x = ar.take<qd::GemmTile>(ntx);
+    L.tiles_y = ar.take<qd::GemmTile>(nty);
+  } else {
+    L.tmp1 = L.tmp2 = nullptr;
+    L.desc = nullptr;
+    L.tiles_x = L.tiles_y = nullptr;
+  }
   return QD_OK;
 }
 
@@ -751,34 +851,45 @@ int run_phase(const Layout &L, const int *perm, int n_dots, const int32_t *rowpt
   const size_t rr_smem = rr_smem_bytes(B);
   QD_CUDA_TRY(cudaFuncSetAttribute(rr_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(rr_smem)));
-  const int refresh = prm.phase32 ? kRefresh32 : kRefresh64;
-  spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col, H, M,
-                                                              b.X, b.HX, b.MX);
-  QD_CHECK_LAUNCH();
   int host_count = n_dots;
   iters_run = 0;
   for (int it = 0; it < prm.max_iter + 1; ++it) {
-    if (it > 0 && it % refresh == 0) {
-      spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col,
-                                                                  H, M, b.X, b.HX, b.MX);
-      QD_CHECK_LAUNCH();
-      spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col,
-                                                                  H, M, b.P, b.HP, b.MP);
-      QD_CHECK_LAUNCH();
+    // explicit H/M products of X and P, residual W = HX - MX Theta and its norms
+    qd::prof_begin(qd::PK_SPMM, s);
+    spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, H, M,
+                                                        L.theta, b.X, b.P, b.HX, b.MX, b.HP,
+                                                        b.MP, b.W, L.norms);
+    qd::prof_end(qd::PK_SPMM, s);
+    QD_CHECK_LAUNCH();
+    if (L.ntx > 0) {
+      qd::prof_begin(qd::PK_PRECOND, s);
+      cudaError_t e = qd::dst_apply<TV>(L.tiles_x, L.ntx, L.tiles_y, L.nty, &L.st[0].active,
+                                        int(sizeof(DotState) / sizeof(int)), L.desc, L.row_off,
+                                        L.mats, B, b.W, b.W, reinterpret_cast<TV *>(L.tmp1),
+                                        reinterpret_cast<TV *>(L.tmp2), s);
+      qd::prof_end(qd::PK_PRECOND, s);
+      if (e != cudaSuccess) return QD_ERR_CUDA;
     }
+    qd::prof_begin(qd::PK_SPMM, s);
+    spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col, H,
+                                                                M, b.W, b.HW, b.MW);
+    qd::prof_end(qd::PK_SPMM, s);
+    QD_CHECK_LAUNCH();
+    qd::prof_begin(qd::PK_GRAM, s);
     gram_kernel<TV, B><<<L.nchunks, GC::THREADS, 0, s>>>(L.chunks, L.st, b.X, b.W, b.P, b.HX,
                                                          b.HW, b.HP, b.MX, b.MW, b.MP,
                                                          L.partial);
+    qd::prof_end(qd::PK_GRAM, s);
     QD_CHECK_LAUNCH();
+    qd::prof_begin(qd::PK_RR, s);
     rr_kernel<B><<<n_dots, 256, rr_smem, s>>>(L.st, L.partial, L.norms, L.theta, L.coef,
                                               L.relres, prm);
+    qd::prof_end(qd::PK_RR, s);
     QD_CHECK_LAUNCH();
-    update_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(
-        L.chunks, L.st, L.coef, L.theta, b.X, b.W, b.P, b.HX, b.HW, b.HP, b.MX, b.MW, b.MP,
-        L.norms);
-    QD_CHECK_LAUNCH();
-    spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col, H,
-                                                                M, b.W, b.HW, b.MW);
+    qd::prof_begin(qd::PK_UPDATE, s);
+    update_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(L.chunks, L.st, L.coef, b.X,
+                                                                  b.W, b.P);
+    qd::prof_end(qd::PK_UPDATE, s);
     QD_CHECK_LAUNCH();
     ++iters_run;
     if (it % 8 == 7 || it == prm.max_iter) {
@@ -794,22 +905,48 @@ int run_phase(const Layout &L, const int *perm, int n_dots, const int32_t *rowpt
 
 template <int B>
 int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
-            const int32_t *d_col, const double *d_H, const double *d_M, int k, int prec_mode,
+            const int32_t *d_col, const double *d_H, const double *d_M,
+            const qd_dst_prec *h_prec, const double *d_mats, int k, int prec_mode,
             double tol, int max_iter, uint64_t seed, double *d_X_out, double *d_E_out,
-            double *d_res_out, int32_t *d_iters_out, int32_t *h_info, void *d_work,
-            size_t work_bytes, cudaStream_t s) {
+            double *d_res_out, int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
+            void *d_work, size_t work_bytes, cudaStream_t s) {
   const int64_t n_rows = h_row_off[n_dots];
   const int nchunks = count_chunks(n_dots, h_row_off);
+  int64_t ntx = 0, nty = 0;
+  if (h_prec) {
+    if (!d_mats) return QD_ERR_INVALID;
+    for (int d = 0; d < n_dots; ++d) {
+      const qd_dst_prec &q = h_prec[d];
+      if (q.nx <= 0) continue;
+      if (q.ny <= 0 || int64_t(q.nx) * q.ny != h_row_off[d + 1] - h_row_off[d] ||
+          q.sx_off < 0 || q.sy_off < 0 || !(q.cx > 0.f) || !(q.cy > 0.f) || !(q.shift >= 0.f))
+        return QD_ERR_INVALID;
+    }
+    qd::dst_tiles(n_dots, h_prec, B, nullptr, &ntx, nullptr, &nty);
+  }
   {
     qd::Arena need(nullptr, 0);
     Layout tmp;
-    carve(need, n_dots, n_rows, B, nchunks, tmp);
+    carve(need, n_dots, n_rows, B, nchunks, ntx, nty, tmp);
     if (need.used > work_bytes) return QD_ERR_WORKSPACE;
   }
   if (reinterpret_cast<uintptr_t>(d_work) % 256 != 0) return QD_ERR_WORKSPACE;
   qd::Arena ar(d_work, work_bytes);
   Layout L;
-  carve(ar, n_dots, n_rows, B, nchunks, L);
+  carve(ar, n_dots, n_rows, B, nchunks, ntx, nty, L);
+  std::vector<qd::GemmTile> htx, hty;
+  if (ntx > 0) {
+    htx.resize(ntx);
+    hty.resize(nty);
+    qd::dst_tiles(n_dots, h_prec, B, htx.data(), &ntx, hty.data(), &nty);
+    L.mats = d_mats;
+    QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_x, htx.data(), ntx * sizeof(qd::GemmTile),
+                                cudaMemcpyHostToDevice, s));
+    QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_y, hty.data(), nty * sizeof(qd::GemmTile),
+                                cudaMemcpyHostToDevice, s));
+    QD_CUDA_TRY(cudaMemcpyAsync(L.desc, h_prec, n_dots * sizeof(qd_dst_prec),
+                                cudaMemcpyHostToDevice, s));
+  }
   // chunk table and per-dot state
   std::vector<Chunk> chunks;
   chunks.reserve(nchunks);
@@ -849,7 +986,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
                                                   b.HW, b.MW, b.HP, b.MP);
     QD_CHECK_LAUNCH();
     prm.phase32 = 1;
-    prm.tol = std::max(tol, kTol32);
+    prm.tol = std::max(100.0 * tol, kTol32Floor);
     int st32 = run_phase<float, B>(L, perm0, n_dots, d_rowptr, d_col, d_H, d_M, prm, s, it32);
     if (st32 != QD_OK) return st32;
     // X (float, slot 0) -> double in slot 1; slot 1 becomes X, slot 0 becomes W
@@ -892,6 +1029,10 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     nconv += (x.status == 1);
     nbreak += (x.status == 2);
   }
+  if (h_counts)
+    for (int d = 0; d < n_dots; ++d)
+      for (int ph = 0; ph < 2; ++ph)
+        for (int kd = 0; kd < 3; ++kd) h_counts[d * 6 + ph * 3 + kd] = st[d].launches[ph][kd];
   if (h_info) {
     h_info[0] = it32 + it64;
     h_info[1] = it32;
@@ -906,25 +1047,29 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
 }  // namespace
 
 extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b,
-                                        int prec_mode, size_t *bytes) {
+                                        int prec_mode, const qd_dst_prec *h_prec,
+                                        size_t *bytes) {
   (void)prec_mode;
   if (!bytes || n_dots <= 0 || n_rows_total <= 0 || b < 4 || b > kMaxB || b % 4) return QD_ERR_INVALID;
   // upper bound on the chunk count: every dot contributes at most one partial chunk
   const int nchunks = int(n_rows_total / kChunkRows) + n_dots;
+  int64_t ntx = 0, nty = 0;
+  if (h_prec) qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);
   Layout L;
-  carve(ar, n_dots, n_rows_total, b, nchunks, L);
+  carve(ar, n_dots, n_rows_total, b, nchunks, ntx, nty, L);
   *bytes = ar.used;
   return QD_OK;
 }
 
 extern "C" int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off,
                                const int32_t *d_row_off, const int32_t *d_rowptr,
-                               const int32_t *d_col, const double *d_H, const double *d_M, int k,
+                               const int32_t *d_col, const double *d_H, const double *d_M,
+                               const qd_dst_prec *h_prec, const double *d_prec_mats, int k,
                                int b, int prec_mode, double tol, int max_iter, uint64_t seed,
                                double *d_X_out, double *d_E_out, double *d_res_out,
-                               int32_t *d_iters_out, int32_t *h_info, void *d_work,
-                               size_t work_bytes, void *stream) {
+                               int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
+                               void *d_work, size_t work_bytes, void *stream) {
   (void)d_row_off;
   if (n_dots <= 0 || !h_row_off || !d_rowptr || !d_col || !d_H || !d_M || !d_X_out ||
       !d_E_out || !d_res_out || !d_iters_out || !d_work)
@@ -939,10 +1084,10 @@ extern "C" int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off,
     if (h_row_off[d + 1] - h_row_off[d] < b + 1) return QD_ERR_INVALID;  // need n > b
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (b) {
-    case 4: return solve_b<4>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, d_work, work_bytes, s);
-    case 8: return solve_b<8>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, d_work, work_bytes, s);
-    case 12: return solve_b<12>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, d_work, work_bytes, s);
-    default: return solve_b<16>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, d_work, work_bytes, s);
+    case 4: return solve_b<4>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
+    case 8: return solve_b<8>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
+    case 12: return solve_b<12>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
+    default: return solve_b<16>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
   }
 }
 
@@ -1000,4 +1145,62 @@ extern "C" int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32, const int32_t *
     default: return QD_ERR_INVALID;
   }
 #undef QD_SPMM_CASE
+}
+
+extern "C" int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int b,
+                                             const qd_dst_prec *h_prec, size_t *bytes) {
+  if (n_dots <= 0 || !h_row_off || !h_prec || !bytes || b < 1) return QD_ERR_INVALID;
+  int64_t ntx = 0, nty = 0;
+  qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
+  qd::Arena ar(nullptr, 0);
+  ar.take<double>(size_t(h_row_off[n_dots]) * b);
+  ar.take<double>(size_t(h_row_off[n_dots]) * b);
+  ar.take<qd_dst_prec>(n_dots);
+  ar.take<int32_t>(n_dots + 1);
+  ar.take<qd::GemmTile>(ntx);
+  ar.take<qd::GemmTile>(nty);
+  *bytes = ar.used;
+  return QD_OK;
+}
+
+extern "C" int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, int b, int vec_fp32,
+                                    const qd_dst_prec *h_prec, const double *d_prec_mats,
+                                    const void *d_in, void *d_out, void *d_work,
+                                    size_t work_bytes, void *stream) {
+  if (n_dots <= 0 || !h_row_off || !h_prec || !d_prec_mats || !d_in || !d_out || !d_work || b < 1)
+    return QD_ERR_INVALID;
+  for (int d = 0; d < n_dots; ++d) {
+    const qd_dst_prec &q = h_prec[d];
+    if (q.nx > 0 && int64_t(q.nx) * q.ny != h_row_off[d + 1] - h_row_off[d]) return QD_ERR_INVALID;
+  }
+  size_t need = 0;
+  int st = qd_dst_precond_workspace_size(n_dots, h_row_off, b, h_prec, &need);
+  if (st != QD_OK) return st;
+  if (need > work_bytes || reinterpret_cast<uintptr_t>(d_work) % 256) return QD_ERR_WORKSPACE;
+  int64_t ntx = 0, nty = 0;
+  qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
+  std::vector<qd::GemmTile> tx(ntx), ty(nty);
+  qd::dst_tiles(n_dots, h_prec, b, tx.data(), &ntx, ty.data(), &nty);
+  qd::Arena ar(d_work, work_bytes);
+  const size_t nv = size_t(h_row_off[n_dots]) * b;
+  double *t1 = ar.take<double>(nv), *t2 = ar.take<double>(nv);
+  qd_dst_prec *desc = ar.take<qd_dst_prec>(n_dots);
+  int32_t *ro = ar.take<int32_t>(n_dots + 1);
+  qd::GemmTile *dtx = ar.take<qd::GemmTile>(ntx), *dty = ar.take<qd::GemmTile>(nty);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  QD_CUDA_TRY(cudaMemcpyAsync(desc, h_prec, n_dots * sizeof(qd_dst_prec), cudaMemcpyHostToDevice, s));
+  QD_CUDA_TRY(cudaMemcpyAsync(ro, h_row_off, (n_dots + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  if (ntx) QD_CUDA_TRY(cudaMemcpyAsync(dtx, tx.data(), ntx * sizeof(qd::GemmTile), cudaMemcpyHostToDevice, s));
+  if (nty) QD_CUDA_TRY(cudaMemcpyAsync(dty, ty.data(), nty * sizeof(qd::GemmTile), cudaMemcpyHostToDevice, s));
+  cudaError_t e;
+  if (vec_fp32)
+    e = qd::dst_apply<float>(dtx, ntx, dty, nty, nullptr, 0, desc, ro, d_prec_mats, b,
+                             static_cast<const float *>(d_in), static_cast<float *>(d_out),
+                             reinterpret_cast<float *>(t1), reinterpret_cast<float *>(t2), s);
+  else
+    e = qd::dst_apply<double>(dtx, ntx, dty, nty, nullptr, 0, desc, ro, d_prec_mats, b,
+                              static_cast<const double *>(d_in), static_cast<double *>(d_out), t1, t2, s);
+  if (e != cudaSuccess) return QD_ERR_CUDA;
+  QD_CUDA_TRY(cudaStreamSynchronize(s));   // host tile tables die at return
+  return QD_OK;
 }

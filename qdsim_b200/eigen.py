@@ -49,11 +49,50 @@ def pack_block_diagonal(mats):
     return np.asarray(row_off, dtype=np.int32), rowptr, col, H, M
 
 
-def workspace_bytes(n_dots: int, n_rows: int, b: int, prec: int) -> int:
+def workspace_bytes(n_dots: int, n_rows: int, b: int, prec: int, h_prec=None) -> int:
     out = C.c_size_t()
-    N.check(N.lib().qd_lobpcg_workspace_size(n_dots, n_rows, b, prec, C.byref(out)),
-            "qd_lobpcg_workspace_size")
+    N.check(N.lib().qd_lobpcg_workspace_size(n_dots, n_rows, b, prec, N.ptr(h_prec),
+                                             C.byref(out)), "qd_lobpcg_workspace_size")
     return int(out.value)
+
+
+class DSTPreconditioner:
+    """Per-dot fast-sine-transform preconditioner data (host descriptors and
+    device DST-I matrices) for structured rectangular meshes with Dirichlet
+    elimination; dots without a lattice get nx = 0 (unpreconditioned)."""
+
+    def __init__(self, specs, device):
+        """specs: per dot (nx, ny, cx, cy, shift) or None."""
+        self.desc = np.zeros(len(specs), dtype=N.DST_PREC_DTYPE)
+        sizes = sorted({s[i] for s in specs if s is not None for i in (0, 1)})
+        offs, mats, pos = {}, [], 0
+        for n in sizes:
+            j = np.arange(1, n + 1)
+            S = np.sqrt(2.0 / (n + 1)) * np.sin(np.pi * np.outer(j, j) / (n + 1))
+            offs[n] = pos
+            mats.append(S.ravel())
+            pos += S.size
+        for d, s in enumerate(specs):
+            if s is None:
+                continue
+            nx, ny, cx, cy, shift = s
+            self.desc[d] = (nx, ny, offs[nx], offs[ny], cx, cy, shift, 0)
+        flat = np.concatenate(mats) if mats else np.zeros(1, np.float64)
+        self.d_mats = torch.from_numpy(flat).to(device)
+
+    @staticmethod
+    def spec_for(mesh, c, V):
+        """(nx, ny, cx, cy, shift) for a StructuredMesh with Dirichlet elimination."""
+        p = mesh.order
+        nx, ny = p * mesh.nx - 1, p * mesh.ny - 1
+        if nx < 1 or ny < 1:
+            return None
+        hx, hy = mesh.Lx / (p * mesh.nx), mesh.Ly / (p * mesh.ny)
+        cbar = float(np.exp(np.mean(np.log(np.asarray(c, np.float64)))))
+        V = np.asarray(V, np.float64)
+        sigma = V.min() - 0.25 * (V.max() - V.min()) - 0.05
+        shift = (max(0.0, -sigma) + 0.05) * hx * hy
+        return (nx, ny, cbar * hy / hx, cbar * hx / hy, shift)
 
 
 class Workspace:
@@ -71,7 +110,7 @@ class Workspace:
 
 def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=1e-6,
                   max_iter=2000, seed=1234, workspace: Workspace | None = None, stream=None,
-                  allow_not_converged=True):
+                  allow_not_converged=True, precond: DSTPreconditioner | None = None):
     """Solve a packed block-diagonal batch; returns (E, X_all, res, iters, info, status)."""
     n_dots = len(row_off) - 1
     n_rows = int(row_off[-1])
@@ -80,22 +119,26 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
     b = int(b)
     prec = N.QD_PREC_MIXED if precision == "mixed" else N.QD_PREC_FP64
     dev = H.device
-    nbytes = workspace_bytes(n_dots, n_rows, b, prec)
+    h_prec = precond.desc if precond is not None else None
+    d_mats = precond.d_mats if precond is not None else None
+    nbytes = workspace_bytes(n_dots, n_rows, b, prec, h_prec)
     ws = (workspace or Workspace(dev)).get(nbytes)
     X = torch.empty(n_rows * k, dtype=torch.float64, device=dev)
     E = torch.empty(n_dots * k, dtype=torch.float64, device=dev)
     R = torch.empty(n_dots * k, dtype=torch.float64, device=dev)
     it = torch.empty(n_dots, dtype=torch.int32, device=dev)
     info = np.zeros(4, dtype=np.int32)
+    counts = np.zeros((n_dots, 6), dtype=np.int32)
     ro = np.ascontiguousarray(row_off, dtype=np.int32)
     st = N.lib().qd_lobpcg_solve(
-        n_dots, N.ptr(ro), None, N.ptr(rowptr), N.ptr(col), N.ptr(H), N.ptr(M), k, b, prec,
+        n_dots, N.ptr(ro), None, N.ptr(rowptr), N.ptr(col), N.ptr(H), N.ptr(M), N.ptr(h_prec),
+        N.ptr(d_mats), k, b, prec,
         float(tol), int(max_iter), int(seed), N.ptr(X), N.ptr(E), N.ptr(R), N.ptr(it),
-        N.ptr(info), N.ptr(ws), ws.numel(), stream_ptr(stream))
+        N.ptr(info), N.ptr(counts), N.ptr(ws), ws.numel(), stream_ptr(stream))
     N.check(st, "qd_lobpcg_solve",
             allow=(N.QD_ERR_NOT_CONVERGED,) if allow_not_converged else ())
     infod = {"iterations": int(info[0]), "iters_fp32": int(info[1]), "iters_fp64": int(info[2]),
-             "converged_dots": int(info[3]), "block": b}
+             "converged_dots": int(info[3]), "block": b, "launch_counts": counts}
     return E.view(n_dots, k), X.view(n_rows, k), R.view(n_dots, k), it, infod, st
 
 

@@ -7,7 +7,7 @@ from oracle import fem as O
 pytestmark = pytest.mark.gpu
 
 
-def _solve_single(cuda, om, c, V, k, precision, b=None, tol=1e-6):
+def _solve_single(cuda, om, c, V, k, precision, b=None, tol=1e-9):
     from qdsim_b200 import fem as F, eigen as G, mesh as Mh
     m = Mh.StructuredMesh(om.order, om.nx, om.ny, om.Lx, om.Ly)
     prob = F.FEMProblem(m, device=cuda)
@@ -39,7 +39,7 @@ def test_c1_lowest10(cuda, precision):
 
 def test_batch_matches_single(cuda):
     from qdsim_b200 import fem as F, eigen as G, mesh as Mh
-    dots = [O.dot_config_sweep(seed, 2, nx) for seed, nx in ((1, 20), (2, 28), (3, 24))]
+    dots = [O.dot_config_sweep(seed, nx=nx) for seed, nx in ((1, 20), (2, 28), (3, 24))]
     mats, probs, refs = [], [], []
     for om, c, V in dots:
         m = Mh.StructuredMesh(2, om.nx, om.ny, om.Lx, om.Ly)
@@ -49,20 +49,20 @@ def test_batch_matches_single(cuda):
         probs.append(p)
         ra = O.assemble(om, c, V)
         refs.append(O.eig_lowest(ra.H, ra.M, 8, O.sigma_below(V))[0])
-    res = G.solve_batch(mats, 8, b=12, precision="mixed", tol=1e-6, max_iter=3000)
+    res = G.solve_batch(mats, 8, b=12, precision="mixed", tol=1e-9, max_iter=3000)
     assert res.status == 0, res.info
     for i in range(3):
         rel = np.abs(res.E[i] - refs[i]) / np.abs(refs[i])
         assert rel.max() <= 1e-9, (i, rel)
     # solving one dot alone gives the same eigenvalues as inside the batch
-    single = G.solve_batch(mats[1:2], 8, b=12, precision="mixed", tol=1e-6, max_iter=3000)
+    single = G.solve_batch(mats[1:2], 8, b=12, precision="mixed", tol=1e-9, max_iter=3000)
     assert np.allclose(single.E[0], res.E[1], rtol=1e-10, atol=0)
 
 
 def test_spmm_dual_matches_scipy(cuda):
     import torch
     from qdsim_b200 import fem as F, mesh as Mh, _native as N
-    om, c, V = O.dot_config_sweep(5, 2, 30)
+    om, c, V = O.dot_config_sweep(5, nx=30)
     m = Mh.StructuredMesh(2, om.nx, om.ny, om.Lx, om.Ly)
     p = F.FEMProblem(m, device=cuda)
     a = p.assemble(c, V)
@@ -84,3 +84,21 @@ def test_spmm_dual_matches_scipy(cuda):
                 ref = A @ Xr
                 err = np.abs(got.double().cpu().numpy() - ref).max() / np.abs(ref).max()
                 assert err < tol, (b, fp32, err)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_preconditioned_sweep_dots(cuda, precision):
+    """Batched solve of sweep dots through the product path (DST-preconditioned)."""
+    from qdsim_b200 import batch as Bt, workloads as W
+    ids = [0, 1, 2, 3, 17]
+    dots = [W.sweep_dot(i, nx=nx) for i, nx in zip(ids, (40, 64, 52, 90, 41))]
+    res = Bt.solve_dots(dots, 8, device=cuda, b=12, precision=precision, tol=1e-9,
+                        max_iter=1000)
+    assert res.status == 0, res.info
+    assert res.info["iterations"] < 200, res.info      # preconditioning works
+    for j, (i, nx) in enumerate(zip(ids, (40, 64, 52, 90, 41))):
+        om, c, V = O.dot_config_sweep(i, nx=nx)
+        a = O.assemble(om, c, V)
+        E0 = O.eig_lowest(a.H, a.M, 8, O.sigma_below(V))[0]
+        rel = np.abs(res.E[j] - E0) / np.abs(E0)
+        assert rel.max() <= 1e-9, (j, rel, res.info)
