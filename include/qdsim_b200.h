@@ -225,9 +225,10 @@ int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states,
 /* ---------------------------------------------------------------------------
  * Per-kernel-kind timing with CUDA events, recorded on the stream of each
  * launch (off by default).  Kinds: 0 SpMM, 1 Gram, 2 Rayleigh-Ritz, 3 update,
- * 4 assembly, 5 PCG, 6 adjoint, 7 DST preconditioner, 8 other.  qd_prof_read
- * synchronises the recorded events and returns cumulative milliseconds and
- * launch counts (arrays of 9); reset != 0 clears the totals.  Benchmark instrumentation with
+ * 4 assembly, 5 PCG, 6 adjoint, 7 DST preconditioner, 8 orthogonalisation,
+ * 9 other.  qd_prof_read synchronises the recorded events and returns
+ * cumulative milliseconds and launch counts (arrays of 10); reset != 0 clears
+ * the totals.  Benchmark instrumentation with
  * no reference counterpart.
  * ------------------------------------------------------------------------- */
 int qd_prof_enable(int on);

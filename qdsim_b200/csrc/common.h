@@ -18,7 +18,7 @@ extern std::atomic<uint64_t> g_launches;
 // default; when enabled every instrumented launch records an event pair on its
 // own stream, resolved by qd_prof_read.
 enum ProfKind { PK_SPMM = 0, PK_GRAM, PK_RR, PK_UPDATE, PK_ASSEMBLE, PK_PCG, PK_ADJOINT, PK_PRECOND,
-                PK_OTHER, PK_COUNT };
+                PK_ORTHO, PK_OTHER, PK_COUNT };
 #ifdef __CUDACC__
 void prof_begin(int kind, cudaStream_t s);
 void prof_end(int kind, cudaStream_t s);

@@ -48,7 +48,13 @@ constexpr int kMaxM = 3 * kMaxB;
 constexpr int kStagWindow = 30;     // FP32 iterations without halving the estimate
 constexpr double kTol32Floor = 1e-7; // FP32 phase target (estimated rel. eigenvalue error)
 constexpr double kSafety = 1.0;
-constexpr double kRelCap = 1e-2;     // never stop while the relative residual exceeds this
+constexpr double kRelCap = 1e-2;
+#ifndef QD_SVQB_TAU64
+#define QD_SVQB_TAU64 1e-12
+#endif
+#ifndef QD_SVQB_TAU32
+#define QD_SVQB_TAU32 1e-6
+#endif     // never stop while the relative residual exceeds this
 
 struct Chunk {
   int dot, begin, end, pad;
@@ -582,7 +588,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   if (tid == 0) {
     double smax = 0.0;
     for (int i = 0; i < m; ++i) smax = fmax(smax, sB[i * m + i]);
-    const double tau = prm.phase32 ? 1e-6 : 1e-12;
+    const double tau = prm.phase32 ? QD_SVQB_TAU32 : QD_SVQB_TAU64;
     int r = 0;
     for (int i = 0; i < m; ++i)
       if (sB[i * m + i] > tau * smax && smax > 0.0) s_keep[r++] = i;
@@ -718,6 +724,115 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
       const size_t o = size_t(r0 + row) * B + j;
       X[o] = TV(x);
       P[o] = TV(p);
+    }
+  }
+}
+
+// M-orthogonalisation of W and P against X, in memory:
+//   C_W = X^T M W = (MX)^T W,  C_P = (MX)^T P   (X is M-orthonormal)
+//   W <- W - X C_W,  P <- P - X C_P,  HP <- HP - HX C_P,  MP <- MP - MX C_P.
+// Near convergence the preconditioned residual is dominated by a component
+// along X and the useful correction is 1e-6..1e-8 of it; removed here by an
+// elementwise subtraction it stays accurate, whereas inside the small
+// Rayleigh-Ritz problem it would sit below the resolution of the Gram matrix
+// and the iteration stalls.
+template <typename TV, int B>
+__global__ void __launch_bounds__(256)
+ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const TV *W,
+                  const TV *P, double *partial) {
+  constexpr int SUB = 32;
+  __shared__ TV sM[SUB * B], sW[SUB * B], sP[SUB * B];
+  const Chunk ch = chunks[blockIdx.x];
+  const DotState &sd = st[ch.dot];
+  if (!sd.active) return;
+  const bool with_p = sd.has_p != 0;
+  const int tid = threadIdx.x;
+  constexpr int NOUT = 2 * B * B;
+  double acc[(NOUT + 255) / 256];
+#pragma unroll
+  for (int q = 0; q < (NOUT + 255) / 256; ++q) acc[q] = 0.0;
+  for (int r0 = ch.begin; r0 < ch.end; r0 += SUB) {
+    const int nr = min(SUB, ch.end - r0);
+    __syncthreads();
+    for (int idx = tid; idx < SUB * B; idx += blockDim.x) {
+      const int rr = idx / B;
+      const size_t o = size_t(r0) * B + idx;
+      sM[idx] = rr < nr ? MX[o] : TV(0);
+      sW[idx] = rr < nr ? W[o] : TV(0);
+      sP[idx] = (rr < nr && with_p) ? P[o] : TV(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < (NOUT + 255) / 256; ++q) {
+      const int e = tid + q * 256;
+      if (e >= NOUT) continue;
+      const int which = e / (B * B), ij = e % (B * B), i = ij / B, j = ij % B;
+      const TV *src = which ? sP : sW;
+      double a = 0.0;
+      for (int rr = 0; rr < nr; ++rr) a = fma(double(sM[rr * B + i]), double(src[rr * B + j]), a);
+      acc[q] += a;
+    }
+  }
+  double *out = partial + size_t(blockIdx.x) * NOUT;
+#pragma unroll
+  for (int q = 0; q < (NOUT + 255) / 256; ++q) {
+    const int e = tid + q * 256;
+    if (e < NOUT) out[e] = acc[q];
+  }
+}
+
+template <typename TV, int B>
+__global__ void __launch_bounds__(UpdCfg<B>::THREADS)
+ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *partial, const TV *X,
+                   const TV *HX, const TV *MX, TV *W, TV *P, TV *HP, TV *MP) {
+  constexpr int R = UpdCfg<B>::R;
+  constexpr int NOUT = 2 * B * B;
+  __shared__ TV sC[NOUT];
+  __shared__ TV sIn[R * 3 * B];
+  const Chunk ch = chunks[blockIdx.x];
+  const DotState &sd = st[ch.dot];
+  if (!sd.active) return;
+  const bool with_p = sd.has_p != 0;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < NOUT; e += blockDim.x) {
+    double a = 0.0;
+    for (int c = sd.chunk0; c < sd.chunk1; ++c) a += partial[size_t(c) * NOUT + e];
+    sC[e] = TV(a);
+  }
+  const TV *src[3] = {X, HX, MX};
+  const int row = tid / B, j = tid % B;
+  for (int r0 = ch.begin; r0 < ch.end; r0 += R) {
+    const int nr = min(R, ch.end - r0);
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (a > 0 && !with_p) break;
+      for (int idx = tid; idx < R * B; idx += blockDim.x) {
+        const int rr = idx / B, cc = idx % B;
+        sIn[rr * 3 * B + a * B + cc] = (rr < nr) ? src[a][size_t(r0 + rr) * B + cc] : TV(0);
+      }
+    }
+    __syncthreads();
+    if (row < nr) {
+      const TV *in = sIn + row * 3 * B;
+      const size_t o = size_t(r0 + row) * B + j;
+      TV dw = 0;
+#pragma unroll
+      for (int i = 0; i < B; ++i) dw = fma(in[i], sC[i * B + j], dw);
+      W[o] = W[o] - dw;
+      if (with_p) {
+        TV dp = 0, dhp = 0, dmp = 0;
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+          const TV c = sC[B * B + i * B + j];
+          dp = fma(in[i], c, dp);
+          dhp = fma(in[B + i], c, dhp);
+          dmp = fma(in[2 * B + i], c, dmp);
+        }
+        P[o] = P[o] - dp;
+        HP[o] = HP[o] - dhp;
+        MP[o] = MP[o] - dmp;
+      }
     }
   }
 }
@@ -870,6 +985,13 @@ int run_phase(const Layout &L, const int *perm, int n_dots, const int32_t *rowpt
       qd::prof_end(qd::PK_PRECOND, s);
       if (e != cudaSuccess) return QD_ERR_CUDA;
     }
+    qd::prof_begin(qd::PK_ORTHO, s);
+    ortho_gram_kernel<TV, B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, b.MX, b.W, b.P, L.partial);
+    QD_CHECK_LAUNCH();
+    ortho_apply_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(
+        L.chunks, L.st, L.partial, b.X, b.HX, b.MX, b.W, b.P, b.HP, b.MP);
+    qd::prof_end(qd::PK_ORTHO, s);
+    QD_CHECK_LAUNCH();
     qd::prof_begin(qd::PK_SPMM, s);
     spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col, H,
                                                                 M, b.W, b.HW, b.MW);
