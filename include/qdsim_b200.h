@@ -203,6 +203,12 @@ int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_
                  double tol, int max_iter, int32_t *h_iters, double *h_relres,
                  void *d_work, size_t work_bytes, void *stream);
 
+/* Y = alpha A X for nrhs row-major columns (generic FP64 CSR product).  Used
+ * for the Poisson right-hand side M (-rho), which
+ * qdsim_cython/solvers/poisson_solver.pyx:254-274 forms as mass_matrix.dot(rhs). */
+int qd_csr_spmv(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_col,
+                const double *d_A, const double *d_X, double *d_Y, double alpha, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Adjoint (Hellmann-Feynman) gradients of L = sum_s w_s E_s with respect to
  * nodal V and the per-element kinetic coefficient c.  With M-normalised

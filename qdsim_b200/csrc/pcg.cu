@@ -14,6 +14,7 @@
 // bitwise reproducible, no atomics.  The step scalars are computed on the
 // device; the host only reads the convergence flag every few iterations.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <vector>
 #include "common.h"
@@ -271,4 +272,32 @@ extern "C" int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const 
   if (h_iters) *h_iters = it;
   if (h_relres) *h_relres = worst;
   return done ? QD_OK : QD_ERR_NOT_CONVERGED;
+}
+
+// Y = alpha * A X for nrhs row-major columns (generic CSR product, FP64).
+__global__ void csr_spmv_multi_kernel(int32_t n, int nrhs, const int32_t *rowptr,
+                                      const int32_t *col, const double *A, const double *X,
+                                      double *Y, double alpha) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < int64_t(n) * nrhs;
+       idx += stride) {
+    const int row = int(idx / nrhs), j = int(idx % nrhs);
+    double acc = 0.0;
+    for (int p = rowptr[row]; p < rowptr[row + 1]; ++p)
+      acc = fma(A[p], X[size_t(col[p]) * nrhs + j], acc);
+    Y[idx] = alpha * acc;
+  }
+}
+
+extern "C" int qd_csr_spmv(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_col,
+                           const double *d_A, const double *d_X, double *d_Y, double alpha,
+                           void *stream) {
+  if (n < 0 || nrhs < 1 || !d_rowptr || !d_col || !d_A || !d_X || !d_Y) return QD_ERR_INVALID;
+  if (n == 0) return QD_OK;
+  const int64_t total = int64_t(n) * nrhs;
+  const int blocks = int(std::min<int64_t>((total + 255) / 256, 148 * 16));
+  csr_spmv_multi_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, nrhs, d_rowptr, d_col, d_A, d_X, d_Y, alpha);
+  QD_CHECK_LAUNCH();
+  return QD_OK;
 }
