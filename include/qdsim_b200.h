@@ -203,6 +203,31 @@ int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_
                  double tol, int max_iter, int32_t *h_iters, double *h_relres,
                  void *d_work, size_t work_bytes, void *stream);
 
+/* Jacobi-PCG without a caller workspace.  No counterpart in the reference.
+ *
+ * Same arguments, results and status codes as qd_pcg_solve, minus the
+ * workspace: the scratch vectors live in a 16 MiB array that the library
+ * reserves on every GPU it is loaded on, for the life of the process.  It is
+ * for callers that cannot allocate device memory themselves -- code that runs
+ * where no allocator is available or allowed (for example a solver step
+ * embedded in another runtime that owns all device memory, or a loop that must
+ * not call cudaMalloc between launches).  This call allocates nothing.
+ *   - Size limit: the layout qd_pcg_workspace_size(n, nrhs) reports must fit
+ *     in qd_pcg_static_scratch_bytes() (16 MiB, roughly n * nrhs <= 400k);
+ *     larger problems return QD_ERR_LIMIT without launching anything.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress, with that device current); make that first call
+ *     before any stream capture.
+ *   - All calls share the one array and it keeps the previous call's
+ *     contents; every scratch word is rewritten before it is read, so nothing
+ *     needs clearing, but calls that overlap on the GPU (other streams, other
+ *     host threads) race on it and must be serialised by the caller. */
+size_t qd_pcg_static_scratch_bytes(void);
+int qd_pcg_solve_static(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_col,
+                        const double *d_A, const double *d_B, double *d_X,
+                        const int32_t *d_fixed, double tol, int max_iter, int32_t *h_iters,
+                        double *h_relres, void *stream);
+
 /* Y = alpha A X for nrhs row-major columns (generic FP64 CSR product).  Used
  * for the Poisson right-hand side M (-rho), which
  * qdsim_cython/solvers/poisson_solver.pyx:254-274 forms as mass_matrix.dot(rhs). */

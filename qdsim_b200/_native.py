@@ -53,6 +53,8 @@ SIGNATURES = {
     "qd_pcg_workspace_size": (_int, [_i32, _int, _p]),
     "qd_pcg_solve": (_int, [_i32, _int, _p, _p, _p, _p, _p, _p, _dbl, _int, _p, _p,
                             _p, _sz, _p]),
+    "qd_pcg_static_scratch_bytes": (_sz, []),
+    "qd_pcg_solve_static": (_int, [_i32, _int, _p, _p, _p, _p, _p, _p, _dbl, _int, _p, _p, _p]),
     "qd_csr_spmv": (_int, [_i32, _int, _p, _p, _p, _p, _p, _dbl, _p]),
     "qd_prof_enable": (_int, [_int]),
     "qd_prof_read": (_int, [_p, _p, _int]),

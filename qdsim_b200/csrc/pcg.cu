@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 #include "common.h"
 
@@ -300,4 +301,108 @@ extern "C" int qd_csr_spmv(int32_t n, int nrhs, const int32_t *d_rowptr, const i
       n, nrhs, d_rowptr, d_col, d_A, d_X, d_Y, alpha);
   QD_CHECK_LAUNCH();
   return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// PCG with library-owned scratch, for callers that cannot allocate device
+// memory themselves (see qd_pcg_solve_static in qdsim_b200.h).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;   // 16 MiB per device
+
+// Every GPU that loads the library reserves this array until the process exits.
+static __device__ __align__(256) unsigned char g_pcg_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mu;
+void *g_static_ptr[64] = {nullptr};
+
+// Device address of g_pcg_scratch on the current device.  In host code the
+// symbol is only a host-side stand-in, so the address must be looked up with
+// cudaGetSymbolAddress, once per device, with that device current.
+int static_scratch(void **out) {
+  int dev = 0;
+  QD_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return QD_ERR_LIMIT;
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void *p = nullptr;
+    QD_CUDA_TRY(cudaGetSymbolAddress(&p, g_pcg_scratch));
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return QD_OK;
+}
+
+}  // namespace
+
+extern "C" size_t qd_pcg_static_scratch_bytes(void) { return kStaticScratchBytes; }
+
+extern "C" int qd_pcg_solve_static(int32_t n, int nrhs, const int32_t *d_rowptr,
+                                   const int32_t *d_col, const double *d_A, const double *d_B,
+                                   double *d_X, const int32_t *d_fixed, double tol, int max_iter,
+                                   int32_t *h_iters, double *h_relres, void *stream) {
+  if (n <= 0 || nrhs < 1 || nrhs > kMaxRhs || !d_rowptr || !d_col || !d_A || !d_B || !d_X ||
+      !(tol > 0.0) || max_iter < 1)
+    return QD_ERR_INVALID;
+  Cfg c = make_cfg(n, nrhs);
+  {
+    qd::Arena need(nullptr, 0);
+    PcgLayout t;
+    carve(need, c, t);
+    if (need.used > kStaticScratchBytes) return QD_ERR_LIMIT;
+  }
+  void *scratch = nullptr;
+  int st = static_scratch(&scratch);
+  if (st != QD_OK) return st;
+  qd::Arena ar(scratch, kStaticScratchBytes);
+  PcgLayout L;
+  carve(ar, c, L);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t smem = size_t(c.threads) * sizeof(double);
+  // Every scratch word (residual, search direction, partial sums, step scalars
+  // and the done flag) is written before it is read in this call, so the
+  // contents left by an earlier call need no clearing.
+  pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
+                                                    L.R, L.Z, L.P, L.dinv, L.part);
+  QD_CHECK_LAUNCH();
+  pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
+  QD_CHECK_LAUNCH();
+  int it = 0, done = 0;
+  for (it = 0; it < max_iter; ++it) {
+    pcg_spmv_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_fixed, L.P,
+                                                      L.AP, L.done, L.part);
+    QD_CHECK_LAUNCH();
+    pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
+    QD_CHECK_LAUNCH();
+    pcg_axpy_kernel<<<c.blocks, c.threads, smem, s>>>(c, L.sc, L.dinv, d_X, L.R, L.Z, L.P, L.AP,
+                                                      L.done, L.part);
+    QD_CHECK_LAUNCH();
+    pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
+    QD_CHECK_LAUNCH();
+    pcg_dir_kernel<<<c.blocks, c.threads, 0, s>>>(c, L.sc, L.Z, L.P, L.done);
+    QD_CHECK_LAUNCH();
+    if ((it + 1) % 16 == 0 || it + 1 == max_iter) {
+      QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
+      QD_CUDA_TRY(cudaStreamSynchronize(s));
+      if (done) {
+        ++it;
+        break;
+      }
+    }
+  }
+  double sc[kMaxRhs * 5];
+  QD_CUDA_TRY(cudaMemcpyAsync(sc, L.sc, size_t(c.nrhs) * 5 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QD_CUDA_TRY(cudaStreamSynchronize(s));
+  double worst = 0.0;
+  for (int j = 0; j < c.nrhs; ++j) {
+    const double rr0 = sc[size_t(j) * 5 + 1], rr = sc[size_t(j) * 5 + 4];
+    worst = std::max(worst, rr0 > 0.0 ? std::sqrt(rr / rr0) : 0.0);
+  }
+  if (h_iters) *h_iters = it;
+  if (h_relres) *h_relres = worst;
+  return done ? QD_OK : QD_ERR_NOT_CONVERGED;
 }
