@@ -38,14 +38,15 @@ def dirichlet_mask(mesh):
     return left, right
 
 
-def solve(mesh, eps_r_elem, rho_nodal, V_p, V_n):
-    """phi (V) at every node.  rho_nodal in C/m^3 ([N] or [N, nrhs])."""
+def solve(mesh, eps_r_elem, rho_nodal, V_p, V_n, length_scale=1e-9):
+    """phi (V) at every node.  rho_nodal in C/m^3 ([N] or [N, nrhs]);
+    ``length_scale`` is the mesh unit in metres (1e-9 for nm, 1 for SI)."""
     K, M = assemble(mesh, eps_r_elem)
     rho = np.asarray(rho_nodal, float)
     one = rho.ndim == 1
     rho = rho.reshape(mesh.num_nodes, -1)
-    # K_r phi = (1e-18 / eps0) M_nm (-rho)
-    b = (1e-18 / EPS0) * (M @ (-rho))
+    # K_r phi = (l^2 / eps0) M (-rho), M in mesh units^2
+    b = (length_scale ** 2 / EPS0) * (M @ (-rho))
     left, right = dirichlet_mask(mesh)
     fixed = left | right
     vp = np.broadcast_to(np.asarray(V_p, float), (rho.shape[1],))

@@ -1,0 +1,94 @@
+"""libqdsim_b200.so loads, exports every entry point include/qdsim_b200.h
+declares, and validates arguments on the host (no GPU compute here)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "qdsim_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(qd_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_all_declared_symbols():
+    from qdsim_b200 import _native as N
+    L = N.lib()
+    names = _declared()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(L, name), name
+        assert name in N.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_status_strings_and_version():
+    from qdsim_b200 import _native as N
+    L = N.lib()
+    assert b"sm_100a" in L.qd_version()
+    for st in (0, -1, -2, -3, -4, -5, -6, -7):
+        assert L.qd_status_string(st) and L.qd_status_string(st) != b"unknown status"
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    from qdsim_b200 import _native as N
+    L = N.lib()
+    assert L.qd_assemble(4, 0, 10, 10, 5, *([None] * 16)) == N.QD_ERR_INVALID
+    assert L.qd_assemble(2, N.QD_ASM_REF_FIXED, 10, 10, 5, *([None] * 16)) == N.QD_ERR_INVALID
+    out = C.c_size_t()
+    assert L.qd_lobpcg_workspace_size(1, 100, 3, 0, None, C.byref(out)) == N.QD_ERR_INVALID
+    assert L.qd_lobpcg_workspace_size(1, 100, 12, 0, None, C.byref(out)) == N.QD_OK
+    assert out.value > 9 * 100 * 12 * 8
+    assert L.qd_pcg_workspace_size(100, 300, C.byref(out)) == N.QD_ERR_INVALID
+    ro = np.array([0, 5], np.int32)
+    info = np.zeros(4, np.int32)
+    # n must exceed the block size
+    assert L.qd_lobpcg_solve(1, N.ptr(ro), None, *([C.c_void_p(8)] * 4), None, None, 4, 8, 0,
+                             1e-9, 10, 1, *([C.c_void_p(8)] * 4), N.ptr(info), None,
+                             C.c_void_p(256), 1 << 20, None) == N.QD_ERR_INVALID
+    assert L.qd_pcg_solve_static(0, 1, *([None] * 6), 1e-9, 10, None, None, None) == N.QD_ERR_INVALID
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_pattern_builder_matches_oracle(order):
+    from oracle import fem as O
+    from qdsim_b200 import fem as F, mesh as Mh
+    for nx, ny, dirichlet in ((5, 4, True), (9, 3, False), (1, 1, False)):
+        m = Mh.StructuredMesh(order, nx, ny, float(nx), float(ny))
+        om = O.structured_mesh(order, nx, ny, float(nx), float(ny))
+        dm, n = F.dof_map_for(m, dirichlet)
+        if n == 0:
+            continue
+        P = F.build_pattern(m.elems, dm, n, m.num_nodes)
+        ip, ind, slot = O.csr_pattern(om.elems, O.dof_map(om, dirichlet), n)
+        assert np.array_equal(P.rowptr, ip) and np.array_equal(P.col, ind)
+        assert P.cptr[-1] == (slot >= 0).sum() == P.slotcnt.sum()
+        # every row's contribution list covers each of its slots
+        for r in range(0, n, max(1, n // 7)):
+            L = P.rowptr[r + 1] - P.rowptr[r]
+            assert (P.slotcnt[P.rowptr[r]:P.rowptr[r + 1]] > 0).all() and L > 0
+
+
+def test_pattern_builder_rejects_bad_input():
+    from qdsim_b200 import _native as N
+    L = N.lib()
+    elems = np.array([[0, 1, 7]], np.int32)      # node 7 out of range
+    dm = np.arange(3, dtype=np.int32)
+    nnz = C.c_int64()
+    st = L.qd_pattern_build(3, 1, 3, N.ptr(elems), N.ptr(dm), 3, C.byref(nnz), None, None,
+                            *([None] * 7))
+    assert st == N.QD_ERR_INVALID
+
+
+def test_node_adjacency_counts():
+    from qdsim_b200 import fem as F, mesh as Mh
+    m = Mh.StructuredMesh(2, 4, 3, 4.0, 3.0)
+    ptr, adj = F.node_adjacency(m.elems, m.num_nodes)
+    assert ptr[-1] == m.elems.size
+    for g in (0, 5, m.num_nodes // 2):
+        for packed in adj[ptr[g]:ptr[g + 1]]:
+            assert m.elems[packed >> 4, packed & 15] == g
