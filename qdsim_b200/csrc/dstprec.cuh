@@ -24,12 +24,18 @@ struct GemmTile {
   int dot, m0, n0, pad;
 };
 
-constexpr int kGemmTile = 64;
+constexpr int kGemmTile = 64;     // rows (M) per tile
+constexpr int kGemmTileN = 64;    // columns (N) per tile
 constexpr int kGemmK = 16;
 
 // out(r, n) = sum_k S[r][k] in(k, n)  (then / lambda when SCALE)
 // x pass: r = ix, n = iy*B + b,  addr = base + (n / B) * nx*B + r*B + n % B
 // y pass: r = iy, n = ix*B + b,  addr = base + r * nx*B + n
+// 256 threads, each owns a 4 (rows) x 4 (columns) block of the 64 x 64 tile
+// (small tiles keep the GPU busy when only a few large dots are still iterating).
+// S is symmetric, so the A tile is read as S[k][r]: coalesced loads and
+// conflict-free shared stores.  The next k-slice is prefetched into registers
+// while the current one is multiplied.
 template <typename TC, typename TI, typename TO, bool YPASS, bool SCALE>
 __global__ void __launch_bounds__(256)
 dst_gemm_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active,
@@ -44,13 +50,12 @@ dst_gemm_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ acti
   const int ncols = YPASS ? nx * B : ny * B;
   const double *S = mats + (YPASS ? d.sy_off : d.sx_off);
   const size_t base = size_t(row_off[t.dot]) * B;
-  const int ldrow = YPASS ? nx * B : B;
   auto addr = [&](int r, int n) -> size_t {
-    if (YPASS) return base + size_t(r) * ldrow + n;
+    if (YPASS) return base + size_t(r) * (size_t(nx) * B) + n;
     return base + size_t(n / B) * (size_t(nx) * B) + size_t(r) * B + (n % B);
   };
-  __shared__ TC As[kGemmK][kGemmTile + 4];
-  __shared__ TC Bs[kGemmK][kGemmTile + 4];
+  __shared__ __align__(16) TC As[kGemmK][kGemmTile + 4];
+  __shared__ __align__(16) TC Bs[kGemmK][kGemmTileN + 4];
   const int tid = threadIdx.x;
   const int ty = tid / 16, tx = tid % 16;
   TC acc[4][4];
@@ -58,20 +63,38 @@ dst_gemm_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ acti
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = TC(0);
+  // per-thread load slots: A 4 elements (1024 / 256), B 4 elements (1024 / 256)
+  TC ra[4], rb[4];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;
+      const int kk = e / kGemmTile, mm = e % kGemmTile;
+      const int gk = k0 + kk, gm = t.m0 + mm;
+      ra[q] = (gk < dim && gm < dim) ? TC(__ldg(S + size_t(gk) * dim + gm)) : TC(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;
+      const int kk = e / kGemmTileN, nn = e % kGemmTileN;
+      const int gk = k0 + kk, gn = t.n0 + nn;
+      rb[q] = (gk < dim && gn < ncols) ? TC(in[addr(gk, gn)]) : TC(0);
+    }
+  };
+  fetch(0);
   for (int k0 = 0; k0 < dim; k0 += kGemmK) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;          // 0..1023
-      // S tile: rows m0..m0+63, cols k0..k0+15  -> As[k][m]
-      const int am = e / kGemmK, ak = e % kGemmK;
-      const int gm = t.m0 + am, gk = k0 + ak;
-      As[ak][am] = (gm < dim && gk < dim) ? TC(__ldg(S + size_t(gm) * dim + gk)) : TC(0);
-      // data tile: rows k0..k0+15, cols n0..n0+63 -> Bs[k][n]
-      const int bk = e / kGemmTile, bn = e % kGemmTile;
-      const int gk2 = k0 + bk, gn = t.n0 + bn;
-      Bs[bk][bn] = (gk2 < dim && gn < ncols) ? TC(in[addr(gk2, gn)]) : TC(0);
+      const int e = tid + q * 256;
+      As[e / kGemmTile][e % kGemmTile] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;
+      Bs[e / kGemmTileN][e % kGemmTileN] = rb[q];
     }
     __syncthreads();
+    if (k0 + kGemmK < dim) fetch(k0 + kGemmK);
 #pragma unroll
     for (int kk = 0; kk < kGemmK; ++kk) {
       TC a[4], b[4];
@@ -86,24 +109,42 @@ dst_gemm_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ acti
     }
     __syncthreads();
   }
+  if (SCALE) {
+    // eigenvalue tables for this tile: rows ky = m0.., columns kx = n0/B..
+    __shared__ double s_sy[kGemmTile];
+    __shared__ double s_sx[kGemmTileN / 4 + 2];
+    const int kx0 = t.n0 / B;
+    const int nkx = (t.n0 + kGemmTileN - 1) / B - kx0 + 1;
+    if (tid < kGemmTile) {
+      const double v = sinpi(double(t.m0 + tid + 1) / double(2 * (ny + 1)));
+      s_sy[tid] = double(d.cy) * 4.0 * v * v;
+    } else if (tid - kGemmTile < nkx) {
+      const double v = sinpi(double(kx0 + tid - kGemmTile + 1) / double(2 * (nx + 1)));
+      s_sx[tid - kGemmTile] = double(d.cx) * 4.0 * v * v;
+    }
+    __syncthreads();
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = t.m0 + ty * 4 + i;
-    if (r >= dim) continue;
+    for (int i = 0; i < 4; ++i) {
+      const int r = t.m0 + ty * 4 + i;
+      if (r >= dim) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = t.n0 + tx * 4 + j;
-      if (n >= ncols) continue;
-      TC v = acc[i][j];
-      if (SCALE) {
-        // y pass: r = ky, n = kx*B + b
-        const int kx = n / B;
-        const double sx = sinpi(double(kx + 1) / double(2 * (nx + 1)));
-        const double sy = sinpi(double(r + 1) / double(2 * (ny + 1)));
-        v = TC(double(v) / (double(d.cx) * 4.0 * sx * sx + double(d.cy) * 4.0 * sy * sy +
-                            double(d.shift)));
+      for (int j = 0; j < 4; ++j) {
+        const int n = t.n0 + tx * 4 + j;
+        if (n >= ncols) continue;
+        const double lam = s_sy[ty * 4 + i] + s_sx[n / B - kx0] + double(d.shift);
+        out[addr(r, n)] = TO(double(acc[i][j]) / lam);
       }
-      out[addr(r, n)] = TO(v);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = t.m0 + ty * 4 + i;
+      if (r >= dim) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int n = t.n0 + tx * 4 + j;
+        if (n < ncols) out[addr(r, n)] = TO(acc[i][j]);
+      }
     }
   }
 }
@@ -116,12 +157,12 @@ inline void dst_tiles(int n_dots, const qd_dst_prec *h, int B, GemmTile *tx, int
     const int nx = h[d].nx, ny = h[d].ny;
     if (nx <= 0 || ny <= 0) continue;
     for (int m0 = 0; m0 < nx; m0 += kGemmTile)
-      for (int n0 = 0; n0 < ny * B; n0 += kGemmTile) {
+      for (int n0 = 0; n0 < ny * B; n0 += kGemmTileN) {
         if (tx) tx[a] = GemmTile{d, m0, n0, 0};
         ++a;
       }
     for (int m0 = 0; m0 < ny; m0 += kGemmTile)
-      for (int n0 = 0; n0 < nx * B; n0 += kGemmTile) {
+      for (int n0 = 0; n0 < nx * B; n0 += kGemmTileN) {
         if (ty) ty[b] = GemmTile{d, m0, n0, 0};
         ++b;
       }

@@ -42,7 +42,7 @@
 
 namespace {
 
-constexpr int kChunkRows = 2048;
+constexpr int kChunkRows = 1024;
 constexpr int kMaxB = 16;
 constexpr int kMaxM = 3 * kMaxB;
 constexpr int kStagWindow = 30;     // FP32 iterations without halving the estimate
@@ -232,65 +232,73 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 template <int B> struct GramCfg {
   static constexpr int m = 3 * B;
   static constexpr int NB = m / 4;
-  static constexpr int NBLK = NB * NB;
-  static constexpr int RG = (256 / NBLK) > 0 ? (256 / NBLK) : 1;
-  static constexpr int SUB = 32;
-  static constexpr int THREADS = ((NBLK * RG + 31) / 32) * 32;
+  static constexpr int NT = NB * (NB + 1) / 2;            // upper-triangle 4x4 blocks
+  static constexpr int RG = (256 / NT) > 0 ? (256 / NT) : 1;
+  static constexpr int THREADS = ((NT * RG + 31) / 32) * 32;
 };
 
+// Each thread owns one upper-triangle 4x4 block (bi <= bj) of both S^T HS and
+// S^T MS for a slice of the sub-tile's rows; the 9 vector blocks of a 64-row
+// sub-tile are staged in shared memory with 16-byte loads.  Off-diagonal
+// blocks are written to both (bi, bj) and (bj, bi), so the per-chunk partial
+// holds the full symmetric matrices.
 template <typename TV, int B>
 __global__ void __launch_bounds__(GramCfg<B>::THREADS)
 gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, const TV *P,
             const TV *HX, const TV *HW, const TV *HP, const TV *MX, const TV *MW, const TV *MP,
             double *partial) {
   using C = GramCfg<B>;
-  constexpr int m = C::m, NB = C::NB, NBLK = C::NBLK, RG = C::RG, SUB = C::SUB;
-  constexpr int STAGE_BYTES = 3 * SUB * m * int(sizeof(TV));
-  constexpr int RED_BYTES = (RG > 1) ? NBLK * 32 * 8 : 8;
+  constexpr int m = C::m, NB = C::NB, NT = C::NT, RG = C::RG;
+  constexpr int SUB = sizeof(TV) == 8 ? 32 : 64;              // rows staged per sub-tile
+  constexpr int LD = m + 4;                                   // padded row (elements)
+  constexpr int STAGE_BYTES = 3 * SUB * LD * int(sizeof(TV));
+  constexpr int RED_BYTES = (RG > 1) ? NT * 32 * 8 : 8;
   constexpr int RAW = STAGE_BYTES > RED_BYTES ? STAGE_BYTES : RED_BYTES;
   __shared__ __align__(16) unsigned char raw[RAW];
   TV *sS = reinterpret_cast<TV *>(raw);
-  TV *sH = sS + SUB * m;
-  TV *sM = sH + SUB * m;
+  TV *sH = sS + SUB * LD;
+  TV *sM = sH + SUB * LD;
 
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].active) return;
   const int tid = threadIdx.x;
   if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
     const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][1]++;
-  const bool worker = tid < NBLK * RG;
-  const int blk = tid % NBLK, rg = tid / NBLK;
-  const int bi = blk / NB, bj = blk % NB;
+  const bool worker = tid < NT * RG;
+  const int task = tid % NT, rg = tid / NT;
+  // task -> (bi, bj) with bi <= bj
+  int bi = 0, rem = task;
+  while (rem >= NB - bi) {
+    rem -= NB - bi;
+    ++bi;
+  }
+  const int bj = bi + rem;
   double aH[4][4], aM[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) aH[a][b] = aM[a][b] = 0.0;
 
-  const TV *srcS[3] = {X, W, P};
-  const TV *srcH[3] = {HX, HW, HP};
-  const TV *srcM[3] = {MX, MW, MP};
+  const TV *srcs[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
+  constexpr int VEC = 16 / int(sizeof(TV));                  // elements per 16-byte load
   for (int r0 = ch.begin; r0 < ch.end; r0 += SUB) {
     const int nr = min(SUB, ch.end - r0);
-    for (int idx = tid; idx < SUB * m; idx += blockDim.x) {
-      const int row = idx / m, c = idx % m;
-      const int blkc = c / B, cc = c % B;
-      TV s = TV(0), h = TV(0), mm = TV(0);
-      if (row < nr) {
-        const size_t o = size_t(r0 + row) * B + cc;
-        s = srcS[blkc][o];
-        h = srcH[blkc][o];
-        mm = srcM[blkc][o];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      TV *dst = (a < 3 ? sS : a < 6 ? sH : sM) + (a % 3) * B;
+      const TV *src = srcs[a] + size_t(r0) * B;
+      for (int v = tid; v < SUB * B / VEC; v += blockDim.x) {
+        const int e = v * VEC, row = e / B, col = e % B;   // B % VEC == 0
+        if (row < nr) {
+          const float4 q = *reinterpret_cast<const float4 *>(src + e);
+          *reinterpret_cast<float4 *>(dst + row * LD + col) = q;
+        } else {
+          *reinterpret_cast<float4 *>(dst + row * LD + col) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
       }
-      sS[idx] = s;
-      sH[idx] = h;
-      sM[idx] = mm;
     }
     __syncthreads();
     if (worker) {
-      // products in the storage precision, summed over this sub-tile, then
-      // added into FP64 accumulators (FP32: exact products are not needed in
-      // the FP32 phase; the FP64 phase runs this with TV = double).
       TV tH[4][4], tM[4][4];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
@@ -300,9 +308,9 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
         TV sa[4], hb[4], mb[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          sa[a] = sS[row * m + 4 * bi + a];
-          hb[a] = sH[row * m + 4 * bj + a];
-          mb[a] = sM[row * m + 4 * bj + a];
+          sa[a] = sS[row * LD + 4 * bi + a];
+          hb[a] = sH[row * LD + 4 * bj + a];
+          mb[a] = sM[row * LD + 4 * bj + a];
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a)
@@ -331,8 +339,8 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
         for (int a = 0; a < 4; ++a)
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
-            red[blk * 32 + a * 4 + b] = aH[a][b];
-            red[blk * 32 + 16 + a * 4 + b] = aM[a][b];
+            red[task * 32 + a * 4 + b] = aH[a][b];
+            red[task * 32 + 16 + a * 4 + b] = aM[a][b];
           }
       }
       __syncthreads();
@@ -341,8 +349,8 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
         for (int a = 0; a < 4; ++a)
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
-            aH[a][b] += red[blk * 32 + a * 4 + b];
-            aM[a][b] += red[blk * 32 + 16 + a * 4 + b];
+            aH[a][b] += red[task * 32 + a * 4 + b];
+            aM[a][b] += red[task * 32 + 16 + a * 4 + b];
           }
       }
       __syncthreads();
@@ -356,6 +364,10 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
         const int i = 4 * bi + a, j = 4 * bj + b;
         out[i * m + j] = aH[a][b];
         out[m * m + i * m + j] = aM[a][b];
+        if (bi != bj) {
+          out[j * m + i] = aH[a][b];
+          out[m * m + j * m + i] = aM[a][b];
+        }
       }
   }
 }
@@ -1271,7 +1283,7 @@ extern "C" int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32, const int32_t *
 
 extern "C" int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int b,
                                              const qd_dst_prec *h_prec, size_t *bytes) {
-  if (n_dots <= 0 || !h_row_off || !h_prec || !bytes || b < 1) return QD_ERR_INVALID;
+  if (n_dots <= 0 || !h_row_off || !h_prec || !bytes || b < 4) return QD_ERR_INVALID;
   int64_t ntx = 0, nty = 0;
   qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);
@@ -1289,7 +1301,7 @@ extern "C" int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, in
                                     const qd_dst_prec *h_prec, const double *d_prec_mats,
                                     const void *d_in, void *d_out, void *d_work,
                                     size_t work_bytes, void *stream) {
-  if (n_dots <= 0 || !h_row_off || !h_prec || !d_prec_mats || !d_in || !d_out || !d_work || b < 1)
+  if (n_dots <= 0 || !h_row_off || !h_prec || !d_prec_mats || !d_in || !d_out || !d_work || b < 4)
     return QD_ERR_INVALID;
   for (int d = 0; d < n_dots; ++d) {
     const qd_dst_prec &q = h_prec[d];

@@ -95,14 +95,23 @@ class FEMProblem:
     mask for inhomogeneous Dirichlet values instead).
     """
 
-    def __init__(self, mesh: StructuredMesh, dirichlet: bool = True, device="cuda"):
+    def __init__(self, mesh: StructuredMesh, dirichlet: bool = True, device="cuda",
+                 eliminate=None):
+        """``eliminate`` (bool per node) overrides ``dirichlet`` with an explicit
+        set of eliminated nodes."""
         self.mesh = mesh
         self.order = mesh.order
         self.device = torch.device(device)
-        self.dof_map, self.n = dof_map_for(mesh, dirichlet)
         key = None
-        if isinstance(mesh, StructuredMesh):
-            key = (mesh.shape_key(), dirichlet)
+        if eliminate is not None:
+            keep = ~np.asarray(eliminate, bool)
+            self.dof_map = np.full(mesh.num_nodes, -1, dtype=np.int32)
+            self.dof_map[keep] = np.arange(int(keep.sum()), dtype=np.int32)
+            self.n = int(keep.sum())
+        else:
+            self.dof_map, self.n = dof_map_for(mesh, dirichlet)
+            if isinstance(mesh, StructuredMesh):
+                key = (mesh.shape_key(), dirichlet)
         if key is not None and key in _PATTERN_CACHE:
             self.pattern = _PATTERN_CACHE[key]
         else:
