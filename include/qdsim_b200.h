@@ -46,7 +46,7 @@ enum {
 /* eigensolver precision modes */
 enum {
   QD_PREC_FP64 = 0,           /* FP64 vectors throughout (the plain form)         */
-  QD_PREC_MIXED = 1           /* FP32 vector phase, then FP64 finishing phase     */
+  QD_PREC_MIXED = 1           /* per dot: FP32 vector phase, then FP64 finishing  */
 };
 
 const char *qd_version(void);
@@ -154,8 +154,8 @@ typedef struct {
  *                M-orthonormal per dot
  *   d_E_out      double[n_dots * k]; d_res_out double[n_dots * k] relative
  *                residuals ||r|| / (|t| ||Mx||); d_iters_out int32[n_dots] (FP32 + FP64 iterations)
- *   h_info       int32[4] (host): total iterations, FP32 iterations, FP64
- *                iterations, number of converged dots
+ *   h_info       int32[4] (host): host iterations, largest FP32 and FP64
+ *                iteration counts of any dot, number of converged dots
  *   h_counts     int32[n_dots*6] (host, may be NULL): per dot, the launches of
  *                SpMM, Gram and update that did work in the FP32 and the FP64
  *                phase (for algorithmic-byte accounting)

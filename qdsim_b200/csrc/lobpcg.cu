@@ -54,14 +54,14 @@ constexpr double kRelCap = 1e-2;
 #endif
 #ifndef QD_SVQB_TAU32
 #define QD_SVQB_TAU32 1e-6
-#endif     // never stop while the relative residual exceeds this
+#endif
 
 struct Chunk {
   int dot, begin, end, pad;
 };
 
 struct DotState {
-  int active;       // iterating in the current phase
+  int active;       // still iterating (either precision)
   int has_p;        // P block is populated
   int iters;        // total iterations (all phases)
   int iters_phase;  // iterations in the current phase
@@ -72,7 +72,9 @@ struct DotState {
   int chunk0, chunk1;
   double best;      // best max relative residual in this phase
   int launches[2][3];   // [FP32, FP64 phase][spmm, gram, update] launches that did work
-  int pad2;
+  int run[2];       // iterating in the FP32 / FP64 phase (kernels of that precision work)
+  int phase;        // 0 FP32, 1 FP64
+  int switching;    // left the FP32 phase this iteration; X still to be converted
 };
 
 // ---------------------------------------------------------------------------
@@ -102,24 +104,6 @@ __global__ void init_kernel(const Chunk *chunks, const int32_t *row_off, uint64_
 }
 
 template <typename TV, int B>
-__global__ void zero_aux_kernel(const Chunk *chunks, TV *W, TV *P, TV *HW, TV *MW, TV *HP, TV *MP) {
-  const Chunk ch = chunks[blockIdx.x];
-  for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
-    const size_t o = size_t(ch.begin) * B + idx;
-    W[o] = P[o] = HW[o] = MW[o] = HP[o] = MP[o] = TV(0);
-  }
-}
-
-template <int B>
-__global__ void convert_kernel(const Chunk *chunks, const float *X32, double *X64) {
-  const Chunk ch = chunks[blockIdx.x];
-  for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
-    const size_t o = size_t(ch.begin) * B + idx;
-    X64[o] = double(X32[o]);
-  }
-}
-
-template <typename TV, int B>
 __global__ void spmm_chunk_kernel(const Chunk *chunks, const DotState *st,
                                   const int32_t *__restrict__ rowptr,
                                   const int32_t *__restrict__ col, const double *__restrict__ H,
@@ -127,7 +111,7 @@ __global__ void spmm_chunk_kernel(const Chunk *chunks, const DotState *st,
                                   TV *__restrict__ HX, TV *__restrict__ MX) {
   constexpr int G = B / 4;
   const Chunk ch = chunks[blockIdx.x];
-  if (!st[ch.dot].active) return;
+  if (!st[ch.dot].run[sizeof(TV) == 8]) return;
   if (threadIdx.x == 0 && blockIdx.x == st[ch.dot].chunk0)
     const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][0]++;
   const int sub = threadIdx.x / G, g = threadIdx.x % G;
@@ -154,7 +138,7 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   __shared__ double s_red[RPP * G2 * 8];
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
-  if (!sd.active) return;
+  if (!sd.run[sizeof(TV) == 8]) return;
   const bool with_p = sd.has_p != 0;
   if (threadIdx.x == 0 && blockIdx.x == sd.chunk0)
     const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][0]++;
@@ -260,7 +244,7 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
   TV *sM = sH + SUB * LD;
 
   const Chunk ch = chunks[blockIdx.x];
-  if (!st[ch.dot].active) return;
+  if (!st[ch.dot].run[sizeof(TV) == 8]) return;
   const int tid = threadIdx.x;
   if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
     const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][1]++;
@@ -378,7 +362,7 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
 
 struct RRParams {
   int k;
-  int phase32;     // 1: FP32 phase (stagnation allowed, scaled residual)
+  double tol32;    // FP32-phase target (then the dot switches to FP64)
   double tol;      // relative residual tolerance for this phase
   int max_iter;    // total iteration cap per dot
 };
@@ -400,9 +384,11 @@ __device__ inline double cta_sum(double v, double *s_red) {
 // Cyclic Jacobi eigensolver for a symmetric n x n matrix A (leading dimension
 // ld, shared memory) with round-robin pairing; V (ld) receives the
 // eigenvectors as columns, A's diagonal the eigenvalues.  A pair is rotated
-// only while |a_pq| > eps sqrt(|a_pp a_qq|) (the relative threshold of
+// only while |a_pq| > 2e-15 sqrt(|a_pp a_qq|) (the relative threshold of
 // Demmel and Veselic), so tiny eigenvalues of a scaled SPD Gram matrix come out
-// with high relative accuracy; the sweeps stop when a sweep rotates nothing.
+// with high relative accuracy, and |a_pq| > 1e-18 ||A||_F (below that the
+// entry is rounding noise and rotating it only costs sweeps); the sweeps stop
+// when a sweep rotates nothing.
 // Odd n uses a dummy index that is never rotated.  All threads must call it.
 __device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, double *s_c,
                            double *s_s, int *s_p, int *s_q) {
@@ -412,7 +398,20 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, d
     const int i = idx / n, j = idx % n;
     V[i * ld + j] = (i == j) ? 1.0 : 0.0;
   }
-  (void)s_red;
+  // absolute floor: off-diagonal entries below 1e-18 ||A||_F are rounding noise
+  double fro = 0.0;
+  for (int idx = tid; idx < n * n; idx += nt) {
+    const double v = A[(idx / n) * ld + idx % n];
+    fro += v * v;
+  }
+  s_red[tid] = fro;
+  __syncthreads();
+  for (int w = nt / 2; w > 0; w >>= 1) {
+    if (tid < w) s_red[tid] += s_red[tid + w];
+    __syncthreads();
+  }
+  const double floor_abs = 1e-18 * sqrt(s_red[0]);
+  __syncthreads();
   const int ne = (n + 1) & ~1;   // even count including the dummy
   if (ne < 2) return;
   for (int sweep = 0; sweep < 60; ++sweep) {
@@ -436,7 +435,7 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, d
         if (q < n) {
           const double apq = A[p * ld + q];
           const double app = A[p * ld + p], aqq = A[q * ld + q];
-          if (fabs(apq) > 1e-300 && fabs(apq) > 1e-16 * sqrt(fabs(app * aqq))) {
+          if (fabs(apq) > floor_abs && fabs(apq) > 2e-15 * sqrt(fabs(app * aqq))) {
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = rsqrt(1.0 + t * t);
@@ -545,11 +544,12 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
         worst = fmax(worst, sR[j]);
         worst_raw = fmax(worst_raw, sE[j]);
       }
+      const bool ph32 = s.phase == 0;
       int stop = 0;
-      if (worst <= prm.tol) {
+      if (worst <= (ph32 ? prm.tol32 : prm.tol)) {
         stop = 1;
-        if (!prm.phase32) s.status = 1;
-      } else if (prm.phase32) {
+        if (!ph32) s.status = 1;
+      } else if (ph32) {
         if (worst_raw < 0.5 * s.best) {
           s.best = worst_raw;
           s.stag = 0;
@@ -559,10 +559,16 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
       }
       if (!stop && s.iters >= prm.max_iter) {
         stop = 1;
-        s.status = prm.phase32 ? 0 : 3;
+        if (!ph32) s.status = 3;
       }
       if (stop) {
-        s.active = 0;
+        if (ph32) {          // hand over to the FP64 phase
+          s.run[0] = 0;
+          s.switching = 1;
+        } else {
+          s.active = 0;
+          s.run[1] = 0;
+        }
         s_flag = 1;
       }
     }
@@ -570,15 +576,11 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     if (s_flag) return;
   }
 
-  // 2. Gram matrices summed over the dot's chunks (fixed order), symmetrised
+  // 2. Gram matrices of the dot (summed over its chunks by dot_reduce_kernel)
+  const double *gsum = partial + size_t(d) * 2 * m * m;
   for (int idx = tid; idx < m * m; idx += nt) {
-    double a = 0.0, b = 0.0;
-    for (int c = s.chunk0; c < s.chunk1; ++c) {
-      a += partial[size_t(c) * 2 * m * m + idx];
-      b += partial[size_t(c) * 2 * m * m + m * m + idx];
-    }
-    sT[idx] = a;
-    sZ[idx] = b;
+    sT[idx] = gsum[idx];
+    sZ[idx] = gsum[m * m + idx];
   }
   __syncthreads();
   const bool has_p = s.has_p != 0;
@@ -600,7 +602,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   if (tid == 0) {
     double smax = 0.0;
     for (int i = 0; i < m; ++i) smax = fmax(smax, sB[i * m + i]);
-    const double tau = prm.phase32 ? QD_SVQB_TAU32 : QD_SVQB_TAU64;
+    const double tau = s.phase == 0 ? QD_SVQB_TAU32 : QD_SVQB_TAU64;
     int r = 0;
     for (int i = 0; i < m; ++i)
       if (sB[i * m + i] > tau * smax && smax > 0.0) s_keep[r++] = i;
@@ -611,6 +613,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   if (r < B || !(r > 0)) {
     if (tid == 0) {
       s.active = 0;
+      s.run[0] = s.run[1] = 0;
       s.status = 2;
     }
     return;
@@ -679,7 +682,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     s.has_p = 1;
     s.iters++;
     s.iters_phase++;
-    if (prm.phase32) s.iters32++;
+    if (s.phase == 0) s.iters32++;
     s.have_res = 1;
   }
 }
@@ -704,7 +707,7 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
   __shared__ ACC sY[m * B];
   __shared__ TV sIn[R * 3 * B];
   const Chunk ch = chunks[blockIdx.x];
-  if (!st[ch.dot].active) return;
+  if (!st[ch.dot].run[sizeof(TV) == 8]) return;
   const int tid = threadIdx.x;
   if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
     const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][2]++;
@@ -756,7 +759,7 @@ ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const T
   __shared__ TV sM[SUB * B], sW[SUB * B], sP[SUB * B];
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
-  if (!sd.active) return;
+  if (!sd.run[sizeof(TV) == 8]) return;
   const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
   constexpr int NOUT = 2 * B * B;
@@ -795,7 +798,7 @@ ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const T
 
 template <typename TV, int B>
 __global__ void __launch_bounds__(UpdCfg<B>::THREADS)
-ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *partial, const TV *X,
+ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, const TV *X,
                    const TV *HX, const TV *MX, TV *W, TV *P, TV *HP, TV *MP) {
   constexpr int R = UpdCfg<B>::R;
   constexpr int NOUT = 2 * B * B;
@@ -803,14 +806,10 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *partia
   __shared__ TV sIn[R * 3 * B];
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
-  if (!sd.active) return;
+  if (!sd.run[sizeof(TV) == 8]) return;
   const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
-  for (int e = tid; e < NOUT; e += blockDim.x) {
-    double a = 0.0;
-    for (int c = sd.chunk0; c < sd.chunk1; ++c) a += partial[size_t(c) * NOUT + e];
-    sC[e] = TV(a);
-  }
+  for (int e = tid; e < NOUT; e += blockDim.x) sC[e] = TV(csum[size_t(ch.dot) * NOUT + e]);
   const TV *src[3] = {X, HX, MX};
   const int row = tid / B, j = tid % B;
   for (int r0 = ch.begin; r0 < ch.end; r0 += R) {
@@ -849,6 +848,28 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *partia
   }
 }
 
+// out[d][v] = sum over the chunks of dot d of partial[c * nvals + v], in chunk
+// order (deterministic).  One thread per (dot, value): the latency of the
+// chunk loop is hidden by the number of threads instead of being paid
+// serially inside one CTA per dot.
+__global__ void dot_reduce_kernel(const DotState *st, int ph, const double *__restrict__ partial,
+                                  int nvals, double *__restrict__ out) {
+  const int d = blockIdx.y;
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const DotState &sd = st[d];
+  if (!sd.run[ph] || v >= nvals) return;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int c = sd.chunk0;
+  for (; c + 3 < sd.chunk1; c += 4) {
+    a0 += partial[size_t(c) * nvals + v];
+    a1 += partial[size_t(c + 1) * nvals + v];
+    a2 += partial[size_t(c + 2) * nvals + v];
+    a3 += partial[size_t(c + 3) * nvals + v];
+  }
+  for (; c < sd.chunk1; ++c) a0 += partial[size_t(c) * nvals + v];
+  out[size_t(d) * nvals + v] = (a0 + a1) + (a2 + a3);
+}
+
 __global__ void count_active_kernel(const DotState *st, int n, int *out) {
   __shared__ int s;
   if (threadIdx.x == 0) s = 0;
@@ -860,11 +881,29 @@ __global__ void count_active_kernel(const DotState *st, int n, int *out) {
   if (threadIdx.x == 0) *out = s;
 }
 
-__global__ void phase_reset_kernel(DotState *st, int n) {
+// FP32 -> FP64 hand-over of the dots that left the FP32 phase this iteration:
+// X64 = X32 on their rows, the other FP64 blocks cleared (P restarts empty).
+template <int B>
+__global__ void transition_rows_kernel(const Chunk *chunks, const DotState *st, const float *X32,
+                                       double *X, double *W, double *P, double *HW, double *MW,
+                                       double *HP, double *MP) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!st[ch.dot].switching) return;
+  for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
+    const size_t o = size_t(ch.begin) * B + idx;
+    X[o] = double(X32[o]);
+    W[o] = P[o] = HW[o] = MW[o] = HP[o] = MP[o] = 0.0;
+  }
+}
+
+__global__ void transition_state_kernel(DotState *st, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   DotState &s = st[i];
-  s.active = (s.status != 2) ? 1 : 0;
+  if (!s.switching) return;
+  s.switching = 0;
+  s.phase = 1;
+  s.run[1] = 1;
   s.has_p = 0;
   s.have_res = 0;
   s.iters_phase = 0;
@@ -901,9 +940,10 @@ struct Layout {
   Chunk *chunks;
   int32_t *row_off;
   DotState *st;
-  double *theta, *coef, *relres, *partial, *norms;
+  double *theta, *coef, *relres, *partial, *norms, *dotsum, *gramsum;
   int *count;
-  double *slot[9];
+  double *slot[9];   // FP64 vector blocks X W P HX HW HP MX MW MP
+  float *slot32[9];  // FP32 vector blocks (mixed precision only)
   int nchunks;
   // DST preconditioner
   double *tmp1, *tmp2;   // used as float in the FP32 phase
@@ -919,7 +959,7 @@ size_t rr_smem_bytes(int B) {
 }
 
 int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t ntx,
-          int64_t nty, Layout &L) {
+          int64_t nty, bool mixed, Layout &L) {
   const int m = 3 * B;
   L.chunks = ar.take<Chunk>(nchunks);
   L.row_off = ar.take<int32_t>(n_dots + 1);
@@ -928,9 +968,12 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t
   L.coef = ar.take<double>(size_t(n_dots) * m * B);
   L.relres = ar.take<double>(size_t(n_dots) * B);
   L.partial = ar.take<double>(size_t(nchunks) * 2 * m * m);
+  L.dotsum = ar.take<double>(size_t(n_dots) * 2 * B * B);
+  L.gramsum = ar.take<double>(size_t(n_dots) * 2 * m * m);
   L.norms = ar.take<double>(size_t(nchunks) * 2 * B);
   L.count = ar.take<int>(4);
   for (int i = 0; i < 9; ++i) L.slot[i] = ar.take<double>(size_t(n_rows) * B);
+  for (int i = 0; i < 9; ++i) L.slot32[i] = mixed ? ar.take<float>(size_t(n_rows) * B) : nullptr;
   L.nchunks = nchunks;
   L.ntx = ntx;
   L.nty = nty;
@@ -958,75 +1001,118 @@ int count_chunks(int n_dots, const int32_t *row_off) {
   return int(c);
 }
 
-template <typename TV, int B>
+template <typename TV>
 struct Bufs {
   TV *X, *W, *P, *HX, *HW, *HP, *MX, *MW, *MP;
-  explicit Bufs(double *const *slot, const int *perm) {
+  template <typename S>
+  explicit Bufs(S *const *slot) {
     TV **dst[9] = {&X, &W, &P, &HX, &HW, &HP, &MX, &MW, &MP};
-    for (int i = 0; i < 9; ++i) *dst[i] = reinterpret_cast<TV *>(slot[perm[i]]);
+    for (int i = 0; i < 9; ++i) *dst[i] = reinterpret_cast<TV *>(slot[i]);
   }
 };
 
+// Everything of one iteration up to the Rayleigh-Ritz step, for the dots in
+// the phase of precision TV.
 template <typename TV, int B>
-int run_phase(const Layout &L, const int *perm, int n_dots, const int32_t *rowptr,
-              const int32_t *col, const double *H, const double *M, const RRParams &prm,
-              cudaStream_t s, int &iters_run) {
-  Bufs<TV, B> b(L.slot, perm);
+int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t *rowptr,
+                   const int32_t *col, const double *H, const double *M, cudaStream_t s) {
   constexpr int G = B / 4;
-  const int spmm_threads = 64 * G;
+  constexpr int PH = sizeof(TV) == 8 ? 1 : 0;
   using GC = GramCfg<B>;
+  qd::prof_begin(qd::PK_SPMM, s);
+  spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, H, M, L.theta,
+                                                      b.X, b.P, b.HX, b.MX, b.HP, b.MP, b.W,
+                                                      L.norms);
+  qd::prof_end(qd::PK_SPMM, s);
+  QD_CHECK_LAUNCH();
+  if (L.ntx > 0) {
+    qd::prof_begin(qd::PK_PRECOND, s);
+    cudaError_t e = qd::dst_apply<TV>(L.tiles_x, L.ntx, L.tiles_y, L.nty, &L.st[0].run[PH],
+                                      int(sizeof(DotState) / sizeof(int)), L.desc, L.row_off,
+                                      L.mats, B, b.W, b.W, reinterpret_cast<TV *>(L.tmp1),
+                                      reinterpret_cast<TV *>(L.tmp2), s);
+    qd::prof_end(qd::PK_PRECOND, s);
+    if (e != cudaSuccess) return QD_ERR_CUDA;
+  }
+  qd::prof_begin(qd::PK_ORTHO, s);
+  ortho_gram_kernel<TV, B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, b.MX, b.W, b.P, L.partial);
+  QD_CHECK_LAUNCH();
+  dot_reduce_kernel<<<dim3((2 * B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, PH, L.partial,
+                                                                         2 * B * B, L.dotsum);
+  QD_CHECK_LAUNCH();
+  ortho_apply_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(
+      L.chunks, L.st, L.dotsum, b.X, b.HX, b.MX, b.W, b.P, b.HP, b.MP);
+  qd::prof_end(qd::PK_ORTHO, s);
+  QD_CHECK_LAUNCH();
+  qd::prof_begin(qd::PK_SPMM, s);
+  spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, H, M, b.W,
+                                                        b.HW, b.MW);
+  qd::prof_end(qd::PK_SPMM, s);
+  QD_CHECK_LAUNCH();
+  qd::prof_begin(qd::PK_GRAM, s);
+  gram_kernel<TV, B><<<L.nchunks, GC::THREADS, 0, s>>>(L.chunks, L.st, b.X, b.W, b.P, b.HX, b.HW,
+                                                       b.HP, b.MX, b.MW, b.MP, L.partial);
+  QD_CHECK_LAUNCH();
+  // the Gram sums of this phase's dots land in L.dotsum; the other phase's
+  // dots are reduced by their own sequence (their partial chunks differ)
+  dot_reduce_kernel<<<dim3((2 * 9 * B * B + 255) / 256, n_dots), 256, 0, s>>>(
+      L.st, PH, L.partial, 2 * 9 * B * B, L.gramsum);
+  qd::prof_end(qd::PK_GRAM, s);
+  QD_CHECK_LAUNCH();
+  return QD_OK;
+}
+
+template <typename TV, int B>
+int update_step(const Layout &L, const Bufs<TV> &b, cudaStream_t s) {
+  qd::prof_begin(qd::PK_UPDATE, s);
+  update_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(L.chunks, L.st, L.coef, b.X, b.W,
+                                                                b.P);
+  qd::prof_end(qd::PK_UPDATE, s);
+  QD_CHECK_LAUNCH();
+  return QD_OK;
+}
+
+// The iteration loop.  In mixed precision every dot starts in the FP32 phase
+// and switches to the FP64 phase on its own (FP32 target reached, stagnation
+// or iteration cap); both phases advance in every host iteration, so a dot's
+// FP64 finish overlaps other dots' FP32 work.
+template <int B>
+int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, const int32_t *col,
+               const double *H, const double *M, const RRParams &prm, cudaStream_t s,
+               int &iters_run) {
+  Bufs<double> b64(L.slot);
   const size_t rr_smem = rr_smem_bytes(B);
   QD_CUDA_TRY(cudaFuncSetAttribute(rr_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(rr_smem)));
   int host_count = n_dots;
   iters_run = 0;
-  for (int it = 0; it < prm.max_iter + 1; ++it) {
-    // explicit H/M products of X and P, residual W = HX - MX Theta and its norms
-    qd::prof_begin(qd::PK_SPMM, s);
-    spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, H, M,
-                                                        L.theta, b.X, b.P, b.HX, b.MX, b.HP,
-                                                        b.MP, b.W, L.norms);
-    qd::prof_end(qd::PK_SPMM, s);
-    QD_CHECK_LAUNCH();
-    if (L.ntx > 0) {
-      qd::prof_begin(qd::PK_PRECOND, s);
-      cudaError_t e = qd::dst_apply<TV>(L.tiles_x, L.ntx, L.tiles_y, L.nty, &L.st[0].active,
-                                        int(sizeof(DotState) / sizeof(int)), L.desc, L.row_off,
-                                        L.mats, B, b.W, b.W, reinterpret_cast<TV *>(L.tmp1),
-                                        reinterpret_cast<TV *>(L.tmp2), s);
-      qd::prof_end(qd::PK_PRECOND, s);
-      if (e != cudaSuccess) return QD_ERR_CUDA;
+  for (int it = 0; it < prm.max_iter + 8; ++it) {
+    int st;
+    if (mixed) {
+      Bufs<float> b32(L.slot32);
+      if ((st = phase_sequence<float, B>(L, b32, n_dots, rowptr, col, H, M, s)) != QD_OK) return st;
     }
-    qd::prof_begin(qd::PK_ORTHO, s);
-    ortho_gram_kernel<TV, B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, b.MX, b.W, b.P, L.partial);
-    QD_CHECK_LAUNCH();
-    ortho_apply_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(
-        L.chunks, L.st, L.partial, b.X, b.HX, b.MX, b.W, b.P, b.HP, b.MP);
-    qd::prof_end(qd::PK_ORTHO, s);
-    QD_CHECK_LAUNCH();
-    qd::prof_begin(qd::PK_SPMM, s);
-    spmm_chunk_kernel<TV, B><<<L.nchunks, spmm_threads, 0, s>>>(L.chunks, L.st, rowptr, col, H,
-                                                                M, b.W, b.HW, b.MW);
-    qd::prof_end(qd::PK_SPMM, s);
-    QD_CHECK_LAUNCH();
-    qd::prof_begin(qd::PK_GRAM, s);
-    gram_kernel<TV, B><<<L.nchunks, GC::THREADS, 0, s>>>(L.chunks, L.st, b.X, b.W, b.P, b.HX,
-                                                         b.HW, b.HP, b.MX, b.MW, b.MP,
-                                                         L.partial);
-    qd::prof_end(qd::PK_GRAM, s);
-    QD_CHECK_LAUNCH();
+    if ((st = phase_sequence<double, B>(L, b64, n_dots, rowptr, col, H, M, s)) != QD_OK) return st;
     qd::prof_begin(qd::PK_RR, s);
-    rr_kernel<B><<<n_dots, 256, rr_smem, s>>>(L.st, L.partial, L.norms, L.theta, L.coef,
+    rr_kernel<B><<<n_dots, 256, rr_smem, s>>>(L.st, L.gramsum, L.norms, L.theta, L.coef,
                                               L.relres, prm);
     qd::prof_end(qd::PK_RR, s);
     QD_CHECK_LAUNCH();
-    qd::prof_begin(qd::PK_UPDATE, s);
-    update_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(L.chunks, L.st, L.coef, b.X,
-                                                                  b.W, b.P);
-    qd::prof_end(qd::PK_UPDATE, s);
-    QD_CHECK_LAUNCH();
+    if (mixed) {
+      Bufs<float> b32(L.slot32);
+      if ((st = update_step<float, B>(L, b32, s)) != QD_OK) return st;
+    }
+    if ((st = update_step<double, B>(L, b64, s)) != QD_OK) return st;
+    if (mixed) {
+      transition_rows_kernel<B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, L.slot32[0], b64.X,
+                                                          b64.W, b64.P, b64.HW, b64.MW, b64.HP,
+                                                          b64.MP);
+      QD_CHECK_LAUNCH();
+      transition_state_kernel<<<(n_dots + 127) / 128, 128, 0, s>>>(L.st, n_dots);
+      QD_CHECK_LAUNCH();
+    }
     ++iters_run;
-    if (it % 8 == 7 || it == prm.max_iter) {
+    if (it % 8 == 7) {
       count_active_kernel<<<1, 256, 0, s>>>(L.st, n_dots, L.count);
       QD_CHECK_LAUNCH();
       QD_CUDA_TRY(cudaMemcpyAsync(&host_count, L.count, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1061,13 +1147,13 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   {
     qd::Arena need(nullptr, 0);
     Layout tmp;
-    carve(need, n_dots, n_rows, B, nchunks, ntx, nty, tmp);
+    carve(need, n_dots, n_rows, B, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, tmp);
     if (need.used > work_bytes) return QD_ERR_WORKSPACE;
   }
   if (reinterpret_cast<uintptr_t>(d_work) % 256 != 0) return QD_ERR_WORKSPACE;
   qd::Arena ar(d_work, work_bytes);
   Layout L;
-  carve(ar, n_dots, n_rows, B, nchunks, ntx, nty, L);
+  carve(ar, n_dots, n_rows, B, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, L);
   std::vector<qd::GemmTile> htx, hty;
   if (ntx > 0) {
     htx.resize(ntx);
@@ -1089,6 +1175,8 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     DotState &x = st[d];
     std::memset(&x, 0, sizeof(x));
     x.active = 1;
+    x.phase = prec_mode == QD_PREC_MIXED ? 0 : 1;
+    x.run[x.phase] = 1;
     x.best = 1e300;
     x.chunk0 = int(chunks.size());
     for (int r = h_row_off[d]; r < h_row_off[d + 1]; r += kChunkRows)
@@ -1096,6 +1184,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     x.chunk1 = int(chunks.size());
     if (x.chunk1 == x.chunk0) {
       x.active = 0;
+      x.run[0] = x.run[1] = 0;
       x.status = 2;
     }
   }
@@ -1109,49 +1198,28 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   QD_CUDA_TRY(cudaMemsetAsync(L.relres, 0, sizeof(double) * size_t(n_dots) * B, s));
   QD_CUDA_TRY(cudaStreamSynchronize(s));   // host staging vectors die at return
 
-  const int perm0[9] = {0, 1, 2, 3, 4, 5, 6, 7, 8};
-  int it32 = 0, it64 = 0;
+  const bool mixed = prec_mode == QD_PREC_MIXED;
   RRParams prm;
   prm.k = k;
   prm.max_iter = max_iter;
-  if (prec_mode == QD_PREC_MIXED) {
-    Bufs<float, B> b(L.slot, perm0);
-    init_kernel<float, B><<<nchunks, 256, 0, s>>>(L.chunks, L.row_off, seed, b.X, b.W, b.P,
-                                                  b.HW, b.MW, b.HP, b.MP);
-    QD_CHECK_LAUNCH();
-    prm.phase32 = 1;
-    prm.tol = std::max(100.0 * tol, kTol32Floor);
-    int st32 = run_phase<float, B>(L, perm0, n_dots, d_rowptr, d_col, d_H, d_M, prm, s, it32);
-    if (st32 != QD_OK) return st32;
-    // X (float, slot 0) -> double in slot 1; slot 1 becomes X, slot 0 becomes W
-    convert_kernel<B><<<nchunks, 256, 0, s>>>(L.chunks, reinterpret_cast<const float *>(L.slot[0]),
-                                              L.slot[1]);
-    QD_CHECK_LAUNCH();
-    const int perm1[9] = {1, 0, 2, 3, 4, 5, 6, 7, 8};
-    Bufs<double, B> b64(L.slot, perm1);
-    zero_aux_kernel<double, B><<<nchunks, 256, 0, s>>>(L.chunks, b64.W, b64.P, b64.HW, b64.MW,
-                                                       b64.HP, b64.MP);
-    QD_CHECK_LAUNCH();
-    phase_reset_kernel<<<(n_dots + 127) / 128, 128, 0, s>>>(L.st, n_dots);
-    QD_CHECK_LAUNCH();
-    prm.phase32 = 0;
-    prm.tol = tol;
-    int st64 = run_phase<double, B>(L, perm1, n_dots, d_rowptr, d_col, d_H, d_M, prm, s, it64);
-    if (st64 != QD_OK) return st64;
-    output_kernel<B><<<nchunks, 256, 0, s>>>(L.chunks, L.slot[1], k, d_X_out);
+  prm.tol = tol;
+  prm.tol32 = std::max(100.0 * tol, kTol32Floor);
+  Bufs<double> b64(L.slot);
+  if (mixed) {
+    Bufs<float> b32(L.slot32);
+    init_kernel<float, B><<<nchunks, 256, 0, s>>>(L.chunks, L.row_off, seed, b32.X, b32.W, b32.P,
+                                                  b32.HW, b32.MW, b32.HP, b32.MP);
     QD_CHECK_LAUNCH();
   } else {
-    Bufs<double, B> b(L.slot, perm0);
-    init_kernel<double, B><<<nchunks, 256, 0, s>>>(L.chunks, L.row_off, seed, b.X, b.W, b.P,
-                                                   b.HW, b.MW, b.HP, b.MP);
-    QD_CHECK_LAUNCH();
-    prm.phase32 = 0;
-    prm.tol = tol;
-    int st64 = run_phase<double, B>(L, perm0, n_dots, d_rowptr, d_col, d_H, d_M, prm, s, it64);
-    if (st64 != QD_OK) return st64;
-    output_kernel<B><<<nchunks, 256, 0, s>>>(L.chunks, L.slot[0], k, d_X_out);
+    init_kernel<double, B><<<nchunks, 256, 0, s>>>(L.chunks, L.row_off, seed, b64.X, b64.W,
+                                                   b64.P, b64.HW, b64.MW, b64.HP, b64.MP);
     QD_CHECK_LAUNCH();
   }
+  int iters_run = 0;
+  int rs = run_solver<B>(L, mixed, n_dots, d_rowptr, d_col, d_H, d_M, prm, s, iters_run);
+  if (rs != QD_OK) return rs;
+  output_kernel<B><<<nchunks, 256, 0, s>>>(L.chunks, b64.X, k, d_X_out);
+  QD_CHECK_LAUNCH();
   finalize_kernel<B><<<(n_dots + 127) / 128, 128, 0, s>>>(L.st, n_dots, k, L.theta, L.relres,
                                                           d_E_out, d_res_out, d_iters_out);
   QD_CHECK_LAUNCH();
@@ -1168,7 +1236,12 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
       for (int ph = 0; ph < 2; ++ph)
         for (int kd = 0; kd < 3; ++kd) h_counts[d * 6 + ph * 3 + kd] = st[d].launches[ph][kd];
   if (h_info) {
-    h_info[0] = it32 + it64;
+    int it32 = 0, it64 = 0;
+    for (auto &x : st) {
+      it32 = std::max(it32, x.iters32);
+      it64 = std::max(it64, x.iters - x.iters32);
+    }
+    h_info[0] = iters_run;
     h_info[1] = it32;
     h_info[2] = it64;
     h_info[3] = nconv;
@@ -1183,7 +1256,6 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
 extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b,
                                         int prec_mode, const qd_dst_prec *h_prec,
                                         size_t *bytes) {
-  (void)prec_mode;
   if (!bytes || n_dots <= 0 || n_rows_total <= 0 || b < 4 || b > kMaxB || b % 4) return QD_ERR_INVALID;
   // upper bound on the chunk count: every dot contributes at most one partial chunk
   const int nchunks = int(n_rows_total / kChunkRows) + n_dots;
@@ -1191,7 +1263,7 @@ extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, in
   if (h_prec) qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);
   Layout L;
-  carve(ar, n_dots, n_rows_total, b, nchunks, ntx, nty, L);
+  carve(ar, n_dots, n_rows_total, b, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, L);
   *bytes = ar.used;
   return QD_OK;
 }
