@@ -80,19 +80,30 @@ class DSTPreconditioner:
         flat = np.concatenate(mats) if mats else np.zeros(1, np.float64)
         self.d_mats = torch.from_numpy(flat).to(device)
 
-    @staticmethod
-    def spec_for(mesh, c, V):
-        """(nx, ny, cx, cy, shift) for a StructuredMesh with Dirichlet elimination."""
+    #: Diagonal shift of the preconditioner in eV (times the lattice cell area).
+    #: The preconditioner only models the kinetic operator, so a small positive
+    #: shift keeps it SPD on coarse lattices without flattening the low end of
+    #: the spectrum; the LOBPCG iteration count on the 256-dot sweep is lowest
+    #: near 0.02 eV (0.01-0.04 eV within 20 %, a shift of |V_min| doubles it).
+    SHIFT_EV = 0.02
+
+    @classmethod
+    def spec_for(cls, mesh, c, V, shift_ev: float | None = None):
+        """(nx, ny, cx, cy, shift) for a StructuredMesh with Dirichlet elimination.
+
+        The operator is ``cx Kx + cy Ky + shift`` on the interior lattice of the
+        order-p nodes, with ``Kx``, ``Ky`` the 1-D second-difference matrices,
+        ``cx = c_bar hy/hx`` and ``cy = c_bar hx/hy`` for the geometric mean
+        ``c_bar`` of the per-element kinetic coefficient.
+        """
         p = mesh.order
         nx, ny = p * mesh.nx - 1, p * mesh.ny - 1
         if nx < 1 or ny < 1:
             return None
         hx, hy = mesh.Lx / (p * mesh.nx), mesh.Ly / (p * mesh.ny)
         cbar = float(np.exp(np.mean(np.log(np.asarray(c, np.float64)))))
-        V = np.asarray(V, np.float64)
-        sigma = V.min() - 0.25 * (V.max() - V.min()) - 0.05
-        shift = (max(0.0, -sigma) + 0.05) * hx * hy
-        return (nx, ny, cbar * hy / hx, cbar * hx / hy, shift)
+        s = cls.SHIFT_EV if shift_ev is None else float(shift_ev)
+        return (nx, ny, cbar * hy / hx, cbar * hx / hy, s * hx * hy)
 
 
 class Workspace:
