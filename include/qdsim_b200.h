@@ -33,7 +33,8 @@ enum {
   QD_ERR_BREAKDOWN = -4,      /* Gram matrix not positive definite / NaN input   */
   QD_ERR_WORKSPACE = -5,      /* workspace too small or misaligned               */
   QD_ERR_DEGENERATE = -6,     /* zero-area element or non-finite coefficient     */
-  QD_ERR_LIMIT = -7           /* a size exceeds a compiled-in limit              */
+  QD_ERR_LIMIT = -7,          /* a size exceeds a compiled-in limit              */
+  QD_ERR_TIMEOUT = -8         /* a device-side wait exceeded its time bound      */
 };
 
 /* assembly modes */
@@ -125,11 +126,13 @@ int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32,
  * dot's reduced DOFs must be the interior points of an nx x ny lattice in
  * row-major order (structured rectangle, homogeneous Dirichlet boundary).
  * T = (cx Kx + cy Ky + shift I)^-1 with Kx, Ky the 1-D second differences,
- * applied as DST-I transforms; nx = 0 disables preconditioning for the dot.
- * d_prec_mats holds the orthonormal DST-I matrices
- * S[i][j] = sqrt(2/(N+1)) sin(pi (i+1)(j+1)/(N+1)) (double, row-major) at
- * sx_off (N = nx) and sy_off (N = ny).  The transforms run in the precision
- * of the vectors they act on. */
+ * applied as DST-I transforms on the tensor cores (BF16 operands, FP32
+ * accumulation); nx = 0 disables preconditioning for the dot.
+ * d_prec_mats holds, for each lattice size N in use, the orthonormal DST-I
+ * matrix S[i][j] = sqrt(2/(N+1)) sin(pi (i+1)(j+1)/(N+1)) in the tensor-core
+ * operand layout written by qd_dst_matrix_fill (BF16, qd_dst_matrix_size(N)
+ * elements), starting at element offset sx_off (N = nx) and sy_off (N = ny);
+ * offsets are multiples of 8 elements. */
 typedef struct {
   int32_t nx, ny;
   int64_t sx_off, sy_off;
@@ -147,7 +150,7 @@ typedef struct {
  *   b            block size (k <= b <= 32; b - k guard vectors)
  *   prec_mode    QD_PREC_FP64 or QD_PREC_MIXED
  *   tol          target relative eigenvalue error: converged when, for all k
- *                pairs, 20 (||r||/||Mx||)^2 / ((t_{b-1} - t) |t|) <= tol with
+ *                pairs, (||r||/||Mx||)^2 / ((t_{b-1} - t) |t|) <= tol with
  *                r = H x - t M x (quadratic residual estimate, gap to the block
  *                edge) and ||r|| <= 1e-2 |t| ||Mx||
  *   d_X_out      double[n_rows_total * k] row-major per row (X[row*k + j]),
@@ -160,7 +163,7 @@ typedef struct {
  *                SpMM, Gram and update that did work in the FP32 and the FP64
  *                phase (for algorithmic-byte accounting)
  *   h_prec/d_prec_mats  optional per-dot DST preconditioner (host descriptor
- *                array, device matrices); NULL = unpreconditioned
+ *                array, device BF16 matrices); NULL = unpreconditioned
  * The initial block is drawn from `seed` (deterministic).  Returns
  * QD_ERR_NOT_CONVERGED if any dot hits max_iter (results still written).
  * ------------------------------------------------------------------------- */
@@ -169,7 +172,7 @@ int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b, int pr
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
                     const int32_t *d_rowptr, const int32_t *d_col,
                     const double *d_H, const double *d_M,
-                    const qd_dst_prec *h_prec, const double *d_prec_mats,
+                    const qd_dst_prec *h_prec, const void *d_prec_mats,
                     int k, int b, int prec_mode, double tol, int max_iter, uint64_t seed,
                     double *d_X_out, double *d_E_out, double *d_res_out, int32_t *d_iters_out,
                     int32_t *h_info, int32_t *h_counts, void *d_work, size_t work_bytes,
@@ -180,8 +183,17 @@ int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_r
  * descriptors as qd_lobpcg_solve; exposed for testing and reuse. */
 int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int b,
                                   const qd_dst_prec *h_prec, size_t *bytes);
+
+/* Element count (BF16) of the DST-I matrix of lattice size n in the
+ * tensor-core layout, and the host routine that writes it (round to nearest
+ * even).  Layout: rows padded to R = 16 ceil(n/16), columns (k) to
+ * 64 ceil(n/64); rows split into blocks of 512; within a block of r rows,
+ * element (row, k) sits at  (k/64) r 64 + ((k%64)/8) r 8 + (row/8) 64 +
+ * (row%8) 8 + k%8  (8 x 8 core matrices, 16 bytes per core-matrix row). */
+int qd_dst_matrix_size(int32_t n, int64_t *elems);
+int qd_dst_matrix_fill(int32_t n, uint16_t *h_out);
 int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, int b, int vec_fp32,
-                         const qd_dst_prec *h_prec, const double *d_prec_mats,
+                         const qd_dst_prec *h_prec, const void *d_prec_mats,
                          const void *d_in, void *d_out, void *d_work, size_t work_bytes,
                          void *stream);
 

@@ -18,6 +18,7 @@ QD_ERR_BREAKDOWN = -4
 QD_ERR_WORKSPACE = -5
 QD_ERR_DEGENERATE = -6
 QD_ERR_LIMIT = -7
+QD_ERR_TIMEOUT = -8
 
 QD_ASM_FEM = 0
 QD_ASM_REF_CYTHON = 1
@@ -50,6 +51,8 @@ SIGNATURES = {
                                _int, _u64, _p, _p, _p, _p, _p, _p, _p, _sz, _p]),
     "qd_dst_precond_workspace_size": (_int, [_i32, _p, _int, _p, _p]),
     "qd_dst_precond_apply": (_int, [_i32, _p, _int, _int, _p, _p, _p, _p, _p, _sz, _p]),
+    "qd_dst_matrix_size": (_int, [_i32, _p]),
+    "qd_dst_matrix_fill": (_int, [_i32, _p]),
     "qd_pcg_workspace_size": (_int, [_i32, _int, _p]),
     "qd_pcg_solve": (_int, [_i32, _int, _p, _p, _p, _p, _p, _p, _dbl, _int, _p, _p,
                             _p, _sz, _p]),

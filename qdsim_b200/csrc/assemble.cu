@@ -227,6 +227,7 @@ extern "C" const char *qd_status_string(int status) {
     case QD_ERR_WORKSPACE: return "workspace too small";
     case QD_ERR_DEGENERATE: return "degenerate element or non-finite coefficient";
     case QD_ERR_LIMIT: return "size exceeds a compiled-in limit";
+    case QD_ERR_TIMEOUT: return "device-side wait exceeded its time bound";
     default: return "unknown status";
   }
 }

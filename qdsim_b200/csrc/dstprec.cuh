@@ -9,14 +9,38 @@
 // shift that makes it positive definite.  DST-I diagonalises Kx and Ky, so
 //   T R = Sx Sy (Lambda^-1 o (Sy Sx R)),   S symmetric orthonormal, S = S^-1,
 // i.e. two transform-GEMMs along x and two along y per application, run for
-// all dots and all B columns at once.  The transforms run in the precision of
-// the vector storage: near convergence T r is dominated by a component along
-// x itself and the useful correction is ~1e-6 of it, below FP32 resolution,
-// so the FP64 finishing phase transforms in FP64.
+// all dots and all B columns at once on the tensor cores (tcgen05, BF16
+// operands, FP32 accumulation in TMEM).  A preconditioner only steers the
+// search directions (the Rayleigh-Ritz step is exact), and a relative
+// perturbation of T of the size of the BF16 rounding leaves the condition
+// number of T A, and with it the iteration count, unchanged.
+//
+// Vector data of one dot is a 3-D array [slow][k][b] or [k][fast] seen by a
+// pass as the GEMM  out(r, n) = sum_k S[r][k] in(k, n),  k the lattice index
+// being transformed and n = (other lattice index, column b):
+//   "grouped":  addr(k, n) = (n / B) * dim * B + k * B + n % B
+//   "row-major": addr(k, n) = k * (other * B) + n
+// Pass 1 (x): W grouped -> t1 row-major [ix][iy][b]
+// Pass 2 (y): t1 grouped -> t2 row-major [ky][kx][b], scaled by 1 / lambda
+// Pass 3 (y): t2 row-major -> t1 grouped [kx][iy][b]
+// Pass 4 (x): t1 row-major -> W grouped [iy][ix][b]
+// so that every pass reads or writes one side with unit stride along n.
+//
+// One CTA computes a 128 (n) x up to 512 (r) block of out^T in TMEM:
+//   A = in^T tile (128 n x 64 k per K slab), staged by the threads from the
+//       vector precision into BF16 shared memory (K-major, no swizzle);
+//   B = S tile (r x 64 k), pre-arranged in global memory in exactly the
+//       shared-memory layout and fetched by one 1-D bulk copy per slab;
+//   D = 128 TMEM lanes (n) x r columns (FP32).
+// Two smem stages: the threads stage slab s+1 while the MMAs of slab s run.
 #pragma once
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <algorithm>
 #include <cstdint>
+#include <mutex>
 #include "common.h"
+#include "tc.cuh"
 
 namespace qd {
 
@@ -24,170 +48,328 @@ struct GemmTile {
   int dot, m0, n0, pad;
 };
 
-constexpr int kGemmTile = 64;     // rows (M) per tile
-constexpr int kGemmTileN = 64;    // columns (N) per tile
-constexpr int kGemmK = 16;
+constexpr int kTcN = 128;        // data columns (n) per CTA = TMEM lanes
+constexpr int kTcK = 64;         // K per shared-memory slab
+constexpr int kTcRows = 512;     // transform rows (r) per CTA = max TMEM columns
+constexpr int kTcThreads = 256;
+constexpr uint64_t kTcWaitNs = 1000000000ull;   // 1 s bound on every wait
+constexpr int kTcABytes = kTcN * kTcK * 2;      // 16 KiB per A stage
 
-// out(r, n) = sum_k S[r][k] in(k, n)  (then / lambda when SCALE)
-// x pass: r = ix, n = iy*B + b,  addr = base + (n / B) * nx*B + r*B + n % B
-// y pass: r = iy, n = ix*B + b,  addr = base + r * nx*B + n
-// 256 threads, each owns a 4 (rows) x 4 (columns) block of the 64 x 64 tile
-// (small tiles keep the GPU busy when only a few large dots are still iterating).
-// S is symmetric, so the A tile is read as S[k][r]: coalesced loads and
-// conflict-free shared stores.  The next k-slice is prefetched into registers
-// while the current one is multiplied.
-template <typename TC, typename TI, typename TO, bool YPASS, bool SCALE>
-__global__ void __launch_bounds__(256)
-dst_gemm_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active,
-                int active_stride, const qd_dst_prec *__restrict__ desc,
-                const int32_t *__restrict__ row_off, const double *__restrict__ mats, int B,
-                const TI *__restrict__ in, TO *__restrict__ out) {
+__host__ __device__ inline int tc_rpad(int dim) { return (dim + 15) / 16 * 16; }
+__host__ __device__ inline int tc_ks(int dim) { return (dim + kTcK - 1) / kTcK; }
+__host__ __device__ inline int64_t tc_mat_elems(int dim) {
+  return int64_t(tc_rpad(dim)) * tc_ks(dim) * kTcK;
+}
+__host__ __device__ inline uint32_t tc_tmem_cols(int rows) {
+  uint32_t c = 32;
+  while (c < uint32_t(rows)) c <<= 1;
+  return c;
+}
+
+// Dynamic shared-memory layout for a launch whose CTAs hold at most
+// `rows_max` transform rows.
+struct TcSmem {
+  uint32_t a_off[2], b_off[2], lam_off, bar_off, total;
+  __host__ __device__ explicit TcSmem(int rows_max) {
+    const uint32_t bb = uint32_t(rows_max) * 128u;   // B stage: rows x 64 k x 2 bytes
+    a_off[0] = 0;
+    a_off[1] = kTcABytes;
+    b_off[0] = 2 * kTcABytes;
+    b_off[1] = b_off[0] + bb;
+    lam_off = b_off[1] + bb;
+    bar_off = lam_off + kTcRows * 4;
+    total = bar_off + 64;
+  }
+};
+
+// Bytes of dynamic shared memory to request: the layout, raised so that no
+// more CTAs fit on an SM than its 512 TMEM columns can serve at once (an SM
+// has 228 KiB of shared memory and reserves 1 KiB per CTA).
+inline size_t tc_smem_request(int rows_max) {
+  const size_t need = TcSmem(rows_max).total;
+  const int allowed = 512 / int(tc_tmem_cols(rows_max));
+  const size_t floor_bytes = 233472 / size_t(allowed + 1) + 1 + 128 - 1024;
+  return need > floor_bytes ? need : floor_bytes;
+}
+
+template <typename T>
+__device__ __forceinline__ float to_f32(T v) {
+  return float(v);
+}
+template <>
+__device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) {
+  return __bfloat162float(v);
+}
+template <typename T>
+__device__ __forceinline__ __nv_bfloat16 to_bf16(T v) {
+  return __float2bfloat16_rn(float(v));
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 to_bf16<double>(double v) {
+  return __double2bfloat16(v);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 to_bf16<__nv_bfloat16>(__nv_bfloat16 v) {
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T from_f32(float v) {
+  return T(v);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+
+// out(r, n) = sum_k S[r][k] in(k, n)  [/ (lambda_r(r) + lambda_n(n / B) + shift)]
+template <typename TI, typename TO, bool YPASS, bool IN_G, bool OUT_G, bool SCALE>
+__global__ void __launch_bounds__(kTcThreads)
+dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active,
+              int active_stride, const qd_dst_prec *__restrict__ desc,
+              const int32_t *__restrict__ row_off, const uint16_t *__restrict__ mats, int B,
+              int rows_max, const TI *__restrict__ in, TO *__restrict__ out, int *err) {
   const GemmTile t = tiles[blockIdx.x];
   if (active && !active[size_t(t.dot) * active_stride]) return;
   const qd_dst_prec d = desc[t.dot];
-  const int nx = d.nx, ny = d.ny;
-  const int dim = YPASS ? ny : nx;
-  const int ncols = YPASS ? nx * B : ny * B;
-  const double *S = mats + (YPASS ? d.sy_off : d.sx_off);
+  const int dim = YPASS ? d.ny : d.nx;
+  const int other = YPASS ? d.nx : d.ny;
+  const int ncols = other * B;
+  const int KS = tc_ks(dim);
+  const int rows = min(kTcRows, tc_rpad(dim) - t.m0);   // multiple of 16
+  const uint32_t tcols = tc_tmem_cols(rows);
+  const uint16_t *S = mats + (YPASS ? d.sy_off : d.sx_off) + int64_t(t.m0) * KS * kTcK;
   const size_t base = size_t(row_off[t.dot]) * B;
-  auto addr = [&](int r, int n) -> size_t {
-    if (YPASS) return base + size_t(r) * (size_t(nx) * B) + n;
-    return base + size_t(n / B) * (size_t(nx) * B) + size_t(r) * B + (n % B);
-  };
-  __shared__ __align__(16) TC As[kGemmK][kGemmTile + 4];
-  __shared__ __align__(16) TC Bs[kGemmK][kGemmTileN + 4];
-  const int tid = threadIdx.x;
-  const int ty = tid / 16, tx = tid % 16;
-  TC acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = TC(0);
-  // per-thread load slots: A 4 elements (1024 / 256), B 4 elements (1024 / 256)
-  TC ra[4], rb[4];
-  auto fetch = [&](int k0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;
-      const int kk = e / kGemmTile, mm = e % kGemmTile;
-      const int gk = k0 + kk, gm = t.m0 + mm;
-      ra[q] = (gk < dim && gm < dim) ? TC(__ldg(S + size_t(gk) * dim + gm)) : TC(0);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;
-      const int kk = e / kGemmTileN, nn = e % kGemmTileN;
-      const int gk = k0 + kk, gn = t.n0 + nn;
-      rb[q] = (gk < dim && gn < ncols) ? TC(in[addr(gk, gn)]) : TC(0);
-    }
-  };
-  fetch(0);
-  for (int k0 = 0; k0 < dim; k0 += kGemmK) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;
-      As[e / kGemmTile][e % kGemmTile] = ra[q];
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;
-      Bs[e / kGemmTileN][e % kGemmTileN] = rb[q];
-    }
-    __syncthreads();
-    if (k0 + kGemmK < dim) fetch(k0 + kGemmK);
-#pragma unroll
-    for (int kk = 0; kk < kGemmK; ++kk) {
-      TC a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
+
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const TcSmem lay(rows_max);
+  uint64_t *bar_full = reinterpret_cast<uint64_t *>(sm + lay.bar_off);
+  uint64_t *bar_mma = bar_full + 2;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar_mma + 2);
+  float *lam = reinterpret_cast<float *>(sm + lay.lam_off);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    tc::mbar_init(&bar_full[0], 1);
+    tc::mbar_init(&bar_full[1], 1);
+    tc::mbar_init(&bar_mma[0], 1);
+    tc::mbar_init(&bar_mma[1], 1);
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, tcols);
+    tc::tmem_relinquish();
   }
   if (SCALE) {
-    // eigenvalue tables for this tile: rows ky = m0.., columns kx = n0/B..
-    __shared__ double s_sy[kGemmTile];
-    __shared__ double s_sx[kGemmTileN / 4 + 2];
-    const int kx0 = t.n0 / B;
-    const int nkx = (t.n0 + kGemmTileN - 1) / B - kx0 + 1;
-    if (tid < kGemmTile) {
-      const double v = sinpi(double(t.m0 + tid + 1) / double(2 * (ny + 1)));
-      s_sy[tid] = double(d.cy) * 4.0 * v * v;
-    } else if (tid - kGemmTile < nkx) {
-      const double v = sinpi(double(kx0 + tid - kGemmTile + 1) / double(2 * (nx + 1)));
-      s_sx[tid - kGemmTile] = double(d.cx) * 4.0 * v * v;
+    const float c_r = YPASS ? d.cy : d.cx;
+    for (int i = tid; i < rows; i += kTcThreads) {
+      const int r = t.m0 + i;
+      float v = 0.f;
+      if (r < dim) {
+        const double sn = sinpi(double(r + 1) / double(2 * (dim + 1)));
+        v = float(double(c_r) * 4.0 * sn * sn);
+      }
+      lam[i] = v;
     }
-    __syncthreads();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  // ---- main loop over K slabs ---------------------------------------------
+  const int n_loc = tid & (kTcN - 1);
+  const int cgrp = tid >> 7;                  // 0 / 1: chunks cgrp, cgrp+2, ...
+  const int n = t.n0 + n_loc;
+  const bool nvalid = n < ncols;
+  const size_t in_base = IN_G ? base + size_t(n / B) * dim * B + (n % B) : base + n;
+  const size_t in_kstride = IN_G ? size_t(B) : size_t(ncols);
+  const uint32_t sA0 = tc::smem_u32(sm + lay.a_off[0]);
+  const uint32_t sB0 = tc::smem_u32(sm + lay.b_off[0]);
+  const uint32_t lboB = uint32_t(rows) * 16u;     // (rows / 8) core matrices x 128 bytes
+  const uint32_t bbytes = uint32_t(rows) * 128u;  // one B slab
+  const uint32_t bstage = lay.b_off[1] - lay.b_off[0];
+  int issued = 0;   // slabs whose copy and MMAs thread 0 has issued
+  bool fail = false;
+  for (int s = 0; s < KS; ++s) {
+    const int st = s & 1;
+    const uint32_t sA = sA0 + uint32_t(st) * kTcABytes, sB = sB0 + uint32_t(st) * bstage;
+    if (s >= 2 && !tc::mbar_wait(&bar_mma[st], ((s - 2) >> 1) & 1, kTcWaitNs)) fail = true;
+    if (tid == 0 && !fail) {
+      tc::mbar_arrive_expect_tx(&bar_full[st], bbytes);
+      tc::bulk_g2s(sm + lay.b_off[0] + st * bstage, S + size_t(s) * rows * kTcK, bbytes,
+                   &bar_full[st]);
+    }
+    // A slab: this thread's n, k chunks c = cgrp + 2j, 8 consecutive k each
+    float v[4][8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = t.m0 + ty * 4 + i;
-      if (r >= dim) continue;
+    for (int j = 0; j < 4; ++j) {
+      const int kc = s * kTcK + (cgrp + 2 * j) * 8;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int n = t.n0 + tx * 4 + j;
-        if (n >= ncols) continue;
-        const double lam = s_sy[ty * 4 + i] + s_sx[n / B - kx0] + double(d.shift);
-        out[addr(r, n)] = TO(double(acc[i][j]) / lam);
+      for (int e = 0; e < 8; ++e) {
+        const int k = kc + e;
+        v[j][e] = (nvalid && k < dim) ? to_f32(in[in_base + size_t(k) * in_kstride]) : 0.f;
+      }
+    }
+    uint8_t *a_st = sm + lay.a_off[0] + st * kTcABytes;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = cgrp + 2 * j;
+      uint4 pk;
+      uint32_t *w = reinterpret_cast<uint32_t *>(&pk);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v[j][2 * e], v[j][2 * e + 1]);
+        w[e] = *reinterpret_cast<const uint32_t *>(&h);
+      }
+      *reinterpret_cast<uint4 *>(a_st + c * (kTcABytes / 8) + (n_loc >> 3) * 128 +
+                                 (n_loc & 7) * 16) = pk;
+    }
+    tc::fence_proxy_async_smem();
+    fail = __syncthreads_or(fail) != 0;
+    if (fail) break;
+    if (tid == 0) {
+      issued = s + 1;
+      if (!tc::mbar_wait(&bar_full[st], (s >> 1) & 1, kTcWaitNs)) {
+        fail = true;
+      } else {
+        tc::fence_after_sync();
+#pragma unroll
+        for (int kk = 0; kk < kTcK / 16; ++kk) {
+          const uint64_t ad = tc::smem_desc(sA + kk * 2 * (kTcABytes / 8), kTcABytes / 8, 128);
+          for (int p0 = 0; p0 < rows; p0 += 256) {
+            const int np = min(256, rows - p0);
+            const uint64_t bd = tc::smem_desc(sB + kk * 2 * lboB + (p0 >> 3) * 128, lboB, 128);
+            tc::mma_bf16(tmem + uint32_t(p0), ad, bd, tc::idesc_bf16_f32(128, np),
+                         (s > 0 || kk > 0) ? 1u : 0u);
+          }
+        }
+        tc::mma_commit(&bar_mma[st]);
+      }
+    }
+  }
+  if (!fail) {
+    const int last = (KS - 1) & 1;
+    if (!tc::mbar_wait(&bar_mma[last], ((KS - 1) >> 1) & 1, kTcWaitNs)) fail = true;
+  }
+  fail = __syncthreads_or(fail) != 0;
+  if (!fail) {
+    tc::fence_after_sync();
+    // ---- epilogue: TMEM lane quarter (warp & 3), column half (warp >> 2) ---
+    const int q = warp & 3, h = warp >> 2;
+    const int ne = t.n0 + q * 32 + lane;
+    const bool ev = ne < ncols;
+    const size_t obase = OUT_G ? base + size_t(ne / B) * dim * B + (ne % B) : base + ne;
+    const size_t ostride = OUT_G ? size_t(B) : size_t(ncols);
+    float lam_n = 0.f;
+    if (SCALE && ev) {
+      const double sn = sinpi(double(ne / B + 1) / double(2 * (other + 1)));
+      lam_n = float(double(YPASS ? d.cx : d.cy) * 4.0 * sn * sn + double(d.shift));
+    }
+    for (int c = h; c < rows / 16; c += 2) {
+      float a[16];
+      tc::tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c * 16), a);
+      if (ev) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int r = t.m0 + c * 16 + j;
+          if (r < dim) {
+            float x = a[j];
+            if (SCALE) x = x / (lam[c * 16 + j] + lam_n);
+            out[obase + size_t(r) * ostride] = from_f32<TO>(x);
+          }
+        }
       }
     }
   } else {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = t.m0 + ty * 4 + i;
-      if (r >= dim) continue;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int n = t.n0 + tx * 4 + j;
-        if (n < ncols) out[addr(r, n)] = TO(acc[i][j]);
+    if (tid == 0) {
+      atomicOr(err, 1);
+      // let this CTA's own bulk copies and MMAs finish before its shared
+      // memory and TMEM are released: the last phase armed on each barrier
+      // (slabs issued-1 and issued-2; a commit covers all earlier MMAs)
+      for (int u = issued - 2; u < issued; ++u) {
+        if (u < 0) continue;
+        tc::mbar_wait(&bar_full[u & 1], (u >> 1) & 1, kTcWaitNs);
+        tc::mbar_wait(&bar_mma[u & 1], (u >> 1) & 1, kTcWaitNs);
       }
     }
   }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, tcols);
 }
 
-// Tile tables of the x and y passes for every dot with a preconditioner.
+// Tile tables of the x passes (dim nx, columns ny*B) and y passes (dim ny,
+// columns nx*B) for every dot with a preconditioner; rows_x / rows_y receive
+// the largest TMEM row block of each.
 inline void dst_tiles(int n_dots, const qd_dst_prec *h, int B, GemmTile *tx, int64_t *ntx,
-                      GemmTile *ty, int64_t *nty) {
+                      GemmTile *ty, int64_t *nty, int *rows_x = nullptr, int *rows_y = nullptr) {
   int64_t a = 0, b = 0;
+  int rx = 16, ry = 16;
   for (int d = 0; d < n_dots; ++d) {
     const int nx = h[d].nx, ny = h[d].ny;
     if (nx <= 0 || ny <= 0) continue;
-    for (int m0 = 0; m0 < nx; m0 += kGemmTile)
-      for (int n0 = 0; n0 < ny * B; n0 += kGemmTileN) {
+    for (int m0 = 0; m0 < tc_rpad(nx); m0 += kTcRows) {
+      rx = std::max(rx, std::min(kTcRows, tc_rpad(nx) - m0));
+      for (int n0 = 0; n0 < ny * B; n0 += kTcN) {
         if (tx) tx[a] = GemmTile{d, m0, n0, 0};
         ++a;
       }
-    for (int m0 = 0; m0 < ny; m0 += kGemmTile)
-      for (int n0 = 0; n0 < nx * B; n0 += kGemmTileN) {
+    }
+    for (int m0 = 0; m0 < tc_rpad(ny); m0 += kTcRows) {
+      ry = std::max(ry, std::min(kTcRows, tc_rpad(ny) - m0));
+      for (int n0 = 0; n0 < nx * B; n0 += kTcN) {
         if (ty) ty[b] = GemmTile{d, m0, n0, 0};
         ++b;
       }
+    }
   }
   *ntx = a;
   *nty = b;
+  if (rows_x) *rows_x = rx;
+  if (rows_y) *rows_y = ry;
 }
 
-// W <- T W using tmp1/tmp2 (TV, n x B each); compute precision = TV.
-template <typename TV>
-inline cudaError_t dst_apply(const GemmTile *tx, int64_t ntx, const GemmTile *ty, int64_t nty,
-                             const int *active, int active_stride, const qd_dst_prec *desc,
-                             const int32_t *row_off, const double *mats, int B, const TV *in,
-                             TV *out, TV *tmp1, TV *tmp2, cudaStream_t s) {
-  if (ntx == 0 || nty == 0) return cudaSuccess;
-  dst_gemm_kernel<TV, TV, TV, false, false><<<unsigned(ntx), 256, 0, s>>>(
-      tx, active, active_stride, desc, row_off, mats, B, in, tmp1);
-  dst_gemm_kernel<TV, TV, TV, true, true><<<unsigned(nty), 256, 0, s>>>(
-      ty, active, active_stride, desc, row_off, mats, B, tmp1, tmp2);
-  dst_gemm_kernel<TV, TV, TV, true, false><<<unsigned(nty), 256, 0, s>>>(
-      ty, active, active_stride, desc, row_off, mats, B, tmp2, tmp1);
-  dst_gemm_kernel<TV, TV, TV, false, false><<<unsigned(ntx), 256, 0, s>>>(
-      tx, active, active_stride, desc, row_off, mats, B, tmp1, out);
-  g_launches.fetch_add(4, std::memory_order_relaxed);
+template <typename TI, typename TO, bool YPASS, bool IN_G, bool OUT_G, bool SCALE>
+inline cudaError_t dst_tc_launch(const GemmTile *tiles, int64_t ntiles, int rows_max,
+                                 const int *active, int active_stride, const qd_dst_prec *desc,
+                                 const int32_t *row_off, const uint16_t *mats, int B,
+                                 const TI *in, TO *out, int *err, cudaStream_t s) {
+  auto kern = dst_tc_kernel<TI, TO, YPASS, IN_G, OUT_G, SCALE>;
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [&] {
+    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+  });
+  if (attr != cudaSuccess) return attr;
+  kern<<<unsigned(ntiles), kTcThreads, tc_smem_request(rows_max), s>>>(
+      tiles, active, active_stride, desc, row_off, mats, B, rows_max, in, out, err);
   return cudaGetLastError();
+}
+
+// W <- T W (in == out allowed) using tmp1/tmp2 (>= n x B bf16 each).
+template <typename TV>
+inline cudaError_t dst_apply(const GemmTile *tx, int64_t ntx, int rows_x, const GemmTile *ty,
+                             int64_t nty, int rows_y, const int *active, int active_stride,
+                             const qd_dst_prec *desc, const int32_t *row_off,
+                             const uint16_t *mats, int B, const TV *in, TV *out, void *tmp1,
+                             void *tmp2, int *err, cudaStream_t s) {
+  if (ntx == 0 || nty == 0) return cudaSuccess;
+  using bf = __nv_bfloat16;
+  bf *t1 = static_cast<bf *>(tmp1), *t2 = static_cast<bf *>(tmp2);
+  cudaError_t e;
+  e = dst_tc_launch<TV, bf, false, true, false, false>(tx, ntx, rows_x, active, active_stride,
+                                                       desc, row_off, mats, B, in, t1, err, s);
+  if (e != cudaSuccess) return e;
+  e = dst_tc_launch<bf, bf, true, true, false, true>(ty, nty, rows_y, active, active_stride,
+                                                     desc, row_off, mats, B, t1, t2, err, s);
+  if (e != cudaSuccess) return e;
+  e = dst_tc_launch<bf, bf, true, false, true, false>(ty, nty, rows_y, active, active_stride,
+                                                      desc, row_off, mats, B, t2, t1, err, s);
+  if (e != cudaSuccess) return e;
+  e = dst_tc_launch<bf, TV, false, false, true, false>(tx, ntx, rows_x, active, active_stride,
+                                                       desc, row_off, mats, B, t1, out, err, s);
+  g_launches.fetch_add(4, std::memory_order_relaxed);
+  return e;
 }
 
 }  // namespace qd

@@ -946,11 +946,13 @@ struct Layout {
   float *slot32[9];  // FP32 vector blocks (mixed precision only)
   int nchunks;
   // DST preconditioner
-  double *tmp1, *tmp2;   // used as float in the FP32 phase
+  void *tmp1, *tmp2;     // BF16 intermediates of the transform passes
   qd_dst_prec *desc;
   qd::GemmTile *tiles_x, *tiles_y;
   int64_t ntx, nty;
-  const double *mats;
+  int rows_x, rows_y;    // largest TMEM row block of the x / y passes
+  const uint16_t *mats;
+  int *dst_err;          // set by a transform kernel whose wait ran out
 };
 
 size_t rr_smem_bytes(int B) {
@@ -978,16 +980,19 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t
   L.ntx = ntx;
   L.nty = nty;
   L.mats = nullptr;
+  L.rows_x = L.rows_y = 16;
   if (ntx > 0) {
-    L.tmp1 = ar.take<double>(size_t(n_rows) * B);
-    L.tmp2 = ar.take<double>(size_t(n_rows) * B);
+    L.tmp1 = ar.take<uint16_t>(size_t(n_rows) * B);
+    L.tmp2 = ar.take<uint16_t>(size_t(n_rows) * B);
     L.desc = ar.take<qd_dst_prec>(n_dots);
     L.tiles_x = ar.take<qd::GemmTile>(ntx);
     L.tiles_y = ar.take<qd::GemmTile>(nty);
+    L.dst_err = ar.take<int>(1);
   } else {
     L.tmp1 = L.tmp2 = nullptr;
     L.desc = nullptr;
     L.tiles_x = L.tiles_y = nullptr;
+    L.dst_err = nullptr;
   }
   return QD_OK;
 }
@@ -1027,10 +1032,10 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   QD_CHECK_LAUNCH();
   if (L.ntx > 0) {
     qd::prof_begin(qd::PK_PRECOND, s);
-    cudaError_t e = qd::dst_apply<TV>(L.tiles_x, L.ntx, L.tiles_y, L.nty, &L.st[0].run[PH],
-                                      int(sizeof(DotState) / sizeof(int)), L.desc, L.row_off,
-                                      L.mats, B, b.W, b.W, reinterpret_cast<TV *>(L.tmp1),
-                                      reinterpret_cast<TV *>(L.tmp2), s);
+    cudaError_t e = qd::dst_apply<TV>(L.tiles_x, L.ntx, L.rows_x, L.tiles_y, L.nty, L.rows_y,
+                                      &L.st[0].run[PH], int(sizeof(DotState) / sizeof(int)),
+                                      L.desc, L.row_off, L.mats, B, b.W, b.W, L.tmp1, L.tmp2,
+                                      L.dst_err, s);
     qd::prof_end(qd::PK_PRECOND, s);
     if (e != cudaSuccess) return QD_ERR_CUDA;
   }
@@ -1126,7 +1131,7 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
 template <int B>
 int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
             const int32_t *d_col, const double *d_H, const double *d_M,
-            const qd_dst_prec *h_prec, const double *d_mats, int k, int prec_mode,
+            const qd_dst_prec *h_prec, const uint16_t *d_mats, int k, int prec_mode,
             double tol, int max_iter, uint64_t seed, double *d_X_out, double *d_E_out,
             double *d_res_out, int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
             void *d_work, size_t work_bytes, cudaStream_t s) {
@@ -1139,7 +1144,8 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
       const qd_dst_prec &q = h_prec[d];
       if (q.nx <= 0) continue;
       if (q.ny <= 0 || int64_t(q.nx) * q.ny != h_row_off[d + 1] - h_row_off[d] ||
-          q.sx_off < 0 || q.sy_off < 0 || !(q.cx > 0.f) || !(q.cy > 0.f) || !(q.shift >= 0.f))
+          q.sx_off < 0 || q.sy_off < 0 || q.sx_off % 8 || q.sy_off % 8 || !(q.cx > 0.f) ||
+          !(q.cy > 0.f) || !(q.shift >= 0.f))
         return QD_ERR_INVALID;
     }
     qd::dst_tiles(n_dots, h_prec, B, nullptr, &ntx, nullptr, &nty);
@@ -1156,10 +1162,12 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   carve(ar, n_dots, n_rows, B, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, L);
   std::vector<qd::GemmTile> htx, hty;
   if (ntx > 0) {
+    if (reinterpret_cast<uintptr_t>(d_mats) % 16) return QD_ERR_INVALID;
     htx.resize(ntx);
     hty.resize(nty);
-    qd::dst_tiles(n_dots, h_prec, B, htx.data(), &ntx, hty.data(), &nty);
+    qd::dst_tiles(n_dots, h_prec, B, htx.data(), &ntx, hty.data(), &nty, &L.rows_x, &L.rows_y);
     L.mats = d_mats;
+    QD_CUDA_TRY(cudaMemsetAsync(L.dst_err, 0, sizeof(int), s));
     QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_x, htx.data(), ntx * sizeof(qd::GemmTile),
                                 cudaMemcpyHostToDevice, s));
     QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_y, hty.data(), nty * sizeof(qd::GemmTile),
@@ -1225,7 +1233,11 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   QD_CHECK_LAUNCH();
   QD_CUDA_TRY(cudaMemcpyAsync(st.data(), L.st, st.size() * sizeof(DotState),
                               cudaMemcpyDeviceToHost, s));
+  int dst_err = 0;
+  if (L.dst_err)
+    QD_CUDA_TRY(cudaMemcpyAsync(&dst_err, L.dst_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   QD_CUDA_TRY(cudaStreamSynchronize(s));
+  if (dst_err) return QD_ERR_TIMEOUT;
   int nconv = 0, nbreak = 0;
   for (auto &x : st) {
     nconv += (x.status == 1);
@@ -1271,12 +1283,13 @@ extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, in
 extern "C" int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off,
                                const int32_t *d_row_off, const int32_t *d_rowptr,
                                const int32_t *d_col, const double *d_H, const double *d_M,
-                               const qd_dst_prec *h_prec, const double *d_prec_mats, int k,
+                               const qd_dst_prec *h_prec, const void *d_prec_mats_v, int k,
                                int b, int prec_mode, double tol, int max_iter, uint64_t seed,
                                double *d_X_out, double *d_E_out, double *d_res_out,
                                int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
                                void *d_work, size_t work_bytes, void *stream) {
   (void)d_row_off;
+  const uint16_t *d_prec_mats = static_cast<const uint16_t *>(d_prec_mats_v);
   if (n_dots <= 0 || !h_row_off || !d_rowptr || !d_col || !d_H || !d_M || !d_X_out ||
       !d_E_out || !d_res_out || !d_iters_out || !d_work)
     return QD_ERR_INVALID;
@@ -1353,60 +1366,125 @@ extern "C" int qd_spmm_dual(int32_t n_rows, int b, int vec_fp32, const int32_t *
 #undef QD_SPMM_CASE
 }
 
+namespace {
+// Layout shared by qd_dst_precond_workspace_size and qd_dst_precond_apply.
+void carve_precond(qd::Arena &ar, int32_t n_dots, int64_t nv, int64_t ntx, int64_t nty,
+                   void **t1, void **t2, qd_dst_prec **desc, int32_t **ro, qd::GemmTile **dtx,
+                   qd::GemmTile **dty, int **err) {
+  *t1 = ar.take<uint16_t>(size_t(nv));
+  *t2 = ar.take<uint16_t>(size_t(nv));
+  *desc = ar.take<qd_dst_prec>(n_dots);
+  *ro = ar.take<int32_t>(n_dots + 1);
+  *dtx = ar.take<qd::GemmTile>(ntx);
+  *dty = ar.take<qd::GemmTile>(nty);
+  *err = ar.take<int>(1);
+}
+}  // namespace
+
+extern "C" int qd_dst_matrix_size(int32_t n, int64_t *elems) {
+  if (n < 1 || !elems) return QD_ERR_INVALID;
+  *elems = qd::tc_mat_elems(n);
+  return QD_OK;
+}
+
+extern "C" int qd_dst_matrix_fill(int32_t n, uint16_t *h_out) {
+  if (n < 1 || !h_out) return QD_ERR_INVALID;
+  const int R = qd::tc_rpad(n), KS = qd::tc_ks(n);
+  const double scale = std::sqrt(2.0 / double(n + 1));
+  auto bf16_bits = [](double x) -> uint16_t {   // round to nearest even via float
+    const float f = float(x);
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return uint16_t(u >> 16);
+  };
+  int64_t pos = 0;
+  for (int m0 = 0; m0 < R; m0 += qd::kTcRows) {
+    const int rows = std::min(qd::kTcRows, R - m0);
+    for (int sl = 0; sl < KS; ++sl)
+      for (int c = 0; c < 8; ++c)
+        for (int g = 0; g < rows / 8; ++g)
+          for (int r8 = 0; r8 < 8; ++r8)
+            for (int k8 = 0; k8 < 8; ++k8) {
+              const int row = m0 + g * 8 + r8, k = sl * qd::kTcK + c * 8 + k8;
+              double v = 0.0;
+              if (row < n && k < n) {
+                // sin(pi (row+1)(k+1)/(n+1)) with the angle reduced exactly in integers
+                const int64_t q = (int64_t(row + 1) * (k + 1)) % (2 * int64_t(n + 1));
+                v = scale * std::sin(M_PI * double(q) / double(n + 1));
+              }
+              h_out[pos++] = bf16_bits(v);
+            }
+  }
+  return QD_OK;
+}
+
 extern "C" int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int b,
                                              const qd_dst_prec *h_prec, size_t *bytes) {
   if (n_dots <= 0 || !h_row_off || !h_prec || !bytes || b < 4) return QD_ERR_INVALID;
   int64_t ntx = 0, nty = 0;
   qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);
-  ar.take<double>(size_t(h_row_off[n_dots]) * b);
-  ar.take<double>(size_t(h_row_off[n_dots]) * b);
-  ar.take<qd_dst_prec>(n_dots);
-  ar.take<int32_t>(n_dots + 1);
-  ar.take<qd::GemmTile>(ntx);
-  ar.take<qd::GemmTile>(nty);
+  void *t1, *t2;
+  qd_dst_prec *desc;
+  int32_t *ro;
+  qd::GemmTile *dtx, *dty;
+  int *err;
+  carve_precond(ar, n_dots, int64_t(h_row_off[n_dots]) * b, ntx, nty, &t1, &t2, &desc, &ro,
+                &dtx, &dty, &err);
   *bytes = ar.used;
   return QD_OK;
 }
 
 extern "C" int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, int b, int vec_fp32,
-                                    const qd_dst_prec *h_prec, const double *d_prec_mats,
+                                    const qd_dst_prec *h_prec, const void *d_prec_mats,
                                     const void *d_in, void *d_out, void *d_work,
                                     size_t work_bytes, void *stream) {
   if (n_dots <= 0 || !h_row_off || !h_prec || !d_prec_mats || !d_in || !d_out || !d_work || b < 4)
     return QD_ERR_INVALID;
+  if (reinterpret_cast<uintptr_t>(d_prec_mats) % 16) return QD_ERR_INVALID;
   for (int d = 0; d < n_dots; ++d) {
     const qd_dst_prec &q = h_prec[d];
-    if (q.nx > 0 && int64_t(q.nx) * q.ny != h_row_off[d + 1] - h_row_off[d]) return QD_ERR_INVALID;
+    if (q.nx > 0 && (int64_t(q.nx) * q.ny != h_row_off[d + 1] - h_row_off[d] ||
+                     q.sx_off < 0 || q.sy_off < 0 || q.sx_off % 8 || q.sy_off % 8))
+      return QD_ERR_INVALID;
   }
   size_t need = 0;
   int st = qd_dst_precond_workspace_size(n_dots, h_row_off, b, h_prec, &need);
   if (st != QD_OK) return st;
   if (need > work_bytes || reinterpret_cast<uintptr_t>(d_work) % 256) return QD_ERR_WORKSPACE;
   int64_t ntx = 0, nty = 0;
+  int rows_x = 16, rows_y = 16;
   qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   std::vector<qd::GemmTile> tx(ntx), ty(nty);
-  qd::dst_tiles(n_dots, h_prec, b, tx.data(), &ntx, ty.data(), &nty);
+  qd::dst_tiles(n_dots, h_prec, b, tx.data(), &ntx, ty.data(), &nty, &rows_x, &rows_y);
   qd::Arena ar(d_work, work_bytes);
-  const size_t nv = size_t(h_row_off[n_dots]) * b;
-  double *t1 = ar.take<double>(nv), *t2 = ar.take<double>(nv);
-  qd_dst_prec *desc = ar.take<qd_dst_prec>(n_dots);
-  int32_t *ro = ar.take<int32_t>(n_dots + 1);
-  qd::GemmTile *dtx = ar.take<qd::GemmTile>(ntx), *dty = ar.take<qd::GemmTile>(nty);
+  void *t1, *t2;
+  qd_dst_prec *desc;
+  int32_t *ro;
+  qd::GemmTile *dtx, *dty;
+  int *err;
+  carve_precond(ar, n_dots, int64_t(h_row_off[n_dots]) * b, ntx, nty, &t1, &t2, &desc, &ro,
+                &dtx, &dty, &err);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   QD_CUDA_TRY(cudaMemcpyAsync(desc, h_prec, n_dots * sizeof(qd_dst_prec), cudaMemcpyHostToDevice, s));
   QD_CUDA_TRY(cudaMemcpyAsync(ro, h_row_off, (n_dots + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   if (ntx) QD_CUDA_TRY(cudaMemcpyAsync(dtx, tx.data(), ntx * sizeof(qd::GemmTile), cudaMemcpyHostToDevice, s));
   if (nty) QD_CUDA_TRY(cudaMemcpyAsync(dty, ty.data(), nty * sizeof(qd::GemmTile), cudaMemcpyHostToDevice, s));
+  QD_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+  const uint16_t *mats = static_cast<const uint16_t *>(d_prec_mats);
   cudaError_t e;
   if (vec_fp32)
-    e = qd::dst_apply<float>(dtx, ntx, dty, nty, nullptr, 0, desc, ro, d_prec_mats, b,
-                             static_cast<const float *>(d_in), static_cast<float *>(d_out),
-                             reinterpret_cast<float *>(t1), reinterpret_cast<float *>(t2), s);
+    e = qd::dst_apply<float>(dtx, ntx, rows_x, dty, nty, rows_y, nullptr, 0, desc, ro, mats, b,
+                             static_cast<const float *>(d_in), static_cast<float *>(d_out), t1,
+                             t2, err, s);
   else
-    e = qd::dst_apply<double>(dtx, ntx, dty, nty, nullptr, 0, desc, ro, d_prec_mats, b,
-                              static_cast<const double *>(d_in), static_cast<double *>(d_out), t1, t2, s);
+    e = qd::dst_apply<double>(dtx, ntx, rows_x, dty, nty, rows_y, nullptr, 0, desc, ro, mats, b,
+                              static_cast<const double *>(d_in), static_cast<double *>(d_out),
+                              t1, t2, err, s);
   if (e != cudaSuccess) return QD_ERR_CUDA;
+  int herr = 0;
+  QD_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
   QD_CUDA_TRY(cudaStreamSynchronize(s));   // host tile tables die at return
-  return QD_OK;
+  return herr ? QD_ERR_TIMEOUT : QD_OK;
 }

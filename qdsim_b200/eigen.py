@@ -56,10 +56,24 @@ def workspace_bytes(n_dots: int, n_rows: int, b: int, prec: int, h_prec=None) ->
     return int(out.value)
 
 
+def dst_matrix_bf16(n: int) -> np.ndarray:
+    """DST-I matrix of lattice size n in the tensor-core operand layout
+    (``qd_dst_matrix_fill``; BF16 bit patterns as uint16)."""
+    L = N.lib()
+    elems = C.c_int64()
+    N.check(L.qd_dst_matrix_size(int(n), C.byref(elems)), "qd_dst_matrix_size")
+    out = np.empty(elems.value, dtype=np.uint16)
+    N.check(L.qd_dst_matrix_fill(int(n), N.ptr(out)), "qd_dst_matrix_fill")
+    return out
+
+
 class DSTPreconditioner:
     """Per-dot fast-sine-transform preconditioner data (host descriptors and
-    device DST-I matrices) for structured rectangular meshes with Dirichlet
-    elimination; dots without a lattice get nx = 0 (unpreconditioned)."""
+    device BF16 DST-I matrices) for structured rectangular meshes with
+    Dirichlet elimination; dots without a lattice get nx = 0
+    (unpreconditioned)."""
+
+    _MATS: dict = {}      # lattice size -> host matrix (shared by all instances)
 
     def __init__(self, specs, device):
         """specs: per dot (nx, ny, cx, cy, shift) or None."""
@@ -67,18 +81,19 @@ class DSTPreconditioner:
         sizes = sorted({s[i] for s in specs if s is not None for i in (0, 1)})
         offs, mats, pos = {}, [], 0
         for n in sizes:
-            j = np.arange(1, n + 1)
-            S = np.sqrt(2.0 / (n + 1)) * np.sin(np.pi * np.outer(j, j) / (n + 1))
+            if n not in self._MATS:
+                self._MATS[n] = dst_matrix_bf16(n)
+            m = self._MATS[n]
             offs[n] = pos
-            mats.append(S.ravel())
-            pos += S.size
+            mats.append(m)
+            pos += m.size
         for d, s in enumerate(specs):
             if s is None:
                 continue
             nx, ny, cx, cy, shift = s
             self.desc[d] = (nx, ny, offs[nx], offs[ny], cx, cy, shift, 0)
-        flat = np.concatenate(mats) if mats else np.zeros(1, np.float64)
-        self.d_mats = torch.from_numpy(flat).to(device)
+        flat = np.concatenate(mats) if mats else np.zeros(8, np.uint16)
+        self.d_mats = torch.from_numpy(flat.view(np.int16)).to(device)
 
     #: Diagonal shift of the preconditioner in eV (times the lattice cell area).
     #: The preconditioner only models the kinetic operator, so a small positive

@@ -30,7 +30,7 @@ def test_status_strings_and_version():
     from qdsim_b200 import _native as N
     L = N.lib()
     assert b"sm_100a" in L.qd_version()
-    for st in (0, -1, -2, -3, -4, -5, -6, -7):
+    for st in (0, -1, -2, -3, -4, -5, -6, -7, -8):
         assert L.qd_status_string(st) and L.qd_status_string(st) != b"unknown status"
 
 
@@ -51,6 +51,34 @@ def test_invalid_arguments_rejected_without_gpu():
                              1e-9, 10, 1, *([C.c_void_p(8)] * 4), N.ptr(info), None,
                              C.c_void_p(256), 1 << 20, None) == N.QD_ERR_INVALID
     assert L.qd_pcg_solve_static(0, 1, *([None] * 6), 1e-9, 10, None, None, None) == N.QD_ERR_INVALID
+
+
+@pytest.mark.parametrize("n", [1, 5, 16, 63, 64, 65, 479, 600])
+def test_dst_matrix_layout(n):
+    """qd_dst_matrix_fill writes the BF16-rounded DST-I matrix in the
+    tensor-core operand layout: undo the layout and compare element-wise."""
+    from dst_emul import bf16, dst_matrix
+    from qdsim_b200 import eigen as G
+    m = G.dst_matrix_bf16(n)
+    R, KS = (n + 15) // 16 * 16, (n + 63) // 64
+    assert m.size == R * KS * 64
+    full = np.zeros((R, KS * 64))
+    pos = 0
+    for m0 in range(0, R, 512):
+        rows = min(512, R - m0)
+        blk = m[pos:pos + rows * KS * 64].astype(np.uint32) << 16
+        blk = blk.view(np.float32).astype(np.float64)
+        # [slab][chunk][row group][row in group][k in chunk]
+        a = blk.reshape(KS, 8, rows // 8, 8, 8).transpose(2, 3, 0, 1, 4)
+        full[m0:m0 + rows] = a.reshape(rows, KS * 64)
+        pos += rows * KS * 64
+    want = np.zeros_like(full)
+    want[:n, :n] = bf16(dst_matrix(n))
+    # the fill reduces the sine's angle exactly (exact zeros where numpy's
+    # sine leaves ~1e-16); a BF16 tie may round apart
+    ulp = np.abs(want) * 2.0 ** -7 + 1e-12
+    assert np.all(np.abs(full - want) <= ulp)
+    assert np.mean(np.abs(full - want) <= 1e-12) > 0.999
 
 
 @pytest.mark.parametrize("order", [1, 2, 3])
