@@ -221,27 +221,37 @@ template <int B> struct GramCfg {
   static constexpr int THREADS = ((NT * RG + 31) / 32) * 32;
 };
 
+// Shared-memory pipeline of the Gram kernel: each sub-tile of SUB rows holds
+// the 9 vector blocks X W P HX HW HP MX MW MP (each SUB x B, row-major, a
+// contiguous range of the global block), fetched by 9 one-dimensional bulk
+// copies that complete on the stage's mbarrier.  STAGES sub-tiles are in
+// flight while the threads multiply the current one.
+template <typename TV, int B> struct GramPipe {
+  static constexpr int SUB = sizeof(TV) == 8 ? 32 : 64;
+  static constexpr int BLK = SUB * B;               // elements of one block in one stage
+  static constexpr int STAGE = 9 * BLK;             // elements per stage
+  static constexpr int STAGES = 3;
+  static constexpr size_t BAR_OFF = size_t(STAGES) * STAGE * sizeof(TV);
+  static constexpr size_t BYTES = BAR_OFF + 64;
+};
+
 // Each thread owns one upper-triangle 4x4 block (bi <= bj) of both S^T HS and
-// S^T MS for a slice of the sub-tile's rows; the 9 vector blocks of a 64-row
-// sub-tile are staged in shared memory with 16-byte loads.  Off-diagonal
-// blocks are written to both (bi, bj) and (bj, bi), so the per-chunk partial
-// holds the full symmetric matrices.
+// S^T MS for a slice (row group rg) of every sub-tile's rows, accumulating
+// in TV within a sub-tile and in FP64 across sub-tiles.  Off-diagonal blocks
+// are written to both (bi, bj) and (bj, bi), so the per-chunk partial holds
+// the full symmetric matrices.
 template <typename TV, int B>
 __global__ void __launch_bounds__(GramCfg<B>::THREADS)
 gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, const TV *P,
             const TV *HX, const TV *HW, const TV *HP, const TV *MX, const TV *MW, const TV *MP,
-            double *partial) {
+            double *partial, int *wait_err) {
   using C = GramCfg<B>;
+  using PP = GramPipe<TV, B>;
   constexpr int m = C::m, NB = C::NB, NT = C::NT, RG = C::RG;
-  constexpr int SUB = sizeof(TV) == 8 ? 32 : 64;              // rows staged per sub-tile
-  constexpr int LD = m + 4;                                   // padded row (elements)
-  constexpr int STAGE_BYTES = 3 * SUB * LD * int(sizeof(TV));
-  constexpr int RED_BYTES = (RG > 1) ? NT * 32 * 8 : 8;
-  constexpr int RAW = STAGE_BYTES > RED_BYTES ? STAGE_BYTES : RED_BYTES;
-  __shared__ __align__(16) unsigned char raw[RAW];
-  TV *sS = reinterpret_cast<TV *>(raw);
-  TV *sH = sS + SUB * LD;
-  TV *sM = sH + SUB * LD;
+  constexpr int SUB = PP::SUB, BLK = PP::BLK, STAGE = PP::STAGE, STAGES = PP::STAGES;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  TV *stage = reinterpret_cast<TV *>(dsm);
+  uint64_t *full = reinterpret_cast<uint64_t *>(dsm + PP::BAR_OFF);
 
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].run[sizeof(TV) == 8]) return;
@@ -257,32 +267,42 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
     ++bi;
   }
   const int bj = bi + rem;
+  // element offsets of this thread's 4 columns inside a stage (B % 4 == 0,
+  // so a group of 4 columns never straddles two blocks)
+  const int offS = ((4 * bi) / B) * BLK + (4 * bi) % B;
+  const int offH = (3 + (4 * bj) / B) * BLK + (4 * bj) % B;
+  const int offM = (6 + (4 * bj) / B) * BLK + (4 * bj) % B;
   double aH[4][4], aM[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) aH[a][b] = aM[a][b] = 0.0;
 
-  const TV *srcs[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
-  constexpr int VEC = 16 / int(sizeof(TV));                  // elements per 16-byte load
-  for (int r0 = ch.begin; r0 < ch.end; r0 += SUB) {
-    const int nr = min(SUB, ch.end - r0);
+  const int nsub = (ch.end - ch.begin + SUB - 1) / SUB;
+  if (tid == 0) {
+    for (int i = 0; i < STAGES; ++i) qd::tc::mbar_init(&full[i], 1);
+    qd::tc::fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int i) {   // thread 0: bulk copies of sub-tile i
+    const TV *srcs[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
+    const int sst = i % STAGES;
+    const int r0 = ch.begin + i * SUB;
+    const uint32_t bytes = uint32_t(min(SUB, ch.end - r0)) * B * sizeof(TV);
+    qd::tc::mbar_arrive_expect_tx(&full[sst], 9 * bytes);
 #pragma unroll
-    for (int a = 0; a < 9; ++a) {
-      TV *dst = (a < 3 ? sS : a < 6 ? sH : sM) + (a % 3) * B;
-      const TV *src = srcs[a] + size_t(r0) * B;
-      for (int v = tid; v < SUB * B / VEC; v += blockDim.x) {
-        const int e = v * VEC, row = e / B, col = e % B;   // B % VEC == 0
-        if (row < nr) {
-          const float4 q = *reinterpret_cast<const float4 *>(src + e);
-          *reinterpret_cast<float4 *>(dst + row * LD + col) = q;
-        } else {
-          *reinterpret_cast<float4 *>(dst + row * LD + col) = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      }
-    }
-    __syncthreads();
-    if (worker) {
+    for (int a = 0; a < 9; ++a)
+      qd::tc::bulk_g2s(stage + sst * STAGE + a * BLK, srcs[a] + size_t(r0) * B, bytes, &full[sst]);
+  };
+  if (tid == 0)
+    for (int i = 0; i < min(STAGES, nsub); ++i) issue(i);
+  bool fail = false;
+  for (int i = 0; i < nsub; ++i) {
+    const int sst = i % STAGES;
+    const int nr = min(SUB, ch.end - (ch.begin + i * SUB));
+    if (!qd::tc::mbar_wait(&full[sst], (i / STAGES) & 1, qd::kTcWaitNs)) fail = true;
+    if (worker && !fail) {
+      const TV *sb = stage + sst * STAGE;
       TV tH[4][4], tM[4][4];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
@@ -292,9 +312,9 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
         TV sa[4], hb[4], mb[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          sa[a] = sS[row * LD + 4 * bi + a];
-          hb[a] = sH[row * LD + 4 * bj + a];
-          mb[a] = sM[row * LD + 4 * bj + a];
+          sa[a] = sb[offS + row * B + a];
+          hb[a] = sb[offH + row * B + a];
+          mb[a] = sb[offM + row * B + a];
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a)
@@ -312,11 +332,21 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
           aM[a][b] += double(tM[a][b]);
         }
     }
-    __syncthreads();
+    __syncthreads();   // stage sst fully consumed
+    if (tid == 0 && !fail && i + STAGES < nsub) issue(i + STAGES);
+  }
+  if (__syncthreads_or(fail)) {
+    if (tid == 0) {
+      atomicOr(wait_err, 1);
+      // let the copies this CTA issued land before its shared memory is released
+      for (int i = max(0, nsub - STAGES); i < nsub; ++i)
+        qd::tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, qd::kTcWaitNs);
+    }
+    return;
   }
   double *out = partial + size_t(blockIdx.x) * 2 * m * m;
   if (RG > 1) {
-    double *red = reinterpret_cast<double *>(raw);
+    double *red = reinterpret_cast<double *>(dsm);   // NT * 32 doubles < one stage
     for (int g = 1; g < RG; ++g) {
       if (worker && rg == g) {
 #pragma unroll
@@ -952,7 +982,7 @@ struct Layout {
   int64_t ntx, nty;
   int rows_x, rows_y;    // largest TMEM row block of the x / y passes
   const uint16_t *mats;
-  int *dst_err;          // set by a transform kernel whose wait ran out
+  int *wait_err;         // set by a kernel whose bounded wait ran out
 };
 
 size_t rr_smem_bytes(int B) {
@@ -974,6 +1004,7 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t
   L.gramsum = ar.take<double>(size_t(n_dots) * 2 * m * m);
   L.norms = ar.take<double>(size_t(nchunks) * 2 * B);
   L.count = ar.take<int>(4);
+  L.wait_err = ar.take<int>(1);
   for (int i = 0; i < 9; ++i) L.slot[i] = ar.take<double>(size_t(n_rows) * B);
   for (int i = 0; i < 9; ++i) L.slot32[i] = mixed ? ar.take<float>(size_t(n_rows) * B) : nullptr;
   L.nchunks = nchunks;
@@ -987,12 +1018,10 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t
     L.desc = ar.take<qd_dst_prec>(n_dots);
     L.tiles_x = ar.take<qd::GemmTile>(ntx);
     L.tiles_y = ar.take<qd::GemmTile>(nty);
-    L.dst_err = ar.take<int>(1);
   } else {
     L.tmp1 = L.tmp2 = nullptr;
     L.desc = nullptr;
     L.tiles_x = L.tiles_y = nullptr;
-    L.dst_err = nullptr;
   }
   return QD_OK;
 }
@@ -1035,7 +1064,7 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
     cudaError_t e = qd::dst_apply<TV>(L.tiles_x, L.ntx, L.rows_x, L.tiles_y, L.nty, L.rows_y,
                                       &L.st[0].run[PH], int(sizeof(DotState) / sizeof(int)),
                                       L.desc, L.row_off, L.mats, B, b.W, b.W, L.tmp1, L.tmp2,
-                                      L.dst_err, s);
+                                      L.wait_err, s);
     qd::prof_end(qd::PK_PRECOND, s);
     if (e != cudaSuccess) return QD_ERR_CUDA;
   }
@@ -1055,8 +1084,17 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_GRAM, s);
-  gram_kernel<TV, B><<<L.nchunks, GC::THREADS, 0, s>>>(L.chunks, L.st, b.X, b.W, b.P, b.HX, b.HW,
-                                                       b.HP, b.MX, b.MW, b.MP, L.partial);
+  {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+      attr = cudaFuncSetAttribute(gram_kernel<TV, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(GramPipe<TV, B>::BYTES));
+    });
+    if (attr != cudaSuccess) return QD_ERR_CUDA;
+  }
+  gram_kernel<TV, B><<<L.nchunks, GC::THREADS, GramPipe<TV, B>::BYTES, s>>>(
+      L.chunks, L.st, b.X, b.W, b.P, b.HX, b.HW, b.HP, b.MX, b.MW, b.MP, L.partial, L.wait_err);
   QD_CHECK_LAUNCH();
   // the Gram sums of this phase's dots land in L.dotsum; the other phase's
   // dots are reduced by their own sequence (their partial chunks differ)
@@ -1167,7 +1205,6 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     hty.resize(nty);
     qd::dst_tiles(n_dots, h_prec, B, htx.data(), &ntx, hty.data(), &nty, &L.rows_x, &L.rows_y);
     L.mats = d_mats;
-    QD_CUDA_TRY(cudaMemsetAsync(L.dst_err, 0, sizeof(int), s));
     QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_x, htx.data(), ntx * sizeof(qd::GemmTile),
                                 cudaMemcpyHostToDevice, s));
     QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_y, hty.data(), nty * sizeof(qd::GemmTile),
@@ -1203,6 +1240,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   QD_CUDA_TRY(cudaMemcpyAsync(L.row_off, h_row_off, sizeof(int32_t) * (n_dots + 1),
                               cudaMemcpyHostToDevice, s));
   QD_CUDA_TRY(cudaMemsetAsync(L.theta, 0, sizeof(double) * size_t(n_dots) * B, s));
+  QD_CUDA_TRY(cudaMemsetAsync(L.wait_err, 0, sizeof(int), s));
   QD_CUDA_TRY(cudaMemsetAsync(L.relres, 0, sizeof(double) * size_t(n_dots) * B, s));
   QD_CUDA_TRY(cudaStreamSynchronize(s));   // host staging vectors die at return
 
@@ -1233,11 +1271,10 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   QD_CHECK_LAUNCH();
   QD_CUDA_TRY(cudaMemcpyAsync(st.data(), L.st, st.size() * sizeof(DotState),
                               cudaMemcpyDeviceToHost, s));
-  int dst_err = 0;
-  if (L.dst_err)
-    QD_CUDA_TRY(cudaMemcpyAsync(&dst_err, L.dst_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  int wait_err = 0;
+  QD_CUDA_TRY(cudaMemcpyAsync(&wait_err, L.wait_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   QD_CUDA_TRY(cudaStreamSynchronize(s));
-  if (dst_err) return QD_ERR_TIMEOUT;
+  if (wait_err) return QD_ERR_TIMEOUT;
   int nconv = 0, nbreak = 0;
   for (auto &x : st) {
     nconv += (x.status == 1);
