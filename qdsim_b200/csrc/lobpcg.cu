@@ -39,6 +39,7 @@
 #include "common.h"
 #include "spmm.cuh"
 #include "dstprec.cuh"
+#include "pipe.cuh"
 
 namespace {
 
@@ -213,6 +214,17 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 // Gram partials: per chunk A_c = S^T HS, B_c = S^T MS  (m = 3B, full m x m)
 // ---------------------------------------------------------------------------
 
+// Opt a kernel into `bytes` of dynamic shared memory (once per kernel).
+template <auto Kern>
+cudaError_t smem_attr(size_t bytes) {
+  static std::once_flag once;
+  static cudaError_t e = cudaSuccess;
+  std::call_once(once, [bytes] {
+    e = cudaFuncSetAttribute(Kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  });
+  return e;
+}
+
 template <int B> struct GramCfg {
   static constexpr int m = 3 * B;
   static constexpr int NB = m / 4;
@@ -221,19 +233,9 @@ template <int B> struct GramCfg {
   static constexpr int THREADS = ((NT * RG + 31) / 32) * 32;
 };
 
-// Shared-memory pipeline of the Gram kernel: each sub-tile of SUB rows holds
-// the 9 vector blocks X W P HX HW HP MX MW MP (each SUB x B, row-major, a
-// contiguous range of the global block), fetched by 9 one-dimensional bulk
-// copies that complete on the stage's mbarrier.  STAGES sub-tiles are in
-// flight while the threads multiply the current one.
-template <typename TV, int B> struct GramPipe {
-  static constexpr int SUB = sizeof(TV) == 8 ? 32 : 64;
-  static constexpr int BLK = SUB * B;               // elements of one block in one stage
-  static constexpr int STAGE = 9 * BLK;             // elements per stage
-  static constexpr int STAGES = 3;
-  static constexpr size_t BAR_OFF = size_t(STAGES) * STAGE * sizeof(TV);
-  static constexpr size_t BYTES = BAR_OFF + 64;
-};
+// The Gram kernel streams the 9 vector blocks X W P HX HW HP MX MW MP of each
+// sub-tile through a 3-stage bulk-copy pipeline.
+template <typename TV, int B> using GramPipe = qd::BlockPipe<TV, B, 9, (sizeof(TV) == 8 ? 32 : 64), 3>;
 
 // Each thread owns one upper-triangle 4x4 block (bi <= bj) of both S^T HS and
 // S^T MS for a slice (row group rg) of every sub-tile's rows, accumulating
@@ -248,10 +250,8 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
   using C = GramCfg<B>;
   using PP = GramPipe<TV, B>;
   constexpr int m = C::m, NB = C::NB, NT = C::NT, RG = C::RG;
-  constexpr int SUB = PP::SUB, BLK = PP::BLK, STAGE = PP::STAGE, STAGES = PP::STAGES;
+  constexpr int BLK = PP::BLK;
   extern __shared__ __align__(128) unsigned char dsm[];
-  TV *stage = reinterpret_cast<TV *>(dsm);
-  uint64_t *full = reinterpret_cast<uint64_t *>(dsm + PP::BAR_OFF);
 
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].run[sizeof(TV) == 8]) return;
@@ -278,31 +278,15 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
 #pragma unroll
     for (int b = 0; b < 4; ++b) aH[a][b] = aM[a][b] = 0.0;
 
-  const int nsub = (ch.end - ch.begin + SUB - 1) / SUB;
-  if (tid == 0) {
-    for (int i = 0; i < STAGES; ++i) qd::tc::mbar_init(&full[i], 1);
-    qd::tc::fence_mbar_init();
-  }
-  __syncthreads();
-  auto issue = [&](int i) {   // thread 0: bulk copies of sub-tile i
-    const TV *srcs[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
-    const int sst = i % STAGES;
-    const int r0 = ch.begin + i * SUB;
-    const uint32_t bytes = uint32_t(min(SUB, ch.end - r0)) * B * sizeof(TV);
-    qd::tc::mbar_arrive_expect_tx(&full[sst], 9 * bytes);
-#pragma unroll
-    for (int a = 0; a < 9; ++a)
-      qd::tc::bulk_g2s(stage + sst * STAGE + a * BLK, srcs[a] + size_t(r0) * B, bytes, &full[sst]);
-  };
-  if (tid == 0)
-    for (int i = 0; i < min(STAGES, nsub); ++i) issue(i);
-  bool fail = false;
-  for (int i = 0; i < nsub; ++i) {
-    const int sst = i % STAGES;
-    const int nr = min(SUB, ch.end - (ch.begin + i * SUB));
-    if (!qd::tc::mbar_wait(&full[sst], (i / STAGES) & 1, qd::kTcWaitNs)) fail = true;
-    if (worker && !fail) {
-      const TV *sb = stage + sst * STAGE;
+  const TV *src[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (worker && ok) {
+      const int nr = pipe.rows(i);
+      const TV *sb = pipe.tile(i, 0);
       TV tH[4][4], tM[4][4];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
@@ -332,18 +316,9 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
           aM[a][b] += double(tM[a][b]);
         }
     }
-    __syncthreads();   // stage sst fully consumed
-    if (tid == 0 && !fail && i + STAGES < nsub) issue(i + STAGES);
+    pipe.release(i, ok);
   }
-  if (__syncthreads_or(fail)) {
-    if (tid == 0) {
-      atomicOr(wait_err, 1);
-      // let the copies this CTA issued land before its shared memory is released
-      for (int i = max(0, nsub - STAGES); i < nsub; ++i)
-        qd::tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, qd::kTcWaitNs);
-    }
-    return;
-  }
+  if (!pipe.finish(ok, wait_err)) return;
   double *out = partial + size_t(blockIdx.x) * 2 * m * m;
   if (RG > 1) {
     double *red = reinterpret_cast<double *>(dsm);   // NT * 32 doubles < one stage
@@ -721,21 +696,20 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
 // Update: X = S Y, P = [W P] Y_wp, HX/HP/MX/MP likewise; W = HX - MX Theta
 // ---------------------------------------------------------------------------
 
-template <int B> struct UpdCfg {
-  static constexpr int R = 256 / B;      // rows per tile
-  static constexpr int THREADS = R * B;
-};
-
 // X = S Y, P = [W P] Y_wp  (S = [X W P]); products are recomputed explicitly
-// at the start of the next iteration.
+// at the start of the next iteration.  X, W, P stream through a bulk-copy
+// pipeline; each thread produces (row, column) outputs of a sub-tile.
+template <typename TV, int B> using UpdPipe = qd::BlockPipe<TV, B, 3, (sizeof(TV) == 8 ? 32 : 64), 4>;
+
 template <typename TV, int B>
-__global__ void __launch_bounds__(UpdCfg<B>::THREADS)
+__global__ void __launch_bounds__(256)
 update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X, const TV *W,
-              TV *P) {
-  constexpr int m = 3 * B, R = UpdCfg<B>::R;
+              TV *P, int *wait_err) {
+  constexpr int m = 3 * B;
+  using PP = UpdPipe<TV, B>;
   using ACC = TV;   // FP32 arithmetic in the FP32 phase, FP64 in the FP64 phase
-  __shared__ ACC sY[m * B];
-  __shared__ TV sIn[R * 3 * B];
+  extern __shared__ __align__(128) unsigned char dsm[];
+  ACC *sY = reinterpret_cast<ACC *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].run[sizeof(TV) == 8]) return;
   const int tid = threadIdx.x;
@@ -744,33 +718,39 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
   const double *Yg = coef + size_t(ch.dot) * m * B;
   for (int i = tid; i < m * B; i += blockDim.x) sY[i] = ACC(Yg[i]);
   const TV *src[3] = {X, W, P};
-  const int row = tid / B, j = tid % B;
-  for (int r0 = ch.begin; r0 < ch.end; r0 += R) {
-    const int nr = min(R, ch.end - r0);
-    __syncthreads();
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (ok) {
+      const int nr = pipe.rows(i), r0 = pipe.row0(i);
+      const TV *tx = pipe.tile(i, 0), *tw = pipe.tile(i, 1), *tp = pipe.tile(i, 2);
+      for (int e = tid; e < nr * B; e += blockDim.x) {
+        const int row = e / B, j = e % B;
+        ACC x = 0, p = 0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-      for (int idx = tid; idx < R * B; idx += blockDim.x) {
-        const int rr_ = idx / B, cc = idx % B;
-        sIn[rr_ * 3 * B + a * B + cc] = (rr_ < nr) ? src[a][size_t(r0 + rr_) * B + cc] : TV(0);
+        for (int q = 0; q < B; ++q) x = fma(ACC(tx[row * B + q]), sY[q * B + j], x);
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+          const ACC v = ACC(tw[row * B + q]) * sY[(B + q) * B + j];
+          x += v;
+          p += v;
+        }
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+          const ACC v = ACC(tp[row * B + q]) * sY[(2 * B + q) * B + j];
+          x += v;
+          p += v;
+        }
+        const size_t o = size_t(r0) * B + e;
+        X[o] = TV(x);
+        P[o] = TV(p);
       }
-    __syncthreads();
-    if (row < nr) {
-      const TV *in = sIn + row * 3 * B;
-      ACC x = 0, p = 0;
-#pragma unroll
-      for (int i = 0; i < B; ++i) x = fma(ACC(in[i]), sY[i * B + j], x);
-#pragma unroll
-      for (int i = B; i < 3 * B; ++i) {
-        const ACC v = ACC(in[i]) * sY[i * B + j];
-        x += v;
-        p += v;
-      }
-      const size_t o = size_t(r0 + row) * B + j;
-      X[o] = TV(x);
-      P[o] = TV(p);
     }
+    pipe.release(i, ok);
   }
+  pipe.finish(ok, wait_err);
 }
 
 // M-orthogonalisation of W and P against X, in memory:
@@ -781,101 +761,142 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
 // elementwise subtraction it stays accurate, whereas inside the small
 // Rayleigh-Ritz problem it would sit below the resolution of the Gram matrix
 // and the iteration stalls.
+template <typename TV, int B> using OgPipe = qd::BlockPipe<TV, B, 3, (sizeof(TV) == 8 ? 32 : 64), 4>;
+template <int B> struct OgCfg {
+  static constexpr int NQ = B / 4;
+  static constexpr int NT = 2 * NQ * NQ;     // 4x4 output blocks of MX^T W and MX^T P
+  static constexpr int RG = 256 / NT;        // row groups
+  static constexpr size_t RED_BYTES = size_t(RG) * NT * 16 * sizeof(double);
+};
+
+// Per chunk: partial = [MX^T W, MX^T P] (B x B each, FP64).  Each thread owns
+// a 4x4 output block for one row group, accumulating in TV within a sub-tile
+// and in FP64 across sub-tiles; the row groups are summed in a fixed order.
 template <typename TV, int B>
 __global__ void __launch_bounds__(256)
 ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const TV *W,
-                  const TV *P, double *partial) {
-  constexpr int SUB = 32;
-  __shared__ TV sM[SUB * B], sW[SUB * B], sP[SUB * B];
+                  const TV *P, double *partial, int *wait_err) {
+  using PP = OgPipe<TV, B>;
+  using C = OgCfg<B>;
+  constexpr int NQ = C::NQ, NT = C::NT, RG = C::RG, NOUT = 2 * B * B;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  double *red = reinterpret_cast<double *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
   if (!sd.run[sizeof(TV) == 8]) return;
-  const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
-  constexpr int NOUT = 2 * B * B;
-  double acc[(NOUT + 255) / 256];
+  const bool worker = tid < NT * RG;
+  const int task = tid % NT, rg = tid / NT;
+  const int which = task / (NQ * NQ), bi = (task % (NQ * NQ)) / NQ, bj = task % NQ;
+  double acc[4][4];
 #pragma unroll
-  for (int q = 0; q < (NOUT + 255) / 256; ++q) acc[q] = 0.0;
-  for (int r0 = ch.begin; r0 < ch.end; r0 += SUB) {
-    const int nr = min(SUB, ch.end - r0);
-    __syncthreads();
-    for (int idx = tid; idx < SUB * B; idx += blockDim.x) {
-      const int rr = idx / B;
-      const size_t o = size_t(r0) * B + idx;
-      sM[idx] = rr < nr ? MX[o] : TV(0);
-      sW[idx] = rr < nr ? W[o] : TV(0);
-      sP[idx] = (rr < nr && with_p) ? P[o] : TV(0);
-    }
-    __syncthreads();
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int q = 0; q < (NOUT + 255) / 256; ++q) {
-      const int e = tid + q * 256;
-      if (e >= NOUT) continue;
-      const int which = e / (B * B), ij = e % (B * B), i = ij / B, j = ij % B;
-      const TV *src = which ? sP : sW;
-      double a = 0.0;
-      for (int rr = 0; rr < nr; ++rr) a = fma(double(sM[rr * B + i]), double(src[rr * B + j]), a);
-      acc[q] += a;
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  const TV *src[3] = {MX, W, P};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (ok && worker) {
+      const int nr = pipe.rows(i);
+      const TV *tm = pipe.tile(i, 0) + 4 * bi, *tr = pipe.tile(i, 1 + which) + 4 * bj;
+      TV t[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) t[a][b] = TV(0);
+      for (int row = rg; row < nr; row += RG) {
+        TV x[4], y[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          x[a] = tm[row * B + a];
+          y[a] = tr[row * B + a];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) t[a][b] = fma(x[a], y[b], t[a][b]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += double(t[a][b]);
     }
+    pipe.release(i, ok);
   }
-  double *out = partial + size_t(blockIdx.x) * NOUT;
+  if (!pipe.finish(ok, wait_err)) return;
+  if (worker) {
 #pragma unroll
-  for (int q = 0; q < (NOUT + 255) / 256; ++q) {
-    const int e = tid + q * 256;
-    if (e < NOUT) out[e] = acc[q];
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) red[(size_t(rg) * NT + task) * 16 + a * 4 + b] = acc[a][b];
+  }
+  __syncthreads();
+  double *out = partial + size_t(blockIdx.x) * NOUT;
+  for (int e = tid; e < NOUT; e += blockDim.x) {
+    const int w = e / (B * B), ij = e % (B * B), i = ij / B, j = ij % B;
+    const int tk = w * NQ * NQ + (i / 4) * NQ + (j / 4), ab = (i % 4) * 4 + (j % 4);
+    double v = 0.0;
+    for (int g = 0; g < RG; ++g) v += red[(size_t(g) * NT + tk) * 16 + ab];
+    out[e] = v;
   }
 }
 
+// W <- W - X C_W;  with P: P <- P - X C_P, HP <- HP - HX C_P, MP <- MP - MX C_P.
+template <typename TV, int B> using OaPipe = qd::BlockPipe<TV, B, 7, (sizeof(TV) == 8 ? 16 : 32), 4>;
+
 template <typename TV, int B>
-__global__ void __launch_bounds__(UpdCfg<B>::THREADS)
+__global__ void __launch_bounds__(256)
 ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, const TV *X,
-                   const TV *HX, const TV *MX, TV *W, TV *P, TV *HP, TV *MP) {
-  constexpr int R = UpdCfg<B>::R;
+                   const TV *HX, const TV *MX, TV *W, TV *P, TV *HP, TV *MP, int *wait_err) {
+  using PP = OaPipe<TV, B>;
   constexpr int NOUT = 2 * B * B;
-  __shared__ TV sC[NOUT];
-  __shared__ TV sIn[R * 3 * B];
+  extern __shared__ __align__(128) unsigned char dsm[];
+  TV *sC = reinterpret_cast<TV *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
   if (!sd.run[sizeof(TV) == 8]) return;
   const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
   for (int e = tid; e < NOUT; e += blockDim.x) sC[e] = TV(csum[size_t(ch.dot) * NOUT + e]);
-  const TV *src[3] = {X, HX, MX};
-  const int row = tid / B, j = tid % B;
-  for (int r0 = ch.begin; r0 < ch.end; r0 += R) {
-    const int nr = min(R, ch.end - r0);
-    __syncthreads();
+  const TV *src[7] = {X, HX, MX, W, P, HP, MP};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (ok) {
+      const int nr = pipe.rows(i), r0 = pipe.row0(i);
+      const TV *tx = pipe.tile(i, 0), *thx = pipe.tile(i, 1), *tmx = pipe.tile(i, 2);
+      const TV *tw = pipe.tile(i, 3), *tp = pipe.tile(i, 4), *thp = pipe.tile(i, 5),
+               *tmp = pipe.tile(i, 6);
+      for (int e = tid; e < nr * B; e += blockDim.x) {
+        const int row = e / B, j = e % B;
+        const size_t o = size_t(r0) * B + e;
+        TV dw = 0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      if (a > 0 && !with_p) break;
-      for (int idx = tid; idx < R * B; idx += blockDim.x) {
-        const int rr = idx / B, cc = idx % B;
-        sIn[rr * 3 * B + a * B + cc] = (rr < nr) ? src[a][size_t(r0 + rr) * B + cc] : TV(0);
-      }
-    }
-    __syncthreads();
-    if (row < nr) {
-      const TV *in = sIn + row * 3 * B;
-      const size_t o = size_t(r0 + row) * B + j;
-      TV dw = 0;
+        for (int q = 0; q < B; ++q) dw = fma(tx[row * B + q], sC[q * B + j], dw);
+        W[o] = tw[e] - dw;
+        if (with_p) {
+          TV dp = 0, dhp = 0, dmp = 0;
 #pragma unroll
-      for (int i = 0; i < B; ++i) dw = fma(in[i], sC[i * B + j], dw);
-      W[o] = W[o] - dw;
-      if (with_p) {
-        TV dp = 0, dhp = 0, dmp = 0;
-#pragma unroll
-        for (int i = 0; i < B; ++i) {
-          const TV c = sC[B * B + i * B + j];
-          dp = fma(in[i], c, dp);
-          dhp = fma(in[B + i], c, dhp);
-          dmp = fma(in[2 * B + i], c, dmp);
+          for (int q = 0; q < B; ++q) {
+            const TV c = sC[B * B + q * B + j];
+            dp = fma(tx[row * B + q], c, dp);
+            dhp = fma(thx[row * B + q], c, dhp);
+            dmp = fma(tmx[row * B + q], c, dmp);
+          }
+          P[o] = tp[e] - dp;
+          HP[o] = thp[e] - dhp;
+          MP[o] = tmp[e] - dmp;
         }
-        P[o] = P[o] - dp;
-        HP[o] = HP[o] - dhp;
-        MP[o] = MP[o] - dmp;
       }
     }
+    pipe.release(i, ok);
   }
+  pipe.finish(ok, wait_err);
 }
 
 // out[d][v] = sum over the chunks of dot d of partial[c * nvals + v], in chunk
@@ -1069,13 +1090,22 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
     if (e != cudaSuccess) return QD_ERR_CUDA;
   }
   qd::prof_begin(qd::PK_ORTHO, s);
-  ortho_gram_kernel<TV, B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, b.MX, b.W, b.P, L.partial);
+  {
+    constexpr size_t bytes = OgPipe<TV, B>::BYTES + OgCfg<B>::RED_BYTES;
+    if (smem_attr<ortho_gram_kernel<TV, B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+    ortho_gram_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, b.MX, b.W, b.P,
+                                                           L.partial, L.wait_err);
+  }
   QD_CHECK_LAUNCH();
   dot_reduce_kernel<<<dim3((2 * B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, PH, L.partial,
                                                                          2 * B * B, L.dotsum);
   QD_CHECK_LAUNCH();
-  ortho_apply_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(
-      L.chunks, L.st, L.dotsum, b.X, b.HX, b.MX, b.W, b.P, b.HP, b.MP);
+  {
+    constexpr size_t bytes = OaPipe<TV, B>::BYTES + 2 * B * B * sizeof(TV);
+    if (smem_attr<ortho_apply_kernel<TV, B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+    ortho_apply_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(
+        L.chunks, L.st, L.dotsum, b.X, b.HX, b.MX, b.W, b.P, b.HP, b.MP, L.wait_err);
+  }
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
@@ -1084,15 +1114,7 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_GRAM, s);
-  {
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-      attr = cudaFuncSetAttribute(gram_kernel<TV, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(GramPipe<TV, B>::BYTES));
-    });
-    if (attr != cudaSuccess) return QD_ERR_CUDA;
-  }
+  if (smem_attr<gram_kernel<TV, B>>(GramPipe<TV, B>::BYTES) != cudaSuccess) return QD_ERR_CUDA;
   gram_kernel<TV, B><<<L.nchunks, GC::THREADS, GramPipe<TV, B>::BYTES, s>>>(
       L.chunks, L.st, b.X, b.W, b.P, b.HX, b.HW, b.HP, b.MX, b.MW, b.MP, L.partial, L.wait_err);
   QD_CHECK_LAUNCH();
@@ -1108,8 +1130,10 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
 template <typename TV, int B>
 int update_step(const Layout &L, const Bufs<TV> &b, cudaStream_t s) {
   qd::prof_begin(qd::PK_UPDATE, s);
-  update_kernel<TV, B><<<L.nchunks, UpdCfg<B>::THREADS, 0, s>>>(L.chunks, L.st, L.coef, b.X, b.W,
-                                                                b.P);
+  constexpr size_t bytes = UpdPipe<TV, B>::BYTES + 3 * B * B * sizeof(TV);
+  if (smem_attr<update_kernel<TV, B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+  update_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, L.coef, b.X, b.W, b.P,
+                                                     L.wait_err);
   qd::prof_end(qd::PK_UPDATE, s);
   QD_CHECK_LAUNCH();
   return QD_OK;

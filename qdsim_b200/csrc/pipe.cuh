@@ -1,0 +1,88 @@
+// Shared-memory streaming of row-major vector blocks (n_rows x B each) for
+// the per-chunk LOBPCG kernels.  A chunk's rows are processed in sub-tiles of
+// SUB rows; one sub-tile of NBLK blocks is NBLK contiguous global ranges,
+// each fetched by a one-dimensional bulk copy (TMA, no multicast) that
+// completes on the stage's mbarrier.  With STAGES stages, STAGES - 1
+// sub-tiles are in flight while the threads work on the current one.
+//
+// Protocol (all threads of the CTA):
+//   pipe.init(dsm, begin, end);            // barriers, prologue copies
+//   for (i = 0; i < pipe.nsub; ++i) {
+//     ok &= pipe.wait(i);                  // bounded wait for sub-tile i
+//     ... read pipe.tile(i, a), pipe.rows(i) ...
+//     pipe.release(i);                     // __syncthreads + next copy
+//   }
+//   pipe.finish(ok, err);                  // uniform failure handling
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "tc.cuh"
+
+namespace qd {
+
+constexpr uint64_t kPipeWaitNs = 1000000000ull;   // 1 s bound on every wait
+
+template <typename TV, int B, int NBLK, int SUB, int STAGES>
+struct BlockPipe {
+  static constexpr int BLK = SUB * B;                 // elements of one block per stage
+  static constexpr int STAGE = NBLK * BLK;            // elements per stage
+  static constexpr size_t BAR_OFF = size_t(STAGES) * STAGE * sizeof(TV);
+  static constexpr size_t BYTES = BAR_OFF + 8 * STAGES;
+
+  TV *stage;
+  uint64_t *full;
+  const TV *const *src;
+  int begin, end, nsub;
+
+  // src: NBLK block base pointers (global, row-major n_rows x B).
+  __device__ void init(unsigned char *dsm, const TV *const *src_, int begin_, int end_) {
+    stage = reinterpret_cast<TV *>(dsm);
+    full = reinterpret_cast<uint64_t *>(dsm + BAR_OFF);
+    src = src_;
+    begin = begin_;
+    end = end_;
+    nsub = (end - begin + SUB - 1) / SUB;
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < STAGES; ++s) tc::mbar_init(&full[s], 1);
+      tc::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < STAGES && i < nsub; ++i) issue(i);
+  }
+  __device__ int rows(int i) const { return min(SUB, end - (begin + i * SUB)); }
+  __device__ int row0(int i) const { return begin + i * SUB; }
+  __device__ const TV *tile(int i, int a) const { return stage + (i % STAGES) * STAGE + a * BLK; }
+  __device__ TV *tile_rw(int i, int a) { return stage + (i % STAGES) * STAGE + a * BLK; }
+
+  __device__ void issue(int i) {   // thread 0
+    const int s = i % STAGES;
+    const uint32_t bytes = uint32_t(rows(i)) * B * sizeof(TV);
+    tc::mbar_arrive_expect_tx(&full[s], NBLK * bytes);
+#pragma unroll
+    for (int a = 0; a < NBLK; ++a)
+      tc::bulk_g2s(stage + s * STAGE + a * BLK, src[a] + size_t(row0(i)) * B, bytes, &full[s]);
+  }
+  __device__ bool wait(int i) {
+    return tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, kPipeWaitNs);
+  }
+  // Every thread is done with sub-tile i: its stage takes sub-tile i + STAGES.
+  __device__ void release(int i, bool ok) {
+    __syncthreads();
+    if (threadIdx.x == 0 && ok && i + STAGES < nsub) issue(i + STAGES);
+  }
+  // Uniform failure handling; returns true when every wait succeeded.  On
+  // failure thread 0 sets *err and waits (bounded) for the copies still in
+  // flight so that the CTA's shared memory is not released under them.
+  __device__ bool finish(bool ok, int *err) {
+    if (!__syncthreads_or(!ok)) return true;
+    if (threadIdx.x == 0) {
+      atomicOr(err, 1);
+      for (int i = nsub - STAGES > 0 ? nsub - STAGES : 0; i < nsub; ++i)
+        tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, kPipeWaitNs);
+    }
+    return false;
+  }
+};
+
+}  // namespace qd
