@@ -177,6 +177,24 @@ def run_reference(args, rank, world):
 # GPU leg
 # ---------------------------------------------------------------------------
 
+def shard_first(rank: int, dots_per_rank: int) -> int:
+    """First dot id of a rank's shard: every rank solves its own dots (weak
+    scaling, no exchange during the solve)."""
+    return rank * dots_per_rank
+
+
+def reduce_over_ranks(ms: float, conv: float, world: int, device):
+    """Job time = max device time over ranks; converged pairs summed."""
+    import torch
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=device)
+    conv_t = torch.tensor([float(conv)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(conv_t, op=dist.ReduceOp.SUM)
+    return float(ms_t.item()), float(conv_t.item())
+
+
 def algorithmic_bytes(hb, counts, k_block):
     """Algorithmic bytes per kernel kind from the per-dot launch counts."""
     nnz = np.asarray(hb.nnz_per_dot, dtype=np.float64)
@@ -215,7 +233,7 @@ def main():
                                 device_id=dev)
     N.lib()
     t_setup = time.perf_counter()
-    dots = W.sweep_batch(args.dots, first=rank * args.dots)
+    dots = W.sweep_batch(args.dots, first=shard_first(rank, args.dots))
     hb = Bt.HostBatch(dots)
     t_setup = time.perf_counter() - t_setup
     db = Bt.DeviceBatch(hb, dev)
@@ -277,13 +295,7 @@ def main():
         maxerr = float(rel.max())
     else:
         conv = int(solver_ok.sum()) * args.k
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    conv_t = torch.tensor([float(conv)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(conv_t, op=dist.ReduceOp.SUM)
-    ms_max = float(ms_t.item())
-    conv_all = float(conv_t.item())
+    ms_max, conv_all = reduce_over_ranks(ms, conv, world, dev)
     value = conv_all / (ms_max / 1000.0)
 
     # ---- roofline of the dominant kernel ------------------------------------

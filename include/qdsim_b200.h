@@ -167,8 +167,8 @@ typedef struct {
  * The initial block is drawn from `seed` (deterministic).  Returns
  * QD_ERR_NOT_CONVERGED if any dot hits max_iter (results still written).
  * ------------------------------------------------------------------------- */
-int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b, int prec_mode,
-                             const qd_dst_prec *h_prec, size_t *bytes);
+int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_total, int b,
+                             int prec_mode, const qd_dst_prec *h_prec, size_t *bytes);
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
                     const int32_t *d_rowptr, const int32_t *d_col,
                     const double *d_H, const double *d_M,

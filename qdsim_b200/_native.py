@@ -46,7 +46,7 @@ SIGNATURES = {
     "qd_assemble": (_int, [_int, _int, _i64, _i64, _i32, _p, _p, _p, _p, _p,
                            _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_spmm_dual": (_int, [_i32, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p]),
-    "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _int, _int, _p, _p]),
+    "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _i64, _int, _int, _p, _p]),
     "qd_lobpcg_solve": (_int, [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _int, _int, _int, _dbl,
                                _int, _u64, _p, _p, _p, _p, _p, _p, _p, _sz, _p]),
     "qd_dst_precond_workspace_size": (_int, [_i32, _p, _int, _p, _p]),

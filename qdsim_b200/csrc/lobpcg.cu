@@ -33,6 +33,7 @@
 // criterion or stagnation, then converts X to FP64 and finishes in FP64.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -50,6 +51,8 @@ constexpr int kStagWindow = 30;     // FP32 iterations without halving the estim
 constexpr double kTol32Floor = 1e-7; // FP32 phase target (estimated rel. eigenvalue error)
 constexpr double kSafety = 1.0;
 constexpr double kRelCap = 1e-2;
+constexpr double kJacobiRel64 = 2e-15;   // relative Jacobi threshold, FP64 phase
+constexpr double kJacobiRel32 = 1e-10;   // FP32 phase
 #ifndef QD_SVQB_TAU64
 #define QD_SVQB_TAU64 1e-12
 #endif
@@ -104,12 +107,38 @@ __global__ void init_kernel(const Chunk *chunks, const int32_t *row_off, uint64_
   }
 }
 
-template <typename TV, int B>
-__global__ void spmm_chunk_kernel(const Chunk *chunks, const DotState *st,
-                                  const int32_t *__restrict__ rowptr,
-                                  const int32_t *__restrict__ col, const double *__restrict__ H,
-                                  const double *__restrict__ M, const TV *__restrict__ X,
-                                  TV *__restrict__ HX, TV *__restrict__ MX) {
+// Largest binary exponents of |H| and |M| (ilogb; zeros do not count).
+__global__ void hm_exponent_kernel(int32_t nnz, const double *__restrict__ H,
+                                   const double *__restrict__ M, int *e2) {
+  int eh = INT_MIN, em = INT_MIN;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x) {
+    const double h = H[p], m = M[p];
+    if (h != 0.0) eh = max(eh, ilogb(h));
+    if (m != 0.0) em = max(em, ilogb(m));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    eh = max(eh, __shfl_xor_sync(0xffffffffu, eh, o));
+    em = max(em, __shfl_xor_sync(0xffffffffu, em, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&e2[0], eh);
+    atomicMax(&e2[1], em);
+  }
+}
+
+// FP32 (H 2^-eh, M 2^-em) pairs of the FP32 phase's SpMMs.
+__global__ void pack_hm32_kernel(int32_t nnz, const double *__restrict__ H,
+                                 const double *__restrict__ M, int eh, int em,
+                                 float2 *__restrict__ hm) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x)
+    hm[p] = make_float2(float(scalbn(H[p], -eh)), float(scalbn(M[p], -em)));
+}
+
+template <typename TV, int B, typename MAT>
+__global__ void __launch_bounds__(64 * (B / 4), 6)
+spmm_chunk_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
+                  const int32_t *__restrict__ col, const MAT A, const TV *__restrict__ X,
+                  TV *__restrict__ HX, TV *__restrict__ MX) {
   constexpr int G = B / 4;
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].run[sizeof(TV) == 8]) return;
@@ -118,17 +147,16 @@ __global__ void spmm_chunk_kernel(const Chunk *chunks, const DotState *st,
   const int sub = threadIdx.x / G, g = threadIdx.x % G;
   const int rpp = blockDim.x / G;
   for (int r = ch.begin + sub; r < ch.end; r += rpp)
-    qd::spmm_row<TV, B, true>(r, g, rowptr, col, H, M, X, HX, MX);
+    qd::spmm_row<TV, B>(r, g, rowptr, col, A, X, HX, MX);
 }
 
 // Explicit products of the current X and P (no drift from implicit updates):
 // HX, MX, HP, MP, the residual W = HX - MX Theta and per-chunk column norms
 // sum r^2 and sum (Mx)^2.  2G threads per row: g < G own X columns, the rest P.
-template <typename TV, int B>
-__global__ void __launch_bounds__(128 * (B / 4))
+template <typename TV, int B, typename MAT>
+__global__ void __launch_bounds__(128 * (B / 4), sizeof(TV) == 4 ? 3 : 2)
 spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
-               const int32_t *__restrict__ col, const double *__restrict__ H,
-               const double *__restrict__ M, const double *__restrict__ theta,
+               const int32_t *__restrict__ col, const MAT A, const double *__restrict__ theta,
                const TV *__restrict__ X, const TV *__restrict__ P, TV *__restrict__ HX,
                TV *__restrict__ MX, TV *__restrict__ HP, TV *__restrict__ MP,
                TV *__restrict__ W, double *__restrict__ norms) {
@@ -148,7 +176,11 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   const int sub = threadIdx.x / G2, gg = threadIdx.x % G2;
   const bool isx = gg < G;
   const int g = isx ? gg : gg - G;
-  double rr[4] = {0, 0, 0, 0}, mm[4] = {0, 0, 0, 0};
+  // FP64 sums of squares (problems posed in SI units have squared residuals
+  // far below FP32's range), kept in this thread's own shared-memory slots
+  double *my_red = s_red + threadIdx.x * 8;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) my_red[c] = 0.0;
   for (int r = ch.begin + sub; r < ch.end; r += RPP) {
     if (!isx && !with_p) {
       double z[4] = {0, 0, 0, 0};
@@ -162,7 +194,8 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 #pragma unroll 4
     for (int p = p0; p < p1; ++p) {
       const int j = __ldg(col + p);
-      const double hv = __ldg(H + p), mv = __ldg(M + p);
+      double hv, mv;
+      A.get(p, hv, mv);
       double x[4];
       qd::V4<TV>::load(src + size_t(j) * B + 4 * g, x);
 #pragma unroll
@@ -179,8 +212,8 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
         // residual from the stored (rounded) products, as the iteration sees them
         const double hq = double(TV(h[c])), mq = double(TV(m[c]));
         res[c] = hq - s_th[4 * g + c] * mq;
-        rr[c] += res[c] * res[c];
-        mm[c] += mq * mq;
+        my_red[2 * c] += res[c] * res[c];
+        my_red[2 * c + 1] += mq * mq;
       }
       qd::V4<TV>::store(HX + o, h);
       qd::V4<TV>::store(MX + o, m);
@@ -191,11 +224,6 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
     }
   }
   // per-chunk column norms (fixed-order reduction over the CTA's rows)
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    s_red[(threadIdx.x * 4 + c) * 2] = rr[c];
-    s_red[(threadIdx.x * 4 + c) * 2 + 1] = mm[c];
-  }
   __syncthreads();
   if (threadIdx.x < B) {
     const int j = threadIdx.x, gj = j / 4, cj = j % 4;
@@ -389,16 +417,25 @@ __device__ inline double cta_sum(double v, double *s_red) {
 // Cyclic Jacobi eigensolver for a symmetric n x n matrix A (leading dimension
 // ld, shared memory) with round-robin pairing; V (ld) receives the
 // eigenvectors as columns, A's diagonal the eigenvalues.  A pair is rotated
-// only while |a_pq| > 2e-15 sqrt(|a_pp a_qq|) (the relative threshold of
-// Demmel and Veselic), so tiny eigenvalues of a scaled SPD Gram matrix come out
-// with high relative accuracy, and |a_pq| > 1e-18 ||A||_F (below that the
-// entry is rounding noise and rotating it only costs sweeps); the sweeps stop
-// when a sweep rotates nothing.
-// Odd n uses a dummy index that is never rotated.  All threads must call it.
-__device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, double *s_c,
-                           double *s_s, int *s_p, int *s_q) {
+// only while |a_pq| > rel sqrt(|a_pp a_qq|) (the relative threshold of
+// Demmel and Veselic: with rel = 2e-15 tiny eigenvalues of a scaled SPD Gram
+// matrix come out with high relative accuracy) and |a_pq| > 1e-18 ||A||_F
+// (below that the entry is rounding noise and rotating it only costs
+// sweeps); the sweeps stop when a sweep rotates nothing.
+// One round = the ne/2 disjoint pairs of the schedule (odd n adds a dummy
+// index that never rotates), in two phases separated by barriers:
+//   (1) pair t computes its rotation R_t from the current a_pp, a_qq, a_pq;
+//   (2) every 2x2 block (t, u), t <= u, becomes R_t^T A_tu R_u in one step
+//       (it depends only on its own old entries and the two rotations; the
+//       annihilated a_pq of a diagonal block is set to 0), mirrored to (u, t),
+//       and V's columns p, q are rotated.
+__device__ void jacobi_cta(double *A, double *V, int n, int ld, double rel, double *s_red,
+                           double *s_c, double *s_s, int *s_p, int *s_q) {
   const int tid = threadIdx.x, nt = blockDim.x;
-  __shared__ int s_rot;
+  // "some pair rotated" flag per sweep, double-buffered: sweep k sets slot
+  // k & 1 and clears the other slot behind a barrier for sweep k + 1
+  __shared__ int s_rot[2];
+  if (tid == 0) s_rot[0] = s_rot[1] = 0;
   for (int idx = tid; idx < n * n; idx += nt) {
     const int i = idx / n, j = idx % n;
     V[i * ld + j] = (i == j) ? 1.0 : 0.0;
@@ -419,12 +456,13 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, d
   __syncthreads();
   const int ne = (n + 1) & ~1;   // even count including the dummy
   if (ne < 2) return;
+  const int np = ne / 2;
+  const int nblk = np * (np + 1) / 2;
   for (int sweep = 0; sweep < 60; ++sweep) {
-    __syncthreads();
-    if (tid == 0) s_rot = 0;
-    __syncthreads();
+    const int cur = sweep & 1;
     for (int round = 0; round < ne - 1; ++round) {
-      if (tid < ne / 2) {
+      // (1) rotations of this round's pairs
+      if (tid < np) {
         int p, q;
         if (tid == 0) {
           p = 0;
@@ -440,17 +478,13 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, d
         if (q < n) {
           const double apq = A[p * ld + q];
           const double app = A[p * ld + p], aqq = A[q * ld + q];
-          if (fabs(apq) > floor_abs && fabs(apq) > 2e-15 * sqrt(fabs(app * aqq))) {
+          if (fabs(apq) > floor_abs && fabs(apq) > rel * sqrt(fabs(app * aqq))) {
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = rsqrt(1.0 + t * t);
             sn = t * c;
-            s_rot = 1;
-          } else {
-            q = -1;
+            s_rot[cur] = 1;
           }
-        } else {
-          q = -1;   // pair with the dummy: no rotation
         }
         s_c[tid] = c;
         s_s[tid] = sn;
@@ -458,32 +492,66 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double *s_red, d
         s_q[tid] = q;
       }
       __syncthreads();
-      const int np = ne / 2;
-      for (int idx = tid; idx < np * n; idx += nt) {   // rows
-        const int t = idx / n, j = idx % n;
-        const int p = s_p[t], q = s_q[t];
-        if (q < 0) continue;
-        const double c = s_c[t], sn = s_s[t];
-        const double a = A[p * ld + j], b = A[q * ld + j];
-        A[p * ld + j] = c * a - sn * b;
-        A[q * ld + j] = sn * a + c * b;
+      // (2) 2x2 blocks (t <= u) of A, then the columns of V
+      if (round == 0 && tid == 0) s_rot[cur ^ 1] = 0;
+      for (int b = tid; b < nblk; b += nt) {
+        int t = 0, rem = b;
+        while (rem >= np - t) {
+          rem -= np - t;
+          ++t;
+        }
+        const int u = t + rem;
+        const int pt = s_p[t], qt = s_q[t], pu = s_p[u], qu = s_q[u];
+        const double ct = s_c[t], st_ = s_s[t], cu = s_c[u], su = s_s[u];
+        if (ct == 1.0 && st_ == 0.0 && cu == 1.0 && su == 0.0) continue;   // nothing rotates
+        const bool qtv = qt < n, quv = qu < n;
+        const double a00 = A[pt * ld + pu];
+        const double a01 = quv ? A[pt * ld + qu] : 0.0;
+        const double a10 = qtv ? A[qt * ld + pu] : 0.0;
+        const double a11 = (qtv && quv) ? A[qt * ld + qu] : 0.0;
+        // rows: [r0; r1] = R_t^T [a0x; a1x] with R = [[c, s], [-s, c]]
+        const double r00 = ct * a00 - st_ * a10, r01 = ct * a01 - st_ * a11;
+        const double r10 = st_ * a00 + ct * a10, r11 = st_ * a01 + ct * a11;
+        // columns: [.. x0, .. x1] R_u
+        double n00 = cu * r00 - su * r01, n01 = su * r00 + cu * r01;
+        double n10 = cu * r10 - su * r11, n11 = su * r10 + cu * r11;
+        if (t == u) {
+          if (st_ != 0.0) n01 = n10 = 0.0;   // the annihilated entry
+          A[pt * ld + pt] = n00;
+          if (qtv) {
+            A[qt * ld + qt] = n11;
+            A[pt * ld + qt] = n01;
+            A[qt * ld + pt] = n10;
+          }
+        } else {
+          A[pt * ld + pu] = n00;
+          A[pu * ld + pt] = n00;
+          if (quv) {
+            A[pt * ld + qu] = n01;
+            A[qu * ld + pt] = n01;
+          }
+          if (qtv) {
+            A[qt * ld + pu] = n10;
+            A[pu * ld + qt] = n10;
+          }
+          if (qtv && quv) {
+            A[qt * ld + qu] = n11;
+            A[qu * ld + qt] = n11;
+          }
+        }
       }
-      __syncthreads();
-      for (int idx = tid; idx < np * n; idx += nt) {   // columns (and V)
+      for (int idx = tid; idx < np * n; idx += nt) {
         const int t = idx / n, i = idx % n;
         const int p = s_p[t], q = s_q[t];
-        if (q < 0) continue;
         const double c = s_c[t], sn = s_s[t];
-        const double a = A[i * ld + p], b = A[i * ld + q];
-        A[i * ld + p] = c * a - sn * b;
-        A[i * ld + q] = sn * a + c * b;
+        if (q >= n || sn == 0.0) continue;
         const double va = V[i * ld + p], vb = V[i * ld + q];
         V[i * ld + p] = c * va - sn * vb;
         V[i * ld + q] = sn * va + c * vb;
       }
       __syncthreads();
     }
-    if (!s_rot) break;
+    if (!s_rot[cur]) break;
   }
   __syncthreads();
 }
@@ -581,6 +649,10 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     if (s_flag) return;
   }
 
+  // Jacobi threshold: the FP32 phase's Gram matrices carry ~1e-7 relative
+  // errors, so resolving the small eigenproblems beyond 1e-10 buys nothing
+  const double jrel = s.phase == 0 ? kJacobiRel32 : kJacobiRel64;
+
   // 2. Gram matrices of the dot (summed over its chunks by dot_reduce_kernel)
   const double *gsum = partial + size_t(d) * 2 * m * m;
   for (int idx = tid; idx < m * m; idx += nt) {
@@ -603,7 +675,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   }
   __syncthreads();
   // 3. SVQB: eigendecompose the scaled basis Gram, keep the well-conditioned span
-  jacobi_cta(sB, sZ, m, m, s_red, s_c, s_s, s_p, s_q);
+  jacobi_cta(sB, sZ, m, m, jrel, s_red, s_c, s_s, s_p, s_q);
   if (tid == 0) {
     double smax = 0.0;
     for (int i = 0; i < m; ++i) smax = fmax(smax, sB[i * m + i]);
@@ -659,7 +731,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   }
   __syncthreads();
   // 4. standard eigenproblem of size r; eigenvectors into sA
-  jacobi_cta(sB, sA, r, m, s_red, s_c, s_s, s_p, s_q);
+  jacobi_cta(sB, sA, r, m, jrel, s_red, s_c, s_s, s_p, s_q);
   if (tid < r) sE[tid] = sB[tid * m + tid];
   __syncthreads();
   if (tid < r) {
@@ -1004,6 +1076,9 @@ struct Layout {
   int rows_x, rows_y;    // largest TMEM row block of the x / y passes
   const uint16_t *mats;
   int *wait_err;         // set by a kernel whose bounded wait ran out
+  float2 *hm32;          // FP32 (H, M) pairs per nonzero (mixed precision only)
+  int *hm_exp;           // largest binary exponents of |H| and |M|
+  double hm_sh, hm_sm;   // 2^exponent: scale of the FP32 pairs
 };
 
 size_t rr_smem_bytes(int B) {
@@ -1011,8 +1086,8 @@ size_t rr_smem_bytes(int B) {
   return size_t(4 * m * m + 2 * m + B) * sizeof(double);
 }
 
-int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t ntx,
-          int64_t nty, bool mixed, Layout &L) {
+int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nchunks,
+          int64_t ntx, int64_t nty, bool mixed, Layout &L) {
   const int m = 3 * B;
   L.chunks = ar.take<Chunk>(nchunks);
   L.row_off = ar.take<int32_t>(n_dots + 1);
@@ -1028,6 +1103,9 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int B, int nchunks, int64_t
   L.wait_err = ar.take<int>(1);
   for (int i = 0; i < 9; ++i) L.slot[i] = ar.take<double>(size_t(n_rows) * B);
   for (int i = 0; i < 9; ++i) L.slot32[i] = mixed ? ar.take<float>(size_t(n_rows) * B) : nullptr;
+  L.hm32 = mixed ? ar.take<float2>(size_t(nnz)) : nullptr;
+  L.hm_exp = ar.take<int>(2);
+  L.hm_sh = L.hm_sm = 1.0;
   L.nchunks = nchunks;
   L.ntx = ntx;
   L.nty = nty;
@@ -1056,6 +1134,18 @@ int count_chunks(int n_dots, const int32_t *row_off) {
   return int(c);
 }
 
+// Matrix values seen by the SpMMs of a phase: interleaved FP32 (H, M) pairs
+// while the vectors are FP32, the caller's FP64 arrays in the FP64 phase.
+template <typename TV> struct MatFor;
+template <> struct MatFor<double> {
+  static qd::MatF64 make(const Layout &, const double *H, const double *M) { return {H, M}; }
+};
+template <> struct MatFor<float> {
+  static qd::MatF32 make(const Layout &L, const double *, const double *) {
+    return {L.hm32, L.hm_sh, L.hm_sm};
+  }
+};
+
 template <typename TV>
 struct Bufs {
   TV *X, *W, *P, *HX, *HW, *HP, *MX, *MW, *MP;
@@ -1075,7 +1165,8 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   constexpr int PH = sizeof(TV) == 8 ? 1 : 0;
   using GC = GramCfg<B>;
   qd::prof_begin(qd::PK_SPMM, s);
-  spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, H, M, L.theta,
+  const auto A = MatFor<TV>::make(L, H, M);
+  spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, L.theta,
                                                       b.X, b.P, b.HX, b.MX, b.HP, b.MP, b.W,
                                                       L.norms);
   qd::prof_end(qd::PK_SPMM, s);
@@ -1109,7 +1200,7 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
-  spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, H, M, b.W,
+  spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, b.W,
                                                         b.HW, b.MW);
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
@@ -1212,16 +1303,36 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     }
     qd::dst_tiles(n_dots, h_prec, B, nullptr, &ntx, nullptr, &nty);
   }
+  int32_t nnz = 0;   // the CSR's own count of nonzeros
+  QD_CUDA_TRY(cudaMemcpyAsync(&nnz, d_rowptr + n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  QD_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nnz <= 0) return QD_ERR_INVALID;
+  const bool mixed_mode = prec_mode == QD_PREC_MIXED;
   {
     qd::Arena need(nullptr, 0);
     Layout tmp;
-    carve(need, n_dots, n_rows, B, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, tmp);
+    carve(need, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, tmp);
     if (need.used > work_bytes) return QD_ERR_WORKSPACE;
   }
   if (reinterpret_cast<uintptr_t>(d_work) % 256 != 0) return QD_ERR_WORKSPACE;
   qd::Arena ar(d_work, work_bytes);
   Layout L;
-  carve(ar, n_dots, n_rows, B, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, L);
+  carve(ar, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, L);
+  if (mixed_mode) {
+    const int init[2] = {INT_MIN, INT_MIN};
+    int e2[2];
+    QD_CUDA_TRY(cudaMemcpyAsync(L.hm_exp, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    hm_exponent_kernel<<<1184, 256, 0, s>>>(nnz, d_H, d_M, L.hm_exp);
+    QD_CHECK_LAUNCH();
+    QD_CUDA_TRY(cudaMemcpyAsync(e2, L.hm_exp, sizeof(e2), cudaMemcpyDeviceToHost, s));
+    QD_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int i = 0; i < 2; ++i)
+      if (e2[i] == INT_MIN) e2[i] = 0;   // all-zero matrix
+    L.hm_sh = std::ldexp(1.0, e2[0]);
+    L.hm_sm = std::ldexp(1.0, e2[1]);
+    pack_hm32_kernel<<<1184, 256, 0, s>>>(nnz, d_H, d_M, e2[0], e2[1], L.hm32);
+    QD_CHECK_LAUNCH();
+  }
   std::vector<qd::GemmTile> htx, hty;
   if (ntx > 0) {
     if (reinterpret_cast<uintptr_t>(d_mats) % 16) return QD_ERR_INVALID;
@@ -1326,17 +1437,20 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
 
 }  // namespace
 
-extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int b,
-                                        int prec_mode, const qd_dst_prec *h_prec,
-                                        size_t *bytes) {
-  if (!bytes || n_dots <= 0 || n_rows_total <= 0 || b < 4 || b > kMaxB || b % 4) return QD_ERR_INVALID;
+extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total,
+                                        int64_t nnz_total, int b, int prec_mode,
+                                        const qd_dst_prec *h_prec, size_t *bytes) {
+  if (!bytes || n_dots <= 0 || n_rows_total <= 0 || nnz_total <= 0 || b < 4 || b > kMaxB ||
+      b % 4)
+    return QD_ERR_INVALID;
   // upper bound on the chunk count: every dot contributes at most one partial chunk
   const int nchunks = int(n_rows_total / kChunkRows) + n_dots;
   int64_t ntx = 0, nty = 0;
   if (h_prec) qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);
   Layout L;
-  carve(ar, n_dots, n_rows_total, b, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED, L);
+  carve(ar, n_dots, n_rows_total, nnz_total, b, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED,
+        L);
   *bytes = ar.used;
   return QD_OK;
 }
@@ -1380,9 +1494,9 @@ __global__ void spmm_plain_kernel(int32_t n, const int32_t *rowptr, const int32_
   const int rpb = blockDim.x / G;
   for (int r = blockIdx.x * rpb + sub; r < n; r += gridDim.x * rpb) {
     if (M && MX)
-      qd::spmm_row<TV, B, true>(r, g, rowptr, col, H, M, X, HX, MX);
+      qd::spmm_row<TV, B>(r, g, rowptr, col, qd::MatF64{H, M}, X, HX, MX);
     else
-      qd::spmm_row<TV, B, false>(r, g, rowptr, col, H, nullptr, X, HX, nullptr);
+      qd::spmv_row<TV, B>(r, g, rowptr, col, H, X, HX);
   }
 }
 

@@ -35,14 +35,59 @@ template <> struct V4<double> {
   }
 };
 
-// One row r, columns [4g, 4g+4): HX = H X, MX = M X (M may be null for a
-// single-matrix product).
-template <typename TV, int B, bool DUAL>
+// Values of the two matrices at a nonzero: separate FP64 arrays, or one
+// interleaved FP32 (H, M) pair per nonzero (8 bytes instead of 16; used while
+// the vectors themselves are stored in FP32).  The FP32 pairs are scaled by
+// powers of two so that the largest magnitudes sit near 1: problems posed in
+// SI units have entries far below FP32's normal range.
+struct MatF64 {
+  const double *H, *M;
+  __device__ void get(int p, double &h, double &m) const {
+    h = __ldg(H + p);
+    m = __ldg(M + p);
+  }
+};
+struct MatF32 {
+  const float2 *HM;   // (H 2^-eh, M 2^-em): scaled into FP32's range
+  double sh, sm;      // 2^eh, 2^em (exact rescaling)
+  __device__ void get(int p, double &h, double &m) const {
+    const float2 v = __ldg(HM + p);
+    h = double(v.x) * sh;
+    m = double(v.y) * sm;
+  }
+};
+
+// One row r, columns [4g, 4g+4): HX = H X, MX = M X.
+template <typename TV, int B, typename MAT>
 __device__ inline void spmm_row(int r, int g, const int32_t *__restrict__ rowptr,
-                                const int32_t *__restrict__ col, const double *__restrict__ H,
-                                const double *__restrict__ M, const TV *__restrict__ X,
-                                TV *__restrict__ HX, TV *__restrict__ MX) {
+                                const int32_t *__restrict__ col, const MAT &A,
+                                const TV *__restrict__ X, TV *__restrict__ HX,
+                                TV *__restrict__ MX) {
   double h[4] = {0.0, 0.0, 0.0, 0.0}, m[4] = {0.0, 0.0, 0.0, 0.0};
+  const int p0 = __ldg(rowptr + r), p1 = __ldg(rowptr + r + 1);
+#pragma unroll 4
+  for (int p = p0; p < p1; ++p) {
+    const int j = __ldg(col + p);
+    double hv, mv;
+    A.get(p, hv, mv);
+    double x[4];
+    V4<TV>::load(X + size_t(j) * B + 4 * g, x);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      h[c] = fma(hv, x[c], h[c]);
+      m[c] = fma(mv, x[c], m[c]);
+    }
+  }
+  V4<TV>::store(HX + size_t(r) * B + 4 * g, h);
+  V4<TV>::store(MX + size_t(r) * B + 4 * g, m);
+}
+
+// Single-matrix variant (qd_spmm_dual with only H).
+template <typename TV, int B>
+__device__ inline void spmv_row(int r, int g, const int32_t *__restrict__ rowptr,
+                                const int32_t *__restrict__ col, const double *__restrict__ H,
+                                const TV *__restrict__ X, TV *__restrict__ HX) {
+  double h[4] = {0.0, 0.0, 0.0, 0.0};
   const int p0 = __ldg(rowptr + r), p1 = __ldg(rowptr + r + 1);
 #pragma unroll 4
   for (int p = p0; p < p1; ++p) {
@@ -52,14 +97,8 @@ __device__ inline void spmm_row(int r, int g, const int32_t *__restrict__ rowptr
     V4<TV>::load(X + size_t(j) * B + 4 * g, x);
 #pragma unroll
     for (int c = 0; c < 4; ++c) h[c] = fma(hv, x[c], h[c]);
-    if (DUAL) {
-      const double mv = __ldg(M + p);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) m[c] = fma(mv, x[c], m[c]);
-    }
   }
   V4<TV>::store(HX + size_t(r) * B + 4 * g, h);
-  if (DUAL) V4<TV>::store(MX + size_t(r) * B + 4 * g, m);
 }
 
 }  // namespace qd

@@ -49,9 +49,9 @@ def pack_block_diagonal(mats):
     return np.asarray(row_off, dtype=np.int32), rowptr, col, H, M
 
 
-def workspace_bytes(n_dots: int, n_rows: int, b: int, prec: int, h_prec=None) -> int:
+def workspace_bytes(n_dots: int, n_rows: int, nnz: int, b: int, prec: int, h_prec=None) -> int:
     out = C.c_size_t()
-    N.check(N.lib().qd_lobpcg_workspace_size(n_dots, n_rows, b, prec, N.ptr(h_prec),
+    N.check(N.lib().qd_lobpcg_workspace_size(n_dots, n_rows, nnz, b, prec, N.ptr(h_prec),
                                              C.byref(out)), "qd_lobpcg_workspace_size")
     return int(out.value)
 
@@ -147,7 +147,7 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
     dev = H.device
     h_prec = precond.desc if precond is not None else None
     d_mats = precond.d_mats if precond is not None else None
-    nbytes = workspace_bytes(n_dots, n_rows, b, prec, h_prec)
+    nbytes = workspace_bytes(n_dots, n_rows, col.numel(), b, prec, h_prec)
     ws = (workspace or Workspace(dev)).get(nbytes)
     X = torch.empty(n_rows * k, dtype=torch.float64, device=dev)
     E = torch.empty(n_dots * k, dtype=torch.float64, device=dev)
