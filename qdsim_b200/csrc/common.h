@@ -20,6 +20,7 @@ extern std::atomic<uint64_t> g_launches;
 enum ProfKind { PK_SPMM = 0, PK_GRAM, PK_RR, PK_UPDATE, PK_ASSEMBLE, PK_PCG, PK_ADJOINT, PK_PRECOND,
                 PK_ORTHO, PK_OTHER, PK_COUNT };
 #ifdef __CUDACC__
+bool prof_enabled();
 void prof_begin(int kind, cudaStream_t s);
 void prof_end(int kind, cudaStream_t s);
 #endif

@@ -190,17 +190,10 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   const uint32_t bstage = lay.b_off[1] - lay.b_off[0];
   int issued = 0;   // slabs whose copy and MMAs thread 0 has issued
   bool fail = false;
-  for (int s = 0; s < KS; ++s) {
-    const int st = s & 1;
-    const uint32_t sA = sA0 + uint32_t(st) * kTcABytes, sB = sB0 + uint32_t(st) * bstage;
-    if (s >= 2 && !tc::mbar_wait(&bar_mma[st], ((s - 2) >> 1) & 1, kTcWaitNs)) fail = true;
-    if (tid == 0 && !fail) {
-      tc::mbar_arrive_expect_tx(&bar_full[st], bbytes);
-      tc::bulk_g2s(sm + lay.b_off[0] + st * bstage, S + size_t(s) * rows * kTcK, bbytes,
-                   &bar_full[st]);
-    }
-    // A slab: this thread's n, k chunks c = cgrp + 2j, 8 consecutive k each
-    float v[4][8];
+  // A slab: this thread's n, k chunks c = cgrp + 2j, 8 consecutive k each;
+  // slab s+1 is loaded into registers while slab s is multiplied
+  float v[4][8];
+  auto load_a = [&](int s) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int kc = s * kTcK + (cgrp + 2 * j) * 8;
@@ -210,6 +203,17 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
         v[j][e] = (nvalid && k < dim) ? to_f32(in[in_base + size_t(k) * in_kstride]) : 0.f;
       }
     }
+  };
+  load_a(0);
+  for (int s = 0; s < KS; ++s) {
+    const int st = s & 1;
+    if (s >= 2 && !tc::mbar_wait(&bar_mma[st], ((s - 2) >> 1) & 1, kTcWaitNs)) fail = true;
+    if (tid == 0 && !fail) {
+      tc::mbar_arrive_expect_tx(&bar_full[st], bbytes);
+      tc::bulk_g2s(sm + lay.b_off[0] + st * bstage, S + size_t(s) * rows * kTcK, bbytes,
+                   &bar_full[st]);
+    }
+    const uint32_t sA = sA0 + uint32_t(st) * kTcABytes, sB = sB0 + uint32_t(st) * bstage;
     uint8_t *a_st = sm + lay.a_off[0] + st * kTcABytes;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -224,6 +228,7 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
       *reinterpret_cast<uint4 *>(a_st + c * (kTcABytes / 8) + (n_loc >> 3) * 128 +
                                  (n_loc & 7) * 16) = pk;
     }
+    if (s + 1 < KS) load_a(s + 1);
     tc::fence_proxy_async_smem();
     fail = __syncthreads_or(fail) != 0;
     if (fail) break;

@@ -35,7 +35,9 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include "common.h"
 #include "spmm.cuh"
@@ -53,6 +55,7 @@ constexpr double kSafety = 1.0;
 constexpr double kRelCap = 1e-2;
 constexpr double kJacobiRel64 = 2e-15;   // relative Jacobi threshold, FP64 phase
 constexpr double kJacobiRel32 = 1e-10;   // FP32 phase
+constexpr double kCholPivot32 = 1e-5;    // smallest Cholesky pivot of the scaled Gram (FP32 phase)
 #ifndef QD_SVQB_TAU64
 #define QD_SVQB_TAU64 1e-12
 #endif
@@ -104,6 +107,18 @@ __global__ void init_kernel(const Chunk *chunks, const int32_t *row_off, uint64_
     const size_t o = size_t(r) * B + j;
     X[o] = TV(u);
     W[o] = P[o] = HW[o] = MW[o] = HP[o] = MP[o] = TV(0);
+  }
+}
+
+// Row sums of the (scaled) FP32 H values, accumulated in FP64: the FP32
+// SpMM differences H against each row's own entry and adds this sum back.
+__global__ void rowsum32_kernel(int64_t n, const int32_t *__restrict__ rowptr,
+                                const float2 *__restrict__ hm, float *__restrict__ rs) {
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    double a = 0.0;
+    for (int p = rowptr[r]; p < rowptr[r + 1]; ++p) a += double(hm[p].x);
+    rs[r] = float(a);
   }
 }
 
@@ -229,6 +244,203 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
     const int j = threadIdx.x, gj = j / 4, cj = j % 4;
     double a = 0.0, b = 0.0;
     for (int sr = 0; sr < RPP; ++sr) {
+      const int t = sr * G2 + gj;
+      a += s_red[(t * 4 + cj) * 2];
+      b += s_red[(t * 4 + cj) * 2 + 1];
+    }
+    norms[size_t(blockIdx.x) * 2 * B + j] = a;
+    norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32-phase SpMM with the CSR streamed through shared memory.
+// Each sub-tile of 64 rows needs the column indices and (H, M) pairs of the
+// nonzero range [rowptr[a], rowptr[b]); both ranges are fetched by 1-D bulk
+// copies (rounded out to 16-byte boundaries; the workspace copies `col32`
+// and `hm32` carry the slack) into a 3-stage mbarrier pipeline, so that the
+// only global access left in the nonzero loop is the gather of a vector row.
+// A sub-tile with more than kCsrCap nonzeros reads the CSR from global memory.
+// XP: products of X and P with the residual W = HX - MX Theta and per-chunk
+// norms; otherwise the products of one block (W -> HW, MW).
+// ---------------------------------------------------------------------------
+constexpr int kCsrSub = 64;                 // rows per sub-tile
+constexpr int kCsrCap = kCsrSub * 20;       // staged nonzeros per sub-tile
+constexpr int kCsrStages = 3;
+struct CsrStage {
+  static constexpr int COL = kCsrCap + 8;   // int32 slots (16-byte rounding slack)
+  static constexpr int HM = kCsrCap + 4;    // float2 slots
+  static constexpr size_t COL_OFF = 0;
+  static constexpr size_t HM_OFF = size_t(kCsrStages) * COL * 4;
+  static constexpr size_t META_OFF = HM_OFF + size_t(kCsrStages) * HM * 8;
+  // barriers, then per stage: col base, hm base, staged flag
+  static constexpr size_t BYTES = META_OFF + kCsrStages * 8 + kCsrStages * 3 * 4;
+};
+
+template <int B, bool XP>
+__global__ void __launch_bounds__(64 * (B / 4) * (XP ? 2 : 1), XP ? 3 : 6)
+spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
+              const int32_t *__restrict__ col32, const float2 *__restrict__ hm32,
+              const float *__restrict__ rs32, double sh, double smv,
+              const double *__restrict__ theta, const float *__restrict__ X,
+              const float *__restrict__ P, float *__restrict__ HX, float *__restrict__ MX,
+              float *__restrict__ HP, float *__restrict__ MP, float *__restrict__ W,
+              double *__restrict__ norms, int *wait_err) {
+  constexpr int G = B / 4;
+  constexpr int G2 = XP ? 2 * G : G;
+  constexpr int NT = kCsrSub * G2;
+  using CS = CsrStage;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  int32_t *s_col = reinterpret_cast<int32_t *>(dsm + CS::COL_OFF);
+  float2 *s_hm = reinterpret_cast<float2 *>(dsm + CS::HM_OFF);
+  uint64_t *full = reinterpret_cast<uint64_t *>(dsm + CS::META_OFF);
+  int *s_cbase = reinterpret_cast<int *>(full + kCsrStages);
+  int *s_hbase = s_cbase + kCsrStages;
+  int *s_staged = s_hbase + kCsrStages;
+  __shared__ double s_th[B];
+  __shared__ double s_red[XP ? NT * 8 : 1];
+
+  const Chunk ch = chunks[blockIdx.x];
+  const DotState &sd = st[ch.dot];
+  if (!sd.run[0]) return;
+  const bool with_p = sd.has_p != 0;
+  const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == sd.chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[0][0]++;
+  if (XP && tid < B) s_th[tid] = theta[size_t(ch.dot) * B + tid];
+  const int sub = tid / G2, gg = tid % G2;
+  const bool isx = gg < G;
+  const int g = isx ? gg : gg - G;
+  double *my_red = XP ? s_red + tid * 8 : nullptr;
+  if (XP) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) my_red[c] = 0.0;
+  }
+  const int nsub = (ch.end - ch.begin + kCsrSub - 1) / kCsrSub;
+  if (tid == 0) {
+    for (int i = 0; i < kCsrStages; ++i) qd::tc::mbar_init(&full[i], 1);
+    qd::tc::fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int i) {   // thread 0
+    const int sst = i % kCsrStages;
+    const int a = ch.begin + i * kCsrSub, b = min(a + kCsrSub, ch.end);
+    const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
+    if (q1 - q0 <= kCsrCap) {
+      const int cb = q0 & ~3, ce = (q1 + 3) & ~3;
+      const int hb = q0 & ~1, he = (q1 + 1) & ~1;
+      s_cbase[sst] = cb;
+      s_hbase[sst] = hb;
+      s_staged[sst] = 1;
+      const uint32_t cbytes = uint32_t(ce - cb) * 4u, hbytes = uint32_t(he - hb) * 8u;
+      qd::tc::mbar_arrive_expect_tx(&full[sst], cbytes + hbytes);
+      if (cbytes) qd::tc::bulk_g2s(s_col + sst * CS::COL, col32 + cb, cbytes, &full[sst]);
+      if (hbytes) qd::tc::bulk_g2s(s_hm + sst * CS::HM, hm32 + hb, hbytes, &full[sst]);
+    } else {
+      s_staged[sst] = 0;
+      qd::tc::mbar_arrive_expect_tx(&full[sst], 0);
+    }
+  };
+  if (tid == 0)
+    for (int i = 0; i < kCsrStages && i < nsub; ++i) issue(i);
+  bool ok = true;
+  for (int i = 0; i < nsub; ++i) {
+    const int sst = i % kCsrStages;
+    const int r = ch.begin + i * kCsrSub + sub;
+    const bool live = r < ch.end;
+    int p0 = 0, p1 = 0;
+    if (live) {
+      p0 = __ldg(rowptr + r);
+      p1 = __ldg(rowptr + r + 1);
+    }
+    ok = qd::tc::mbar_wait(&full[sst], (i / kCsrStages) & 1, qd::kPipeWaitNs) && ok;
+    if (ok && live) {
+      if (XP && !isx && !with_p) {
+        const double z[4] = {0, 0, 0, 0};
+        qd::V4<float>::store(HP + size_t(r) * B + 4 * g, z);
+        qd::V4<float>::store(MP + size_t(r) * B + 4 * g, z);
+      } else {
+        const float *src = (XP && !isx) ? P : X;
+        // FP32 arithmetic, H differenced against the row's own entry:
+        //   (H x)_i = sum_j H_ij (x_j - x_i) + (sum_j H_ij) x_i
+        // The stiffness part of H has (near) zero row sums, so the terms are
+        // small where x is smooth and FP32 accumulation stays ~1e-6 accurate
+        // relative to H x (undifferenced, the terms exceed H x by up to 1e4).
+        const float4 xi = __ldg(reinterpret_cast<const float4 *>(src + size_t(r) * B + 4 * g));
+        float h[4] = {0.f, 0.f, 0.f, 0.f}, m[4] = {0.f, 0.f, 0.f, 0.f};
+        auto row = [&](auto getc, auto getv) {
+#pragma unroll 4
+          for (int p = p0; p < p1; ++p) {
+            const int j = getc(p);
+            const float2 v = getv(p);
+            const float4 xj = __ldg(reinterpret_cast<const float4 *>(src + size_t(j) * B + 4 * g));
+            h[0] = fmaf(v.x, xj.x - xi.x, h[0]);
+            h[1] = fmaf(v.x, xj.y - xi.y, h[1]);
+            h[2] = fmaf(v.x, xj.z - xi.z, h[2]);
+            h[3] = fmaf(v.x, xj.w - xi.w, h[3]);
+            m[0] = fmaf(v.y, xj.x, m[0]);
+            m[1] = fmaf(v.y, xj.y, m[1]);
+            m[2] = fmaf(v.y, xj.z, m[2]);
+            m[3] = fmaf(v.y, xj.w, m[3]);
+          }
+        };
+        if (s_staged[sst]) {
+          const int32_t *cs = s_col + sst * CS::COL;
+          const float2 *hs = s_hm + sst * CS::HM;
+          const int cb = s_cbase[sst], hb = s_hbase[sst];
+          row([&](int p) { return cs[p - cb]; }, [&](int p) { return hs[p - hb]; });
+        } else {
+          row([&](int p) { return __ldg(col32 + p); }, [&](int p) { return __ldg(hm32 + p); });
+        }
+        const float rs = __ldg(rs32 + r);
+        h[0] = fmaf(rs, xi.x, h[0]);
+        h[1] = fmaf(rs, xi.y, h[1]);
+        h[2] = fmaf(rs, xi.z, h[2]);
+        h[3] = fmaf(rs, xi.w, h[3]);
+        const size_t o = size_t(r) * B + 4 * g;
+        // back to the matrices' own scale (powers of two: exact)
+        const float fsh = float(sh), fsm = float(smv);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          h[c] *= fsh;
+          m[c] *= fsm;
+        }
+        if (XP && isx) {
+          double res[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            // residual from the stored (rounded) products, as the iteration sees them
+            const double hq = double(h[c]), mq = double(m[c]);
+            res[c] = hq - s_th[4 * g + c] * mq;
+            my_red[2 * c] += res[c] * res[c];
+            my_red[2 * c + 1] += mq * mq;
+          }
+          *reinterpret_cast<float4 *>(HX + o) = make_float4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<float4 *>(MX + o) = make_float4(m[0], m[1], m[2], m[3]);
+          qd::V4<float>::store(W + o, res);
+        } else {
+          float *oh = XP ? HP : HX, *om = XP ? MP : MX;
+          *reinterpret_cast<float4 *>(oh + o) = make_float4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<float4 *>(om + o) = make_float4(m[0], m[1], m[2], m[3]);
+        }
+      }
+    }
+    __syncthreads();   // stage sst consumed
+    if (tid == 0 && ok && i + kCsrStages < nsub) issue(i + kCsrStages);
+  }
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicOr(wait_err, 1);
+      for (int i = max(0, nsub - kCsrStages); i < nsub; ++i)
+        qd::tc::mbar_wait(&full[i % kCsrStages], (i / kCsrStages) & 1, qd::kPipeWaitNs);
+    }
+    return;
+  }
+  if (XP && tid < B) {
+    // per-chunk column norms (fixed-order reduction over the CTA's rows)
+    const int j = tid, gj = j / 4, cj = j % 4;
+    double a = 0.0, b = 0.0;
+    for (int sr = 0; sr < kCsrSub; ++sr) {
       const int t = sr * G2 + gj;
       a += s_red[(t * 4 + cj) * 2];
       b += s_red[(t * 4 + cj) * 2 + 1];
@@ -458,6 +670,31 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double rel, doub
   if (ne < 2) return;
   const int np = ne / 2;
   const int nblk = np * (np + 1) / 2;
+  // this thread's 2x2 blocks (t <= u) and V tasks (pair t, row i): fixed for
+  // all rounds, decoded once (nblk <= 300 and np * n <= 1152 for n <= 48)
+  constexpr int kBT = 2, kVT = 5;
+  int bt[kBT], bu[kBT], vt[kVT], vi[kVT];
+#pragma unroll
+  for (int q = 0; q < kBT; ++q) {
+    const int b = tid + q * nt;
+    bt[q] = -1;
+    bu[q] = -1;
+    if (b < nblk) {
+      int t = 0, rem = b;
+      while (rem >= np - t) {
+        rem -= np - t;
+        ++t;
+      }
+      bt[q] = t;
+      bu[q] = t + rem;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kVT; ++q) {
+    const int idx = tid + q * nt;
+    vt[q] = idx < np * n ? idx / n : -1;
+    vi[q] = idx < np * n ? idx % n : 0;
+  }
   for (int sweep = 0; sweep < 60; ++sweep) {
     const int cur = sweep & 1;
     for (int round = 0; round < ne - 1; ++round) {
@@ -494,13 +731,10 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double rel, doub
       __syncthreads();
       // (2) 2x2 blocks (t <= u) of A, then the columns of V
       if (round == 0 && tid == 0) s_rot[cur ^ 1] = 0;
-      for (int b = tid; b < nblk; b += nt) {
-        int t = 0, rem = b;
-        while (rem >= np - t) {
-          rem -= np - t;
-          ++t;
-        }
-        const int u = t + rem;
+#pragma unroll
+      for (int qb = 0; qb < kBT; ++qb) {
+        const int t = bt[qb], u = bu[qb];
+        if (t < 0) continue;
         const int pt = s_p[t], qt = s_q[t], pu = s_p[u], qu = s_q[u];
         const double ct = s_c[t], st_ = s_s[t], cu = s_c[u], su = s_s[u];
         if (ct == 1.0 && st_ == 0.0 && cu == 1.0 && su == 0.0) continue;   // nothing rotates
@@ -540,8 +774,10 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double rel, doub
           }
         }
       }
-      for (int idx = tid; idx < np * n; idx += nt) {
-        const int t = idx / n, i = idx % n;
+#pragma unroll
+      for (int qv = 0; qv < kVT; ++qv) {
+        const int t = vt[qv], i = vi[qv];
+        if (t < 0) continue;
         const int p = s_p[t], q = s_q[t];
         const double c = s_c[t], sn = s_s[t];
         if (q >= n || sn == 0.0) continue;
@@ -674,38 +910,106 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     sB[idx] = 0.5 * (sZ[i * m + j] + sZ[j * m + i]) * dd;
   }
   __syncthreads();
-  // 3. SVQB: eigendecompose the scaled basis Gram, keep the well-conditioned span
-  jacobi_cta(sB, sZ, m, m, jrel, s_red, s_c, s_s, s_p, s_q);
-  if (tid == 0) {
-    double smax = 0.0;
-    for (int i = 0; i < m; ++i) smax = fmax(smax, sB[i * m + i]);
-    const double tau = s.phase == 0 ? QD_SVQB_TAU32 : QD_SVQB_TAU64;
-    int r = 0;
-    for (int i = 0; i < m; ++i)
-      if (sB[i * m + i] > tau * smax && smax > 0.0) s_keep[r++] = i;
-    s_r = r;
+  // 3. Orthonormal basis of span[X W P] in the scaled B-inner product, as
+  //    Q (m x r) in sT.  FP32 phase: Cholesky B' = L L^T (outer-product form,
+  //    one barrier per column) and Q = L^-T, as long as every pivot stays above
+  //    kCholPivot32 (the scaled Gram has a unit diagonal, so a pivot is the
+  //    squared distance of a basis vector from the span of the previous ones).
+  //    Otherwise, and always in the FP64 phase: SVQB (Jacobi on B', drop
+  //    directions with S < tau max S, Q = U_keep S_keep^-1/2).
+  bool chol = false;
+  if (s.phase == 0) {
+    const int mu = has_p ? m : 2 * B;
+    bool usable = true;
+    for (int i = 0; i < mu; ++i) usable = usable && sD[i] > 0.0;
+    if (usable) {
+      for (int idx = tid; idx < m * m; idx += nt) sZ[idx] = sB[idx];
+      __syncthreads();
+      bool ok = true;
+      for (int k = 0; k < mu; ++k) {
+        const double piv = sZ[k * m + k];   // final since the previous barrier
+        if (!(piv > kCholPivot32)) {        // every thread reads the same value
+          ok = false;
+          break;
+        }
+        const double ip = 1.0 / piv;
+        const int R = mu - k - 1;
+        for (int idx = tid; idx < R * R; idx += nt) {
+          const int i = k + 1 + idx / R, j = k + 1 + idx % R;
+          if (j <= i) sZ[i * m + j] -= sZ[i * m + k] * sZ[j * m + k] * ip;
+        }
+        __syncthreads();
+      }
+      if (ok) {
+        // L[k][k] = sqrt(piv_k), L[i][k] = sZ[i][k] / sqrt(piv_k); 1/L[k][k] in sE
+        if (tid < mu) sE[tid] = rsqrt(sZ[tid * m + tid]);
+        __syncthreads();
+        for (int idx = tid; idx < mu * mu; idx += nt) {
+          const int i = idx / mu, k = idx % mu;
+          if (k < i) sZ[i * m + k] *= sE[k];
+        }
+        __syncthreads();
+        if (tid < mu) sZ[tid * m + tid] = 1.0 / sE[tid];
+        __syncthreads();
+        // L^-1 (lower) into sB, one column per thread
+        if (tid < mu) {
+          const int j = tid;
+          for (int i = 0; i < j; ++i) sB[i * m + j] = 0.0;
+          sB[j * m + j] = sE[j];
+          for (int i = j + 1; i < mu; ++i) {
+            double sum = 0.0;
+            for (int l = j; l < i; ++l) sum += sZ[i * m + l] * sB[l * m + j];
+            sB[i * m + j] = -sum * sE[i];
+          }
+        }
+        __syncthreads();
+        // Q = L^-T (rows >= mu are unused directions)
+        for (int idx = tid; idx < m * m; idx += nt) {
+          const int i = idx / m, c = idx % m;
+          sT[idx] = (i < mu && c < mu && c >= i) ? sB[c * m + i] : 0.0;
+        }
+        if (tid == 0) s_r = mu;
+        __syncthreads();
+        chol = true;
+      } else {
+        __syncthreads();
+      }
+    }
   }
-  __syncthreads();
-  const int r = s_r;
-  if (r < B || !(r > 0)) {
+  if (!chol) {
+    jacobi_cta(sB, sZ, m, m, jrel, s_red, s_c, s_s, s_p, s_q);
     if (tid == 0) {
-      s.active = 0;
-      s.run[0] = s.run[1] = 0;
-      s.status = 2;
+      double smax = 0.0;
+      for (int i = 0; i < m; ++i) smax = fmax(smax, sB[i * m + i]);
+      const double tau = s.phase == 0 ? QD_SVQB_TAU32 : QD_SVQB_TAU64;
+      int r = 0;
+      for (int i = 0; i < m; ++i)
+        if (sB[i * m + i] > tau * smax && smax > 0.0) s_keep[r++] = i;
+      s_r = r;
     }
-    return;
-  }
-  // Q = U_keep S_keep^-1/2 (m x r) into sT
-  for (int idx = tid; idx < m * m; idx += nt) {
-    const int i = idx / m, c = idx % m;
-    double q = 0.0;
-    if (c < r) {
-      const int kc = s_keep[c];
-      q = sZ[i * m + kc] * rsqrt(sB[kc * m + kc]);
+    __syncthreads();
+    const int r = s_r;
+    if (r < B || !(r > 0)) {
+      if (tid == 0) {
+        s.active = 0;
+        s.run[0] = s.run[1] = 0;
+        s.status = 2;
+      }
+      return;
     }
-    sT[idx] = q;
+    // Q = U_keep S_keep^-1/2 (m x r) into sT
+    for (int idx = tid; idx < m * m; idx += nt) {
+      const int i = idx / m, c = idx % m;
+      double q = 0.0;
+      if (c < r) {
+        const int kc = s_keep[c];
+        q = sZ[i * m + kc] * rsqrt(sB[kc * m + kc]);
+      }
+      sT[idx] = q;
+    }
+    __syncthreads();
   }
-  __syncthreads();
+  const int r = s_r;
   // sZ = A' Q (m x r);  sB = Q^T sZ (r x r)
   for (int idx = tid; idx < m * r; idx += nt) {
     const int i = idx / r, c = idx % r;
@@ -1077,6 +1381,8 @@ struct Layout {
   const uint16_t *mats;
   int *wait_err;         // set by a kernel whose bounded wait ran out
   float2 *hm32;          // FP32 (H, M) pairs per nonzero (mixed precision only)
+  int32_t *col32;        // copy of the column indices with bulk-copy slack (mixed only)
+  float *rs32;           // row sums of the FP32 H values, summed in FP64 (mixed only)
   int *hm_exp;           // largest binary exponents of |H| and |M|
   double hm_sh, hm_sm;   // 2^exponent: scale of the FP32 pairs
 };
@@ -1103,7 +1409,10 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   L.wait_err = ar.take<int>(1);
   for (int i = 0; i < 9; ++i) L.slot[i] = ar.take<double>(size_t(n_rows) * B);
   for (int i = 0; i < 9; ++i) L.slot32[i] = mixed ? ar.take<float>(size_t(n_rows) * B) : nullptr;
-  L.hm32 = mixed ? ar.take<float2>(size_t(nnz)) : nullptr;
+  // +slack: the FP32 SpMM rounds its bulk copies out to 16-byte boundaries
+  L.hm32 = mixed ? ar.take<float2>(size_t(nnz) + 2) : nullptr;
+  L.col32 = mixed ? ar.take<int32_t>(size_t(nnz) + 4) : nullptr;
+  L.rs32 = mixed ? ar.take<float>(size_t(n_rows)) : nullptr;
   L.hm_exp = ar.take<int>(2);
   L.hm_sh = L.hm_sm = 1.0;
   L.nchunks = nchunks;
@@ -1166,9 +1475,16 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   using GC = GramCfg<B>;
   qd::prof_begin(qd::PK_SPMM, s);
   const auto A = MatFor<TV>::make(L, H, M);
-  spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, L.theta,
-                                                      b.X, b.P, b.HX, b.MX, b.HP, b.MP, b.W,
-                                                      L.norms);
+  if constexpr (sizeof(TV) == 4) {
+    if (smem_attr<spmm32_kernel<B, true>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
+    spmm32_kernel<B, true><<<L.nchunks, 128 * G, CsrStage::BYTES, s>>>(
+        L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.X, b.P,
+        b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err);
+  } else {
+    spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A,
+                                                        L.theta, b.X, b.P, b.HX, b.MX, b.HP,
+                                                        b.MP, b.W, L.norms);
+  }
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
   if (L.ntx > 0) {
@@ -1200,8 +1516,15 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
-  spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, b.W,
-                                                        b.HW, b.MW);
+  if constexpr (sizeof(TV) == 4) {
+    if (smem_attr<spmm32_kernel<B, false>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
+    spmm32_kernel<B, false><<<L.nchunks, 64 * G, CsrStage::BYTES, s>>>(
+        L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W,
+        nullptr, b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err);
+  } else {
+    spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, b.W,
+                                                          b.HW, b.MW);
+  }
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_GRAM, s);
@@ -1242,41 +1565,90 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
   const size_t rr_smem = rr_smem_bytes(B);
   QD_CUDA_TRY(cudaFuncSetAttribute(rr_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(rr_smem)));
-  int host_count = n_dots;
-  iters_run = 0;
-  for (int it = 0; it < prm.max_iter + 8; ++it) {
+  // One LOBPCG iteration for every dot (both phases), enqueued on stream q.
+  auto iteration = [&](cudaStream_t q) -> int {
     int st;
     if (mixed) {
       Bufs<float> b32(L.slot32);
-      if ((st = phase_sequence<float, B>(L, b32, n_dots, rowptr, col, H, M, s)) != QD_OK) return st;
+      if ((st = phase_sequence<float, B>(L, b32, n_dots, rowptr, col, H, M, q)) != QD_OK) return st;
     }
-    if ((st = phase_sequence<double, B>(L, b64, n_dots, rowptr, col, H, M, s)) != QD_OK) return st;
-    qd::prof_begin(qd::PK_RR, s);
-    rr_kernel<B><<<n_dots, 256, rr_smem, s>>>(L.st, L.gramsum, L.norms, L.theta, L.coef,
+    if ((st = phase_sequence<double, B>(L, b64, n_dots, rowptr, col, H, M, q)) != QD_OK) return st;
+    qd::prof_begin(qd::PK_RR, q);
+    rr_kernel<B><<<n_dots, 256, rr_smem, q>>>(L.st, L.gramsum, L.norms, L.theta, L.coef,
                                               L.relres, prm);
-    qd::prof_end(qd::PK_RR, s);
+    qd::prof_end(qd::PK_RR, q);
     QD_CHECK_LAUNCH();
     if (mixed) {
       Bufs<float> b32(L.slot32);
-      if ((st = update_step<float, B>(L, b32, s)) != QD_OK) return st;
+      if ((st = update_step<float, B>(L, b32, q)) != QD_OK) return st;
     }
-    if ((st = update_step<double, B>(L, b64, s)) != QD_OK) return st;
+    if ((st = update_step<double, B>(L, b64, q)) != QD_OK) return st;
     if (mixed) {
-      transition_rows_kernel<B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, L.slot32[0], b64.X,
+      transition_rows_kernel<B><<<L.nchunks, 256, 0, q>>>(L.chunks, L.st, L.slot32[0], b64.X,
                                                           b64.W, b64.P, b64.HW, b64.MW, b64.HP,
                                                           b64.MP);
       QD_CHECK_LAUNCH();
-      transition_state_kernel<<<(n_dots + 127) / 128, 128, 0, s>>>(L.st, n_dots);
+      transition_state_kernel<<<(n_dots + 127) / 128, 128, 0, q>>>(L.st, n_dots);
       QD_CHECK_LAUNCH();
     }
-    ++iters_run;
-    if (it % 8 == 7) {
-      count_active_kernel<<<1, 256, 0, s>>>(L.st, n_dots, L.count);
-      QD_CHECK_LAUNCH();
-      QD_CUDA_TRY(cudaMemcpyAsync(&host_count, L.count, sizeof(int), cudaMemcpyDeviceToHost, s));
-      QD_CUDA_TRY(cudaStreamSynchronize(s));
-      if (host_count == 0) break;
+    return QD_OK;
+  };
+  // Iterations run in blocks of kGraphBlock; after each block one host
+  // read of the number of active dots decides whether to stop.  The first
+  // block is enqueued directly (it also sets every kernel's attributes); the
+  // following blocks replay a CUDA graph of one block, captured once on a
+  // private stream and launched into the caller's stream.  Kernel arguments
+  // are the same in every iteration (per-dot progress lives on the device),
+  // so one graph serves all blocks.  With per-kernel timing enabled, or
+  // QD_GRAPHS=0 in the environment, every block is enqueued directly.
+  constexpr int kGraphBlock = 8;
+  const char *genv = std::getenv("QD_GRAPHS");
+  const bool graphs = !qd::prof_enabled() && !(genv && genv[0] == '0');
+  struct GraphGuard {
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~GraphGuard() {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (cap) cudaStreamDestroy(cap);
     }
+  } gg;
+  uint64_t graph_launches = 0;
+  int host_count = n_dots;
+  iters_run = 0;
+  for (int blk = 0; iters_run < prm.max_iter + kGraphBlock; ++blk) {
+    if (blk == 0 || !graphs) {
+      for (int i = 0; i < kGraphBlock; ++i) {
+        const int st = iteration(s);
+        if (st != QD_OK) return st;
+      }
+    } else {
+      if (!gg.exec) {
+        QD_CUDA_TRY(cudaStreamCreateWithFlags(&gg.cap, cudaStreamNonBlocking));
+        const uint64_t l0 = qd::g_launches.load();
+        cudaGraph_t graph = nullptr;
+        QD_CUDA_TRY(cudaStreamBeginCapture(gg.cap, cudaStreamCaptureModeThreadLocal));
+        int st = QD_OK;
+        for (int i = 0; i < kGraphBlock && st == QD_OK; ++i) st = iteration(gg.cap);
+        const cudaError_t ce = cudaStreamEndCapture(gg.cap, &graph);
+        if (st != QD_OK || ce != cudaSuccess) {
+          if (graph) cudaGraphDestroy(graph);
+          return st != QD_OK ? st : QD_ERR_CUDA;
+        }
+        graph_launches = qd::g_launches.load() - l0;   // counted once, for this replay
+        const cudaError_t ie = cudaGraphInstantiate(&gg.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return QD_ERR_CUDA;
+      } else {
+        qd::g_launches.fetch_add(graph_launches, std::memory_order_relaxed);
+      }
+      QD_CUDA_TRY(cudaGraphLaunch(gg.exec, s));
+    }
+    iters_run += kGraphBlock;
+    count_active_kernel<<<1, 256, 0, s>>>(L.st, n_dots, L.count);
+    QD_CHECK_LAUNCH();
+    QD_CUDA_TRY(cudaMemcpyAsync(&host_count, L.count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QD_CUDA_TRY(cudaStreamSynchronize(s));
+    if (host_count == 0) break;
   }
   return QD_OK;
 }
@@ -1331,6 +1703,10 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     L.hm_sh = std::ldexp(1.0, e2[0]);
     L.hm_sm = std::ldexp(1.0, e2[1]);
     pack_hm32_kernel<<<1184, 256, 0, s>>>(nnz, d_H, d_M, e2[0], e2[1], L.hm32);
+    QD_CHECK_LAUNCH();
+    QD_CUDA_TRY(cudaMemcpyAsync(L.col32, d_col, size_t(nnz) * sizeof(int32_t),
+                                cudaMemcpyDeviceToDevice, s));
+    rowsum32_kernel<<<1184, 256, 0, s>>>(n_rows, d_rowptr, L.hm32, L.rs32);
     QD_CHECK_LAUNCH();
   }
   std::vector<qd::GemmTile> htx, hty;

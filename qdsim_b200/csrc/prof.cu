@@ -20,6 +20,11 @@ double g_ms[PK_COUNT] = {0};
 int64_t g_n[PK_COUNT] = {0};
 }  // namespace
 
+bool prof_enabled() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_on;
+}
+
 void prof_begin(int kind, cudaStream_t s) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_on) return;
