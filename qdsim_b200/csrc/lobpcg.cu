@@ -193,9 +193,11 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   const int g = isx ? gg : gg - G;
   // FP64 sums of squares (problems posed in SI units have squared residuals
   // far below FP32's range), kept in this thread's own shared-memory slots
-  double *my_red = s_red + threadIdx.x * 8;
+  // slot layout [8][threads]: consecutive threads hit consecutive banks
+  constexpr int NTX = RPP * G2;
+  double *my_red = s_red + threadIdx.x;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) my_red[c] = 0.0;
+  for (int c = 0; c < 8; ++c) my_red[c * NTX] = 0.0;
   for (int r = ch.begin + sub; r < ch.end; r += RPP) {
     if (!isx && !with_p) {
       double z[4] = {0, 0, 0, 0};
@@ -227,8 +229,8 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
         // residual from the stored (rounded) products, as the iteration sees them
         const double hq = double(TV(h[c])), mq = double(TV(m[c]));
         res[c] = hq - s_th[4 * g + c] * mq;
-        my_red[2 * c] += res[c] * res[c];
-        my_red[2 * c + 1] += mq * mq;
+        my_red[(2 * c) * NTX] += res[c] * res[c];
+        my_red[(2 * c + 1) * NTX] += mq * mq;
       }
       qd::V4<TV>::store(HX + o, h);
       qd::V4<TV>::store(MX + o, m);
@@ -245,8 +247,8 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
     double a = 0.0, b = 0.0;
     for (int sr = 0; sr < RPP; ++sr) {
       const int t = sr * G2 + gj;
-      a += s_red[(t * 4 + cj) * 2];
-      b += s_red[(t * 4 + cj) * 2 + 1];
+      a += s_red[(2 * cj) * NTX + t];
+      b += s_red[(2 * cj + 1) * NTX + t];
     }
     norms[size_t(blockIdx.x) * 2 * B + j] = a;
     norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
@@ -311,10 +313,11 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
   const int sub = tid / G2, gg = tid % G2;
   const bool isx = gg < G;
   const int g = isx ? gg : gg - G;
-  double *my_red = XP ? s_red + tid * 8 : nullptr;
+  // norm slots, layout [8][threads]: consecutive threads hit consecutive banks
+  double *my_red = XP ? s_red + tid : nullptr;
   if (XP) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) my_red[c] = 0.0;
+    for (int c = 0; c < 8; ++c) my_red[c * NT] = 0.0;
   }
   const int nsub = (ch.end - ch.begin + kCsrSub - 1) / kCsrSub;
   if (tid == 0) {
@@ -412,8 +415,8 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
             // residual from the stored (rounded) products, as the iteration sees them
             const double hq = double(h[c]), mq = double(m[c]);
             res[c] = hq - s_th[4 * g + c] * mq;
-            my_red[2 * c] += res[c] * res[c];
-            my_red[2 * c + 1] += mq * mq;
+            my_red[(2 * c) * NT] += res[c] * res[c];
+            my_red[(2 * c + 1) * NT] += mq * mq;
           }
           *reinterpret_cast<float4 *>(HX + o) = make_float4(h[0], h[1], h[2], h[3]);
           *reinterpret_cast<float4 *>(MX + o) = make_float4(m[0], m[1], m[2], m[3]);
@@ -442,8 +445,8 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
     double a = 0.0, b = 0.0;
     for (int sr = 0; sr < kCsrSub; ++sr) {
       const int t = sr * G2 + gj;
-      a += s_red[(t * 4 + cj) * 2];
-      b += s_red[(t * 4 + cj) * 2 + 1];
+      a += s_red[(2 * cj) * NT + t];
+      b += s_red[(2 * cj + 1) * NT + t];
     }
     norms[size_t(blockIdx.x) * 2 * B + j] = a;
     norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
