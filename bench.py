@@ -50,7 +50,10 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--dots", type=int, default=256)
     ap.add_argument("--k", type=int, default=8)
-    ap.add_argument("--block", type=int, default=12)
+    ap.add_argument("--block", type=int, default=None,
+                    help="LOBPCG block size (default: the autotuned value, else 12)")
+    ap.add_argument("--no-tuned", action="store_true",
+                    help="ignore the autotuner's cached configuration")
     ap.add_argument("--tol", type=float, default=1e-9)
     ap.add_argument("--max-iter", type=int, default=4000)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -255,8 +258,18 @@ def main():
     db = Bt.DeviceBatch(hb, dev)
     db.upload(non_blocking=False)
     stream = torch.cuda.current_stream()
+    # solver configuration: the autotuner's cached choice for this batch shape
+    # on this GPU (python -m qdsim_b200.autotune), else the library defaults
+    from qdsim_b200 import autotune as AT
+    tuned = None if args.no_tuned else AT.load(hb, args.k, args.tol, dev)
+    cfg = dict(AT.DEFAULTS, **(tuned or {}))
+    if args.block is not None:
+        cfg["block"] = args.block
+    args.block = int(cfg["block"])
+    db.set_shift(cfg["shift_ev"])
     solve_kw = dict(b=args.block, precision=args.precision, tol=args.tol,
-                    max_iter=args.max_iter)
+                    max_iter=args.max_iter, tol32=cfg["tol32"],
+                    stag_window=cfg["stag_window"])
 
     def step():
         db.assemble()
@@ -360,6 +373,7 @@ def main():
         "config": {"workload": f"sweep of {args.dots} P2 dots per GPU, nx~U{{40..240}}, ny=nx/2, "
                                "1 nm cells, circular wells; k=8; assemble + batched LOBPCG",
                    "n_dots": args.dots, "k": args.k, "block": args.block,
+                   "solver": {"tuned": tuned is not None, **cfg},
                    "precision": args.precision, "tol": args.tol, "dofs": hb.n, "nnz": hb.nnz,
                    "l2": "inputs larger than L2 (matrices 2.2 GB), no flush",
                    "parallelism": f"{world} GPU(s), independent dots per rank"},

@@ -169,6 +169,18 @@ typedef struct {
  * ------------------------------------------------------------------------- */
 int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_total, int b,
                              int prec_mode, const qd_dst_prec *h_prec, size_t *bytes);
+/* Solver options (pass NULL for the defaults):
+ *   tol32        estimate at which a dot leaves the FP32 phase (<= 0: max(100 tol, 1e-7))
+ *   stag_window  FP32 iterations without halving the estimate before a dot
+ *                switches to FP64 anyway (<= 0: 12)
+ *   graphs       nonzero: replay blocks of 8 iterations as one CUDA graph
+ *                (default); 0: enqueue every kernel directly */
+typedef struct {
+  double tol32;
+  int32_t stag_window;
+  int32_t graphs;
+} qd_lobpcg_opts;
+
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
                     const int32_t *d_rowptr, const int32_t *d_col,
                     const double *d_H, const double *d_M,
@@ -176,7 +188,7 @@ int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_r
                     int k, int b, int prec_mode, double tol, int max_iter, uint64_t seed,
                     double *d_X_out, double *d_E_out, double *d_res_out, int32_t *d_iters_out,
                     int32_t *h_info, int32_t *h_counts, void *d_work, size_t work_bytes,
-                    void *stream);
+                    const qd_lobpcg_opts *opts, void *stream);
 
 /* Apply the DST preconditioner W = T R to a batch of b-column blocks
  * (b >= 4; row-major, float if vec_fp32 else double; in-place allowed).  Same

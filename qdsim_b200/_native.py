@@ -48,7 +48,7 @@ SIGNATURES = {
     "qd_spmm_dual": (_int, [_i32, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _i64, _int, _int, _p, _p]),
     "qd_lobpcg_solve": (_int, [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _int, _int, _int, _dbl,
-                               _int, _u64, _p, _p, _p, _p, _p, _p, _p, _sz, _p]),
+                               _int, _u64, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p]),
     "qd_dst_precond_workspace_size": (_int, [_i32, _p, _int, _p, _p]),
     "qd_dst_precond_apply": (_int, [_i32, _p, _int, _int, _p, _p, _p, _p, _p, _sz, _p]),
     "qd_dst_matrix_size": (_int, [_i32, _p]),
@@ -72,6 +72,11 @@ DST_PREC_DTYPE = _np.dtype([("nx", _np.int32), ("ny", _np.int32), ("sx_off", _np
                             ("sy_off", _np.int64), ("cx", _np.float32), ("cy", _np.float32),
                             ("shift", _np.float32), ("pad", _np.int32)], align=True)
 assert DST_PREC_DTYPE.itemsize == 40
+
+# struct qd_lobpcg_opts (include/qdsim_b200.h)
+LOBPCG_OPTS_DTYPE = _np.dtype([("tol32", _np.float64), ("stag_window", _np.int32),
+                               ("graphs", _np.int32)], align=True)
+assert LOBPCG_OPTS_DTYPE.itemsize == 16
 
 
 class QDError(RuntimeError):

@@ -89,8 +89,15 @@ class HostBatch:
         self.n = row_off
         self.nnz = nnz_off
         self.row_off = np.asarray(self.row_off, dtype=np.int32)
-        self.prec_specs = ([DSTPreconditioner.spec_for(d.mesh, d.c, d.V) for d in dots]
-                           if (precondition and dirichlet) else None)
+        self._prec_src = [(d.mesh, d.c, d.V) for d in dots] if (precondition and dirichlet) else None
+        self.prec_specs = self.prec_specs_for(None)
+
+    def prec_specs_for(self, shift_ev):
+        """Per-dot DST preconditioner specs with the given shift (eV; None:
+        the default), or None for a batch without preconditioning."""
+        if self._prec_src is None:
+            return None
+        return [DSTPreconditioner.spec_for(m, c, V, shift_ev) for m, c, V in self._prec_src]
 
     def pin(self):
         """Page-locked copies of the input arrays (for timed host->device copies)."""
@@ -114,6 +121,11 @@ class DeviceBatch:
         self.ws = Workspace(self.device)
         self.precond = (DSTPreconditioner(host.prec_specs, self.device)
                         if host.prec_specs is not None else None)
+
+    def set_shift(self, shift_ev):
+        """Rebuild the DST preconditioner with another shift (eV)."""
+        specs = self.host.prec_specs_for(shift_ev)
+        self.precond = DSTPreconditioner(specs, self.device) if specs is not None else None
 
     def upload(self, pinned=None, non_blocking=True):
         src = pinned if pinned is not None else {k: torch.from_numpy(v) for k, v in self.host.arrays.items()}

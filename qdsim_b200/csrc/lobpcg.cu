@@ -49,7 +49,7 @@ namespace {
 constexpr int kChunkRows = 1024;
 constexpr int kMaxB = 16;
 constexpr int kMaxM = 3 * kMaxB;
-constexpr int kStagWindow = 30;     // FP32 iterations without halving the estimate
+constexpr int kStagWindow = 12;     // FP32 iterations without halving the estimate
 constexpr double kTol32Floor = 1e-7; // FP32 phase target (estimated rel. eigenvalue error)
 constexpr double kSafety = 1.0;
 constexpr double kRelCap = 1e-2;
@@ -613,6 +613,7 @@ struct RRParams {
   double tol32;    // FP32-phase target (then the dot switches to FP64)
   double tol;      // relative residual tolerance for this phase
   int max_iter;    // total iteration cap per dot
+  int stag_window; // FP32 iterations without halving the estimate before the switch
 };
 
 __device__ inline double cta_sum(double v, double *s_red) {
@@ -865,7 +866,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
         if (worst_raw < 0.5 * s.best) {
           s.best = worst_raw;
           s.stag = 0;
-        } else if (++s.stag >= kStagWindow) {
+        } else if (++s.stag >= prm.stag_window) {
           stop = 1;
         }
       }
@@ -1315,14 +1316,15 @@ __global__ void count_active_kernel(const DotState *st, int n, int *out) {
 // X64 = X32 on their rows, the other FP64 blocks cleared (P restarts empty).
 template <int B>
 __global__ void transition_rows_kernel(const Chunk *chunks, const DotState *st, const float *X32,
-                                       double *X, double *W, double *P, double *HW, double *MW,
-                                       double *HP, double *MP) {
+                                       const float *P32, double *X, double *W, double *P,
+                                       double *HW, double *MW, double *HP, double *MP) {
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].switching) return;
   for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
     const size_t o = size_t(ch.begin) * B + idx;
     X[o] = double(X32[o]);
-    W[o] = P[o] = HW[o] = MW[o] = HP[o] = MP[o] = 0.0;
+    P[o] = double(P32[o]);   // the search direction carries over (its products are explicit)
+    W[o] = HW[o] = MW[o] = HP[o] = MP[o] = 0.0;
   }
 }
 
@@ -1334,7 +1336,6 @@ __global__ void transition_state_kernel(DotState *st, int n) {
   s.switching = 0;
   s.phase = 1;
   s.run[1] = 1;
-  s.has_p = 0;
   s.have_res = 0;
   s.iters_phase = 0;
   s.stag = 0;
@@ -1562,8 +1563,8 @@ int update_step(const Layout &L, const Bufs<TV> &b, cudaStream_t s) {
 // FP64 finish overlaps other dots' FP32 work.
 template <int B>
 int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, const int32_t *col,
-               const double *H, const double *M, const RRParams &prm, cudaStream_t s,
-               int &iters_run) {
+               const double *H, const double *M, const RRParams &prm, bool use_graphs,
+               cudaStream_t s, int &iters_run) {
   Bufs<double> b64(L.slot);
   const size_t rr_smem = rr_smem_bytes(B);
   QD_CUDA_TRY(cudaFuncSetAttribute(rr_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1587,9 +1588,9 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
     }
     if ((st = update_step<double, B>(L, b64, q)) != QD_OK) return st;
     if (mixed) {
-      transition_rows_kernel<B><<<L.nchunks, 256, 0, q>>>(L.chunks, L.st, L.slot32[0], b64.X,
-                                                          b64.W, b64.P, b64.HW, b64.MW, b64.HP,
-                                                          b64.MP);
+      transition_rows_kernel<B><<<L.nchunks, 256, 0, q>>>(L.chunks, L.st, L.slot32[0],
+                                                          L.slot32[2], b64.X, b64.W, b64.P,
+                                                          b64.HW, b64.MW, b64.HP, b64.MP);
       QD_CHECK_LAUNCH();
       transition_state_kernel<<<(n_dots + 127) / 128, 128, 0, q>>>(L.st, n_dots);
       QD_CHECK_LAUNCH();
@@ -1603,10 +1604,9 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
   // private stream and launched into the caller's stream.  Kernel arguments
   // are the same in every iteration (per-dot progress lives on the device),
   // so one graph serves all blocks.  With per-kernel timing enabled, or
-  // QD_GRAPHS=0 in the environment, every block is enqueued directly.
+  // graphs switched off in the options, every block is enqueued directly.
   constexpr int kGraphBlock = 8;
-  const char *genv = std::getenv("QD_GRAPHS");
-  const bool graphs = !qd::prof_enabled() && !(genv && genv[0] == '0');
+  const bool graphs = use_graphs && !qd::prof_enabled();
   struct GraphGuard {
     cudaStream_t cap = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1662,7 +1662,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
             const qd_dst_prec *h_prec, const uint16_t *d_mats, int k, int prec_mode,
             double tol, int max_iter, uint64_t seed, double *d_X_out, double *d_E_out,
             double *d_res_out, int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
-            void *d_work, size_t work_bytes, cudaStream_t s) {
+            void *d_work, size_t work_bytes, const qd_lobpcg_opts *opts, cudaStream_t s) {
   const int64_t n_rows = h_row_off[n_dots];
   const int nchunks = count_chunks(n_dots, h_row_off);
   int64_t ntx = 0, nty = 0;
@@ -1764,6 +1764,13 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   prm.max_iter = max_iter;
   prm.tol = tol;
   prm.tol32 = std::max(100.0 * tol, kTol32Floor);
+  prm.stag_window = kStagWindow;
+  bool graphs = true;
+  if (opts) {
+    if (opts->tol32 > 0.0) prm.tol32 = std::max(opts->tol32, tol);
+    if (opts->stag_window > 0) prm.stag_window = opts->stag_window;
+    graphs = opts->graphs != 0;
+  }
   Bufs<double> b64(L.slot);
   if (mixed) {
     Bufs<float> b32(L.slot32);
@@ -1776,7 +1783,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     QD_CHECK_LAUNCH();
   }
   int iters_run = 0;
-  int rs = run_solver<B>(L, mixed, n_dots, d_rowptr, d_col, d_H, d_M, prm, s, iters_run);
+  int rs = run_solver<B>(L, mixed, n_dots, d_rowptr, d_col, d_H, d_M, prm, graphs, s, iters_run);
   if (rs != QD_OK) return rs;
   output_kernel<B><<<nchunks, 256, 0, s>>>(L.chunks, b64.X, k, d_X_out);
   QD_CHECK_LAUNCH();
@@ -1841,7 +1848,8 @@ extern "C" int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off,
                                int b, int prec_mode, double tol, int max_iter, uint64_t seed,
                                double *d_X_out, double *d_E_out, double *d_res_out,
                                int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
-                               void *d_work, size_t work_bytes, void *stream) {
+                               void *d_work, size_t work_bytes, const qd_lobpcg_opts *opts,
+                               void *stream) {
   (void)d_row_off;
   const uint16_t *d_prec_mats = static_cast<const uint16_t *>(d_prec_mats_v);
   if (n_dots <= 0 || !h_row_off || !d_rowptr || !d_col || !d_H || !d_M || !d_X_out ||
@@ -1857,10 +1865,10 @@ extern "C" int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off,
     if (h_row_off[d + 1] - h_row_off[d] < b + 1) return QD_ERR_INVALID;  // need n > b
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (b) {
-    case 4: return solve_b<4>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
-    case 8: return solve_b<8>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
-    case 12: return solve_b<12>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
-    default: return solve_b<16>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, s);
+    case 4: return solve_b<4>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, opts, s);
+    case 8: return solve_b<8>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, opts, s);
+    case 12: return solve_b<12>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, opts, s);
+    default: return solve_b<16>(n_dots, h_row_off, d_rowptr, d_col, d_H, d_M, h_prec, d_prec_mats, k, prec_mode, tol, max_iter, seed, d_X_out, d_E_out, d_res_out, d_iters_out, h_info, h_counts, d_work, work_bytes, opts, s);
   }
 }
 

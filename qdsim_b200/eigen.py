@@ -136,8 +136,14 @@ class Workspace:
 
 def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=1e-6,
                   max_iter=2000, seed=1234, workspace: Workspace | None = None, stream=None,
-                  allow_not_converged=True, precond: DSTPreconditioner | None = None):
-    """Solve a packed block-diagonal batch; returns (E, X_all, res, iters, info, status)."""
+                  allow_not_converged=True, precond: DSTPreconditioner | None = None,
+                  tol32: float | None = None, stag_window: int | None = None,
+                  graphs: bool = True):
+    """Solve a packed block-diagonal batch; returns (E, X_all, res, iters, info, status).
+
+    ``tol32`` / ``stag_window`` tune the FP32 -> FP64 hand-over of the mixed
+    mode (``None``: library defaults); ``graphs=False`` enqueues every kernel
+    instead of replaying CUDA graphs."""
     n_dots = len(row_off) - 1
     n_rows = int(row_off[-1])
     if b is None:
@@ -156,11 +162,14 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
     info = np.zeros(4, dtype=np.int32)
     counts = np.zeros((n_dots, 6), dtype=np.int32)
     ro = np.ascontiguousarray(row_off, dtype=np.int32)
+    opts = np.zeros(1, dtype=N.LOBPCG_OPTS_DTYPE)
+    opts[0] = (float(tol32) if tol32 else 0.0, int(stag_window) if stag_window else 0,
+               1 if graphs else 0)
     st = N.lib().qd_lobpcg_solve(
         n_dots, N.ptr(ro), None, N.ptr(rowptr), N.ptr(col), N.ptr(H), N.ptr(M), N.ptr(h_prec),
         N.ptr(d_mats), k, b, prec,
         float(tol), int(max_iter), int(seed), N.ptr(X), N.ptr(E), N.ptr(R), N.ptr(it),
-        N.ptr(info), N.ptr(counts), N.ptr(ws), ws.numel(), stream_ptr(stream))
+        N.ptr(info), N.ptr(counts), N.ptr(ws), ws.numel(), N.ptr(opts), stream_ptr(stream))
     N.check(st, "qd_lobpcg_solve",
             allow=(N.QD_ERR_NOT_CONVERGED,) if allow_not_converged else ())
     infod = {"iterations": int(info[0]), "iters_fp32": int(info[1]), "iters_fp64": int(info[2]),

@@ -54,7 +54,7 @@ def test_invalid_arguments_rejected_without_gpu():
     # n must exceed the block size
     assert L.qd_lobpcg_solve(1, N.ptr(ro), None, *([C.c_void_p(8)] * 4), None, None, 4, 8, 0,
                              1e-9, 10, 1, *([C.c_void_p(8)] * 4), N.ptr(info), None,
-                             C.c_void_p(256), 1 << 20, None) == N.QD_ERR_INVALID
+                             C.c_void_p(256), 1 << 20, None, None) == N.QD_ERR_INVALID
     assert L.qd_pcg_solve_static(0, 1, *([None] * 6), 1e-9, 10, None, None, None) == N.QD_ERR_INVALID
 
 
