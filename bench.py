@@ -38,6 +38,11 @@ UNIT = "eigenpairs/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "sweep256.npz")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
+# DRAM traffic over algorithmic bytes per kernel kind, from one ncu capture of
+# the first 24 dots of the sweep (dram__bytes_read.sum + dram__bytes_write.sum
+# of the FP32-phase SpMM launches divided by their algorithmic bytes); the
+# roofline's `traffic` is the algorithmic bytes per launch times this ratio.
+TRAFFIC_RATIO = {"spmm": 1.031}
 KIND_NAMES = ["spmm", "gram", "rayleigh_ritz", "update", "assemble", "pcg", "adjoint",
               "dst_precond", "ortho", "other"]
 
@@ -362,7 +367,10 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": (achieved / peak if achieved else None),
                 "peak_source": f"{peak_src} hbm_gbs",
-                "traffic": None,
+                "traffic": (TRAFFIC_RATIO[dom_name] * bytes_kind[dom_name] / max(prof_n[dom], 1)
+                            if dom_name in TRAFFIC_RATIO and dom_name in bytes_kind else None),
+                "traffic_source": ("ncu capture of the 24-dot sweep, scaled to a full launch by "
+                                   "the rows processed" if dom_name in TRAFFIC_RATIO else None),
                 "bytes_per_launch": (bytes_kind.get(dom_name, 0.0) / max(prof_n[dom], 1))}
 
     result = {
