@@ -174,11 +174,15 @@ int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_t
  *   stag_window  FP32 iterations without halving the estimate before a dot
  *                switches to FP64 anyway (<= 0: 12)
  *   graphs       nonzero: replay blocks of 8 iterations as one CUDA graph
- *                (default); 0: enqueue every kernel directly */
+ *                (default); 0: enqueue every kernel directly
+ *   x0           optional device array (rows x k, the layout of d_X_out): warm
+ *                start for the first k block vectors (e.g. the previous
+ *                self-consistent iteration's eigenvectors); NULL: random */
 typedef struct {
   double tol32;
   int32_t stag_window;
   int32_t graphs;
+  const double *x0;
 } qd_lobpcg_opts;
 
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
@@ -208,6 +212,36 @@ int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, int b, int ve
                          const qd_dst_prec *h_prec, const void *d_prec_mats,
                          const void *d_in, void *d_out, void *d_work, size_t work_bytes,
                          void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Self-consistent Poisson-Schrodinger loop batched over nb bias points (the
+ * loop of qdsim_cython/solvers/self_consistent_solver.pyx:130-286 with the
+ * mixing of backend/src/self_consistent.cpp:1262-1468).  Potentials, densities
+ * and the mixing history are [node][bias] (qd_pcg_solve's right-hand-side
+ * layout); the Schrodinger potential is [bias][node] (the batched union mesh).
+ *
+ * qd_sc_potential   V_out[b][i] = V_static[i] - phi[i][b]   (eV, phi in V)
+ * qd_sc_density     per bias: E_F = E_0 + kT/2, Fermi-Dirac occupations of the
+ *                   k states, n = sum f psi^2 rescaled to mean N_D, classical
+ *                   holes p = N_A exp(-phi/V_T) where phi > 0 else N_A,
+ *                   rho = q (p - n) [C/m^3]; X is rows x k with bias b's rows
+ *                   at b * rows_per_bias + dof[i] (dof[i] < 0: boundary node)
+ * qd_sc_mix         damping (anderson = 0) or Anderson mixing with history
+ *                   h_hist_* (host arrays of nhist device pointers, oldest
+ *                   first; this update and its residual are written to slot
+ *                   nhist-1): phi_new, per-bias damping factor (adapted in
+ *                   place), previous error and error ||phi_new-phi_old||/||phi_new||
+ * ------------------------------------------------------------------------- */
+int qd_sc_potential(int32_t nb, int64_t n_nodes, const double *d_V_static, const double *d_phi,
+                    double *d_V_out, void *stream);
+int qd_sc_density(int32_t nb, int64_t n_nodes, int k, int64_t rows_per_bias,
+                  const int32_t *d_dof, const double *d_X, const double *d_E, double kT_eV,
+                  double N_A, double N_D, const double *d_phi, double *d_n, double *d_p,
+                  double *d_rho, void *stream);
+int qd_sc_mix(int32_t nb, int64_t n_nodes, int anderson, int nhist, const double *d_phi_old,
+              const double *d_phi_upd, double *const *h_hist_upd, double *const *h_hist_res,
+              double *d_phi_new, double *d_damping, double *d_prev_error, double *d_error,
+              void *stream);
 
 /* ---------------------------------------------------------------------------
  * Jacobi-preconditioned CG, FP64, for nrhs right-hand sides sharing one SPD

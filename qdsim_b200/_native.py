@@ -61,6 +61,10 @@ SIGNATURES = {
     "qd_csr_spmv": (_int, [_i32, _int, _p, _p, _p, _p, _p, _dbl, _p]),
     "qd_prof_enable": (_int, [_int]),
     "qd_prof_read": (_int, [_p, _p, _int]),
+    "qd_sc_potential": (_int, [_i32, _i64, _p, _p, _p, _p]),
+    "qd_sc_density": (_int, [_i32, _i64, _int, _i64, _p, _p, _p, _dbl, _dbl, _dbl, _p, _p, _p,
+                             _p, _p]),
+    "qd_sc_mix": (_int, [_i32, _i64, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_adjoint": (_int, [_int, _i64, _i64, _int, _p, _p, _p, _p, _p, _p, _p, _p,
                           _p, _p, _p]),
 }
@@ -75,8 +79,8 @@ assert DST_PREC_DTYPE.itemsize == 40
 
 # struct qd_lobpcg_opts (include/qdsim_b200.h)
 LOBPCG_OPTS_DTYPE = _np.dtype([("tol32", _np.float64), ("stag_window", _np.int32),
-                               ("graphs", _np.int32)], align=True)
-assert LOBPCG_OPTS_DTYPE.itemsize == 16
+                               ("graphs", _np.int32), ("x0", _np.uint64)], align=True)
+assert LOBPCG_OPTS_DTYPE.itemsize == 24
 
 
 class QDError(RuntimeError):

@@ -97,7 +97,8 @@ __device__ inline uint64_t splitmix64(uint64_t x) {
 
 template <typename TV, int B>
 __global__ void init_kernel(const Chunk *chunks, const int32_t *row_off, uint64_t seed, TV *X,
-                            TV *W, TV *P, TV *HW, TV *MW, TV *HP, TV *MP) {
+                            TV *W, TV *P, TV *HW, TV *MW, TV *HP, TV *MP, const double *X0,
+                            int k) {
   const Chunk ch = chunks[blockIdx.x];
   const int r0 = row_off[ch.dot];
   for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
@@ -105,7 +106,8 @@ __global__ void init_kernel(const Chunk *chunks, const int32_t *row_off, uint64_
     const uint64_t h = splitmix64(seed * 0x100000001b3ull + uint64_t(r - r0) * B + j);
     const double u = double(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
     const size_t o = size_t(r) * B + j;
-    X[o] = TV(u);
+    // warm start: the caller's k vectors (row-major rows x k), random guard columns
+    X[o] = (X0 && j < k) ? TV(X0[size_t(r) * k + j]) : TV(u);
     W[o] = P[o] = HW[o] = MW[o] = HP[o] = MP[o] = TV(0);
   }
 }
@@ -1766,6 +1768,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   prm.tol32 = std::max(100.0 * tol, kTol32Floor);
   prm.stag_window = kStagWindow;
   bool graphs = true;
+  const double *x0 = opts ? opts->x0 : nullptr;
   if (opts) {
     if (opts->tol32 > 0.0) prm.tol32 = std::max(opts->tol32, tol);
     if (opts->stag_window > 0) prm.stag_window = opts->stag_window;
@@ -1775,11 +1778,11 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   if (mixed) {
     Bufs<float> b32(L.slot32);
     init_kernel<float, B><<<nchunks, 256, 0, s>>>(L.chunks, L.row_off, seed, b32.X, b32.W, b32.P,
-                                                  b32.HW, b32.MW, b32.HP, b32.MP);
+                                                  b32.HW, b32.MW, b32.HP, b32.MP, x0, k);
     QD_CHECK_LAUNCH();
   } else {
     init_kernel<double, B><<<nchunks, 256, 0, s>>>(L.chunks, L.row_off, seed, b64.X, b64.W,
-                                                   b64.P, b64.HW, b64.MW, b64.HP, b64.MP);
+                                                   b64.P, b64.HW, b64.MW, b64.HP, b64.MP, x0, k);
     QD_CHECK_LAUNCH();
   }
   int iters_run = 0;

@@ -116,3 +116,36 @@ def c2_dot(seed: int = 0, nx: int = 400, ny: int = 200, Lx: float = 200.0, Ly: f
     mstar = np.where(Vc < -0.05, 0.041, 0.067)
     W = cap_profile(x, y, Lx, Ly, 0.05, 10.0)
     return Dot(mesh, C0_EV_NM2 / mstar, Vn, W)
+
+
+@dataclass
+class Junction:
+    """Self-consistent p-n junction batched over bias points."""
+    mesh: StructuredMesh
+    eps_r: np.ndarray       # per element
+    c: np.ndarray           # per element, hbar^2/(2 m*) in eV nm^2
+    V_static: np.ndarray    # nodal, eV
+    biases: np.ndarray      # V_n per bias point (V_p = 0), V
+    N_A: float = 1e24
+    N_D: float = 1e24
+    T: float = 300.0
+
+
+def c5_junction(n_bias: int = 64, seed: int = 0, nx: int = 300, ny: int = 100,
+                Lx: float = 300.0, Ly: float = 100.0) -> Junction:
+    """P1 300x100 cells on 300x100 nm; eps_r 13.9; conduction-band offset 0.2 eV
+    on the p side (x < Lx/2); Gaussian dot -0.3 exp(-r^2/(2 8^2)) eV at the
+    junction; m* 0.041 m0 where the dot is deeper than 0.15 eV, else 0.067 m0;
+    N_A = N_D = 1e24 m^-3; bias points V_n ~ U[0, 1] V (seeded), V_p = 0."""
+    rng = np.random.default_rng([seed, 5])
+    mesh = StructuredMesh(1, nx, ny, Lx, Ly)
+    x, y = mesh.nodes[:, 0], mesh.nodes[:, 1]
+
+    def dot(xx, yy):
+        return -0.3 * np.exp(-((xx - Lx / 2) ** 2 + (yy - Ly / 2) ** 2) / (2 * 8.0 ** 2))
+
+    V = np.where(x < Lx / 2, 0.2, 0.0) + dot(x, y)
+    cen = mesh.centroids()
+    c = C0_EV_NM2 / np.where(dot(cen[:, 0], cen[:, 1]) < -0.15, 0.041, 0.067)
+    return Junction(mesh, np.full(mesh.num_elements, 13.9), c, V,
+                    np.sort(rng.uniform(0.0, 1.0, n_bias)))

@@ -90,3 +90,33 @@ def test_poisson_oracle_linear_ramp():
     om = O.structured_mesh(1, 10, 4, 50.0, 20.0)
     phi = OP.solve(om, np.full(om.num_elements, 12.0), np.zeros(om.num_nodes), 0.0, 1.0)
     assert np.allclose(phi, om.nodes[:, 0] / 50.0, atol=1e-12)
+
+
+def test_anderson_coefficients_restatement():
+    """Full-rank least squares equals lstsq; clipping and the sum cap apply."""
+    from oracle import sc as OS
+    rng = np.random.default_rng(3)
+    r = [rng.standard_normal(50) for _ in range(3)]
+    al = OS.anderson_coefficients(r)
+    F = np.stack([r[0] - r[2], r[1] - r[2]], axis=1)
+    ref, *_ = np.linalg.lstsq(F, -r[2], rcond=None)
+    ref = np.clip(ref, -2, 2)
+    if abs(ref.sum()) > 2:
+        ref *= 2 / abs(ref.sum())
+    assert np.allclose(al, ref, rtol=1e-10)
+    # a dependent pair takes the regularised branch and stays finite
+    r2 = [r[0], 2 * r[0] - r[2] + 0 * r[1], r[2]]
+    r2[1] = r[2] + 2 * (r[0] - r[2])
+    al2 = OS.anderson_coefficients(r2)
+    assert al2 is not None and np.all(np.isfinite(al2)) and abs(al2.sum()) <= 2 + 1e-12
+
+
+def test_sc_restatement_runs_and_contracts():
+    """The oracle loop on a tiny junction: the error drops over the iterations."""
+    import dataclasses
+    from oracle import fem as O, sc as OS
+    from qdsim_b200 import workloads as W
+    j = W.c5_junction(n_bias=2, nx=16, ny=8, Lx=16.0, Ly=8.0)
+    j = dataclasses.replace(j, mesh=O.structured_mesh(1, 16, 8, 16.0, 8.0))
+    phi, err, E = OS.run(j, k=3, iterations=15)
+    assert np.all(np.isfinite(phi)) and err[-1].max() < err[0].max()
