@@ -203,6 +203,46 @@ def reduce_over_ranks(ms: float, conv: float, world: int, device):
     return float(ms_t.item()), float(conv_t.item())
 
 
+def sc_measurement(dev):
+    """The self-consistent p-n junction batched over 64 bias points (P1
+    300x100 cells, 10 states, 40 iterations, mixed-precision eigensolves,
+    FP64 PCG), then the implicit dE1/dbias; beside it the FP64 restatement
+    (scipy) timed on a bounded sample of map evaluations on one core."""
+    import dataclasses
+    import torch
+    from qdsim_b200 import workloads as W
+    from qdsim_b200.sc import BatchedSC
+    j = W.c5_junction(64)
+    sc = BatchedSC(j, k=10, device=dev)
+    sc.solve(iterations=2)                        # warm-up: workspaces, graphs
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    phi, err = sc.solve(iterations=40)
+    e1.record()
+    dE = sc.dE1_dbias(phi)
+    e2.record()
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1) / 1000.0
+    t_adj = e1.elapsed_time(e2) / 1000.0
+    # CPU: the restatement's map for 2 bias points x 2 iterations
+    from oracle import fem as O, sc as OS
+    jo = dataclasses.replace(j, biases=j.biases[:2],
+                             mesh=O.structured_mesh(1, 300, 100, 300.0, 100.0))
+    t0 = time.perf_counter()
+    OS.run(jo, k=10, iterations=2)
+    t_cpu = time.perf_counter() - t0
+    return {"workload": "p-n junction, P1 300x100 cells, 64 bias points, 10 states, "
+                        "40 iterations (damping, then Anderson)",
+            "seconds": t_loop, "bias_iterations_per_s": 64 * 40 / t_loop,
+            "final_error_max": float(err[-1].max().item()),
+            "dE1_dbias_seconds": t_adj, "gmres_residual": sc.gmres_residual,
+            "dE1_dbias_range": [float(dE.min().item()), float(dE.max().item())],
+            "cpu_port": {"bias_iterations_per_s": 4 / t_cpu, "cores": 1,
+                         "sample": "FP64 restatement (scipy shift-invert eigsh, splu), "
+                                   f"2 bias points x 2 iterations, {t_cpu:.1f} s"}}
+
+
 def algorithmic_bytes(hb, counts, k_block):
     """Algorithmic bytes per kernel kind, from the per-dot launch counts.
 
@@ -450,6 +490,7 @@ def main():
                                     "mixed_batched_over_plain": value / (cp / tp) if cp else None}
             del sdb, sub
             result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+            result["sc_junction"] = sc_measurement(dev)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -203,7 +203,7 @@ int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int 
 /* Element count (BF16) of the DST-I matrix of lattice size n in the
  * tensor-core layout, and the host routine that writes it (round to nearest
  * even).  Layout: rows padded to R = 16 ceil(n/16), columns (k) to
- * 64 ceil(n/64); rows split into blocks of 512; within a block of r rows,
+ * 64 ceil(n/64); rows split into blocks of 256; within a block of r rows,
  * element (row, k) sits at  (k/64) r 64 + ((k%64)/8) r 8 + (row/8) 64 +
  * (row%8) 8 + k%8  (8 x 8 core matrices, 16 bytes per core-matrix row). */
 int qd_dst_matrix_size(int32_t n, int64_t *elems);

@@ -26,7 +26,7 @@
 // Pass 4 (x): t1 row-major -> W grouped [iy][ix][b]
 // so that every pass reads or writes one side with unit stride along n.
 //
-// One CTA computes a 128 (n) x up to 512 (r) block of out^T in TMEM:
+// One CTA computes a 128 (n) x up to 256 (r) block of out^T in TMEM:
 //   A = in^T tile (128 n x 64 k per K slab), staged by the threads from the
 //       vector precision into BF16 shared memory (K-major, no swizzle);
 //   B = S tile (r x 64 k), pre-arranged in global memory in exactly the
@@ -50,7 +50,7 @@ struct GemmTile {
 
 constexpr int kTcN = 128;        // data columns (n) per CTA = TMEM lanes
 constexpr int kTcK = 64;         // K per shared-memory slab
-constexpr int kTcRows = 512;     // transform rows (r) per CTA = max TMEM columns
+constexpr int kTcRows = 256;     // transform rows (r) per CTA = TMEM columns (2 CTAs per SM)
 constexpr int kTcThreads = 256;
 constexpr uint64_t kTcWaitNs = 1000000000ull;   // 1 s bound on every wait
 constexpr int kTcABytes = kTcN * kTcK * 2;      // 16 KiB per A stage
@@ -313,20 +313,20 @@ inline void dst_tiles(int n_dots, const qd_dst_prec *h, int B, GemmTile *tx, int
   for (int d = 0; d < n_dots; ++d) {
     const int nx = h[d].nx, ny = h[d].ny;
     if (nx <= 0 || ny <= 0) continue;
-    for (int m0 = 0; m0 < tc_rpad(nx); m0 += kTcRows) {
-      rx = std::max(rx, std::min(kTcRows, tc_rpad(nx) - m0));
-      for (int n0 = 0; n0 < ny * B; n0 += kTcN) {
+    // row blocks innermost: the CTAs of one data tile run side by side and
+    // the later ones read the tile from L2
+    for (int n0 = 0; n0 < ny * B; n0 += kTcN)
+      for (int m0 = 0; m0 < tc_rpad(nx); m0 += kTcRows) {
+        rx = std::max(rx, std::min(kTcRows, tc_rpad(nx) - m0));
         if (tx) tx[a] = GemmTile{d, m0, n0, 0};
         ++a;
       }
-    }
-    for (int m0 = 0; m0 < tc_rpad(ny); m0 += kTcRows) {
-      ry = std::max(ry, std::min(kTcRows, tc_rpad(ny) - m0));
-      for (int n0 = 0; n0 < nx * B; n0 += kTcN) {
+    for (int n0 = 0; n0 < nx * B; n0 += kTcN)
+      for (int m0 = 0; m0 < tc_rpad(ny); m0 += kTcRows) {
+        ry = std::max(ry, std::min(kTcRows, tc_rpad(ny) - m0));
         if (ty) ty[b] = GemmTile{d, m0, n0, 0};
         ++b;
       }
-    }
   }
   *ntx = a;
   *nty = b;

@@ -69,8 +69,8 @@ def test_dst_matrix_layout(n):
     assert m.size == R * KS * 64
     full = np.zeros((R, KS * 64))
     pos = 0
-    for m0 in range(0, R, 512):
-        rows = min(512, R - m0)
+    for m0 in range(0, R, 256):
+        rows = min(256, R - m0)
         blk = m[pos:pos + rows * KS * 64].astype(np.uint32) << 16
         blk = blk.view(np.float32).astype(np.float64)
         # [slab][chunk][row group][row in group][k in chunk]

@@ -8,7 +8,7 @@ from dst_emul import apply_bf16, apply_exact
 pytestmark = pytest.mark.gpu
 
 # (nx, ny): ragged tiles, a 5 x 3 lattice (one 16-row block, one K slab), a
-# 600-wide lattice (two TMEM row blocks of 512 + 96 rows, two MMA parts)
+# 600-wide lattice (three TMEM row blocks of 256 + 256 + 96 rows)
 SHAPES = [(37, 21), (130, 65), (5, 3), (600, 7)]
 
 
