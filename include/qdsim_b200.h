@@ -177,12 +177,16 @@ int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_t
  *                (default); 0: enqueue every kernel directly
  *   x0           optional device array (rows x k, the layout of d_X_out): warm
  *                start for the first k block vectors (e.g. the previous
- *                self-consistent iteration's eigenvectors); NULL: random */
+ *                self-consistent iteration's eigenvectors); NULL: random
+ *   eig_scale    energy below which eigenvalue errors are measured absolutely:
+ *                the estimate divides by max(|t|, eig_scale) instead of |t|
+ *                (levels near zero energy); <= 0: purely relative */
 typedef struct {
   double tol32;
   int32_t stag_window;
   int32_t graphs;
   const double *x0;
+  double eig_scale;
 } qd_lobpcg_opts;
 
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,

@@ -79,8 +79,9 @@ assert DST_PREC_DTYPE.itemsize == 40
 
 # struct qd_lobpcg_opts (include/qdsim_b200.h)
 LOBPCG_OPTS_DTYPE = _np.dtype([("tol32", _np.float64), ("stag_window", _np.int32),
-                               ("graphs", _np.int32), ("x0", _np.uint64)], align=True)
-assert LOBPCG_OPTS_DTYPE.itemsize == 24
+                               ("graphs", _np.int32), ("x0", _np.uint64),
+                               ("eig_scale", _np.float64)], align=True)
+assert LOBPCG_OPTS_DTYPE.itemsize == 32
 
 
 class QDError(RuntimeError):

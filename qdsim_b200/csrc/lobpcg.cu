@@ -616,6 +616,7 @@ struct RRParams {
   double tol;      // relative residual tolerance for this phase
   int max_iter;    // total iteration cap per dot
   int stag_window; // FP32 iterations without halving the estimate before the switch
+  double eig_scale; // floor of |theta| in the relative error estimate (0: none)
 };
 
 __device__ inline double cta_sum(double v, double *s_red) {
@@ -842,7 +843,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
         rr += norms[size_t(c) * 2 * B + tid];
         mx += norms[size_t(c) * 2 * B + B + tid];
       }
-      const double at = fmax(fabs(th[tid]), 1e-300);
+      const double at = fmax(fmax(fabs(th[tid]), prm.eig_scale), 1e-300);
       const double ares = sqrt(rr / fmax(mx, 1e-300));
       const double gap = fmax(th[B - 1] - th[tid], 1e-300);
       const double rel = ares / at;
@@ -1767,11 +1768,13 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   prm.tol = tol;
   prm.tol32 = std::max(100.0 * tol, kTol32Floor);
   prm.stag_window = kStagWindow;
+  prm.eig_scale = 0.0;
   bool graphs = true;
   const double *x0 = opts ? opts->x0 : nullptr;
   if (opts) {
     if (opts->tol32 > 0.0) prm.tol32 = std::max(opts->tol32, tol);
     if (opts->stag_window > 0) prm.stag_window = opts->stag_window;
+    if (opts->eig_scale > 0.0) prm.eig_scale = opts->eig_scale;
     graphs = opts->graphs != 0;
   }
   Bufs<double> b64(L.slot);

@@ -96,21 +96,41 @@ __global__ void pcg_spmv_kernel(Cfg c, const int32_t *rowptr, const int32_t *col
 }
 
 // scalars: mode 0 -> initial (rz, rr0); mode 1 -> alpha = rz / pAp; mode 2 -> beta, convergence
-__global__ void pcg_scalar_kernel(Cfg c, int mode, const double *part, double *sc, int *done,
-                                  double tol) {
+// The per-block partials of a column are summed by L = kScalarThreads / nrhs
+// lanes (lane l takes blocks l, l + L, ...), then the L lane sums in lane
+// order: a fixed order, so the result is reproducible.
+constexpr int kScalarThreads = 1024;
+
+__global__ void __launch_bounds__(kScalarThreads)
+pcg_scalar_kernel(Cfg c, int mode, const double *part, double *sc, int *done, double tol) {
   // sc layout per column: [rz, rr0, alpha, beta, rr]
-  const int j = threadIdx.x;
+  __shared__ double s_a[kScalarThreads], s_b[kScalarThreads];
   __shared__ int s_all;
-  if (j == 0) s_all = 1;
-  __syncthreads();
+  const int t = threadIdx.x;
+  const int L = kScalarThreads / c.nrhs;
+  const int j = t / L, l = t % L;
+  if (t == 0) s_all = 1;
+  // partial kinds: 0 r.z, 1 r.r (modes 0, 2); 2 p.Ap (mode 1)
+  const int ka = mode == 1 ? 2 : 0, kb = 1;
+  double a = 0.0, b = 0.0;
   if (j < c.nrhs) {
+    for (int blk = l; blk < c.blocks; blk += L) {
+      a += part[size_t(blk) * 3 * c.nrhs + size_t(ka) * c.nrhs + j];
+      if (mode != 1) b += part[size_t(blk) * 3 * c.nrhs + size_t(kb) * c.nrhs + j];
+    }
+  }
+  s_a[t] = a;
+  s_b[t] = b;
+  __syncthreads();
+  if (j < c.nrhs && l == 0) {
+    double sa = 0.0, sb = 0.0;
+    for (int q = 0; q < L; ++q) {
+      sa += s_a[t + q];
+      sb += s_b[t + q];
+    }
     double *s = sc + size_t(j) * 5;
     if (mode == 0) {
-      double rz = 0.0, rr = 0.0;
-      for (int b = 0; b < c.blocks; ++b) {
-        rz += part[size_t(b) * 3 * c.nrhs + j];
-        rr += part[size_t(b) * 3 * c.nrhs + c.nrhs + j];
-      }
+      const double rz = sa, rr = sb;
       s[0] = rz;
       s[1] = rr;
       s[4] = rr;
@@ -118,15 +138,10 @@ __global__ void pcg_scalar_kernel(Cfg c, int mode, const double *part, double *s
       const bool conv = !(rr > 0.0);
       if (!conv) atomicAnd(&s_all, 0);
     } else if (mode == 1) {
-      double pap = 0.0;
-      for (int b = 0; b < c.blocks; ++b) pap += part[size_t(b) * 3 * c.nrhs + 2 * c.nrhs + j];
+      const double pap = sa;
       s[2] = (pap > 0.0 && s[4] > tol * tol * s[1]) ? s[0] / pap : 0.0;
     } else {
-      double rz = 0.0, rr = 0.0;
-      for (int b = 0; b < c.blocks; ++b) {
-        rz += part[size_t(b) * 3 * c.nrhs + j];
-        rr += part[size_t(b) * 3 * c.nrhs + c.nrhs + j];
-      }
+      const double rz = sa, rr = sb;
       s[3] = (s[0] > 0.0) ? rz / s[0] : 0.0;
       s[0] = rz;
       s[4] = rr;
@@ -135,7 +150,7 @@ __global__ void pcg_scalar_kernel(Cfg c, int mode, const double *part, double *s
     }
   }
   __syncthreads();
-  if (j == 0 && mode != 1) *done = s_all;
+  if (t == 0 && mode != 1) *done = s_all;
 }
 
 // x += alpha p, r -= alpha Ap, z = D^-1 r; partials r.z, r.r
@@ -234,7 +249,7 @@ extern "C" int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const 
   pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
                                                     L.R, L.Z, L.P, L.dinv, L.part);
   QD_CHECK_LAUNCH();
-  pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
+  pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
   QD_CHECK_LAUNCH();
   int it = 0, done = 0;
   const int check = 16;
@@ -242,12 +257,12 @@ extern "C" int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const 
     pcg_spmv_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_fixed, L.P,
                                                       L.AP, L.done, L.part);
     QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
+    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
     QD_CHECK_LAUNCH();
     pcg_axpy_kernel<<<c.blocks, c.threads, smem, s>>>(c, L.sc, L.dinv, d_X, L.R, L.Z, L.P, L.AP,
                                                       L.done, L.part);
     QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
+    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
     QD_CHECK_LAUNCH();
     pcg_dir_kernel<<<c.blocks, c.threads, 0, s>>>(c, L.sc, L.Z, L.P, L.done);
     QD_CHECK_LAUNCH();
@@ -367,19 +382,19 @@ extern "C" int qd_pcg_solve_static(int32_t n, int nrhs, const int32_t *d_rowptr,
   pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
                                                     L.R, L.Z, L.P, L.dinv, L.part);
   QD_CHECK_LAUNCH();
-  pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
+  pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
   QD_CHECK_LAUNCH();
   int it = 0, done = 0;
   for (it = 0; it < max_iter; ++it) {
     pcg_spmv_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_fixed, L.P,
                                                       L.AP, L.done, L.part);
     QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
+    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
     QD_CHECK_LAUNCH();
     pcg_axpy_kernel<<<c.blocks, c.threads, smem, s>>>(c, L.sc, L.dinv, d_X, L.R, L.Z, L.P, L.AP,
                                                       L.done, L.part);
     QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kMaxRhs, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
+    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
     QD_CHECK_LAUNCH();
     pcg_dir_kernel<<<c.blocks, c.threads, 0, s>>>(c, L.sc, L.Z, L.P, L.done);
     QD_CHECK_LAUNCH();

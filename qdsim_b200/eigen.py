@@ -138,13 +138,14 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
                   max_iter=2000, seed=1234, workspace: Workspace | None = None, stream=None,
                   allow_not_converged=True, precond: DSTPreconditioner | None = None,
                   tol32: float | None = None, stag_window: int | None = None,
-                  graphs: bool = True, x0=None):
+                  graphs: bool = True, x0=None, eig_scale: float = 0.0):
     """Solve a packed block-diagonal batch; returns (E, X_all, res, iters, info, status).
 
     ``tol32`` / ``stag_window`` tune the FP32 -> FP64 hand-over of the mixed
     mode (``None``: library defaults); ``graphs=False`` enqueues every kernel
     instead of replaying CUDA graphs; ``x0`` (device float64 [n_rows, k])
-    warm-starts the first k block vectors."""
+    warm-starts the first k block vectors; ``eig_scale`` (eV) measures
+    eigenvalue errors relative to max(|E|, eig_scale) (levels near zero)."""
     n_dots = len(row_off) - 1
     n_rows = int(row_off[-1])
     if b is None:
@@ -169,7 +170,8 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
         if x0.numel() != n_rows * k:
             raise ValueError("x0 must hold n_rows x k values")
     opts[0] = (float(tol32) if tol32 else 0.0, int(stag_window) if stag_window else 0,
-               1 if graphs else 0, int(x0.data_ptr()) if x0 is not None else 0)
+               1 if graphs else 0, int(x0.data_ptr()) if x0 is not None else 0,
+               float(eig_scale))
     st = N.lib().qd_lobpcg_solve(
         n_dots, N.ptr(ro), None, N.ptr(rowptr), N.ptr(col), N.ptr(H), N.ptr(M), N.ptr(h_prec),
         N.ptr(d_mats), k, b, prec,

@@ -13,8 +13,8 @@ damping, the damping factor shrinking by 0.8 whenever the error grows.
 All bias points advance together: one batched LOBPCG over the bias points'
 potentials (one mesh, one dot per bias), one batched Jacobi-PCG (one stiffness,
 one right-hand side per bias), densities and mixing in ``qd_sc_density`` /
-``qd_sc_mix`` (one CTA per bias).  Eigenvectors of one iteration warm-start the
-next.  Units: nm, eV for Schrodinger; V and C/m^3 for Poisson.
+``qd_sc_mix`` (one CTA per bias).  The eigenvectors of one iteration warm-start
+the next.  Units: nm, eV for Schrodinger; V and C/m^3 for Poisson.
 
 ``dE1_dbias`` differentiates the converged lowest level with respect to the
 bias through the fixed point phi* = G(phi*, V): the bias enters G only through
@@ -42,14 +42,18 @@ K_B_EV = 8.617333262e-5     # Boltzmann constant, eV/K
 
 class BatchedSC:
     def __init__(self, junction: Junction, k: int = 10, device="cuda", precision="mixed",
-                 tol=1e-9, pcg_tol=1e-12, block=None):
+                 tol=1e-9, pcg_tol=1e-12, block=None, warm_start=True, eig_scale=0.1,
+                 shift_ev=0.5):
         self.j = junction
         self.device = torch.device(device)
         self.k = int(k)
         self.nb = len(junction.biases)
         self.kT = K_B_EV * junction.T
+        # levels of the biased junction cross zero energy: errors are measured
+        # relative to max(|E|, eig_scale) (eV) rather than |E|
         self.solve_kw = dict(precision=precision, tol=tol, max_iter=4000,
-                             b=block or max(8, (self.k + 4 + 3) // 4 * 4))
+                             b=block or max(8, (self.k + 4 + 3) // 4 * 4),
+                             eig_scale=eig_scale)
         self.pcg_tol = pcg_tol
         mesh = junction.mesh
         self.n = mesh.num_nodes
@@ -58,6 +62,12 @@ class BatchedSC:
         self.hb = HostBatch(dots)
         self.db = DeviceBatch(self.hb, self.device)
         self.db.upload(non_blocking=False)
+        # DST preconditioner shift (eV): the junction's potential spans ~1 eV,
+        # and on the 64-bias config a 0.5 eV shift needs 56-72 LOBPCG
+        # iterations per self-consistent step where the sweep's 0.02 eV needs
+        # 144-168
+        if shift_ev is not None:
+            self.db.set_shift(shift_ev)
         dm, nrow = dof_map_for(mesh, True)
         self.rows = nrow
         self.d_dof = torch.from_numpy(dm).to(self.device)
@@ -69,6 +79,8 @@ class BatchedSC:
         self.p_h = torch.zeros(self.n, self.nb, **f64)
         self.rho = torch.zeros(self.n, self.nb, **f64)
         self._X = None          # last eigenvectors (warm start)
+        # warm-start each eigensolve from the previous iteration's vectors
+        self.warm_start = bool(warm_start)
         self.E = None
         self.X = None
 
@@ -79,7 +91,8 @@ class BatchedSC:
                                   N.ptr(self.db.d["V"]), stream_ptr()), "qd_sc_potential")
         self.db.assemble()
         # warm start from the last stored eigenvectors (random the first time)
-        E, X, _, _, info, _ = self.db.solve(self.k, x0=self._X, **self.solve_kw)
+        E, X, _, _, info, _ = self.db.solve(self.k, x0=self._X if self.warm_start else None,
+                                            **self.solve_kw)
         return E, X, info
 
     def g_map(self, phi, store=True):
