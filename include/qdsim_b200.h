@@ -281,7 +281,8 @@ int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_
  *     (cudaGetSymbolAddress, with that device current); make that first call
  *     before any stream capture.
  *   - All calls share the one array and it keeps the previous call's
- *     contents; every scratch word is rewritten before it is read, so nothing
+ *     contents; each call zeroes its block counter (a memset on the stream)
+ *     and rewrites every other scratch word before reading it, so nothing
  *     needs clearing, but calls that overlap on the GPU (other streams, other
  *     host threads) race on it and must be serialised by the caller. */
 size_t qd_pcg_static_scratch_bytes(void);

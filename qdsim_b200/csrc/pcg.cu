@@ -10,9 +10,18 @@
 //
 // Vectors are row-major (x[row*nrhs + j]).  Every thread owns one fixed
 // column j = tid % nrhs for the whole launch (block size and grid stride are
-// multiples of nrhs), so the per-column dot products reduce in a fixed order:
-// bitwise reproducible, no atomics.  The step scalars are computed on the
-// device; the host only reads the convergence flag every few iterations.
+// multiples of nrhs) and steps over rows, so the per-column dot products
+// reduce in a fixed order: bitwise reproducible, no atomics on values.
+//
+// One iteration is two launches.  (1) p = z + beta p_prev fused into
+// Ap = A p: every gathered neighbour value is recomputed as
+// fma(beta, p_prev, z), the same expression the row's owner stores, so the
+// product sees exactly the stored direction (p alternates between two
+// buffers).  (2) x += alpha p, r -= alpha Ap, z = D^-1 r.  Each launch leaves
+// per-block column partials; the block that finishes last (block counter)
+// sums them in block order and computes the step scalars, so no separate
+// reduction launch sits between the two.  The host reads only the
+// convergence flag, every 16 iterations.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -23,33 +32,105 @@
 namespace {
 
 constexpr int kMaxRhs = 256;
+constexpr int kThreads = 1024;     // per block, rounded down to a multiple of nrhs
+constexpr int kGridBlocks = 2 * 148;   // two blocks per SM of a B200 (32 registers)
 
 struct Cfg {
   int n, nrhs, threads, blocks;
 };
 
-__device__ inline void block_col_reduce(double v, double *red, int nrhs, double *out_block) {
-  // red: blockDim doubles; threads t and t' share a column iff t % nrhs == t' % nrhs
+// partials: part[(kind * nrhs + j) * blocks + block]; kinds 0 r.z, 1 r.r, 2 p.Ap
+// step scalars per column: sc[j * 5 + {0 rz, 1 rr0, 2 alpha, 3 beta, 4 rr}]
+
+// Column sums of this block's per-thread values into part[kind] (threads
+// t, t + nrhs, ... in order).
+__device__ inline void block_col_reduce(double v, double *red, const Cfg &c, double *part_k) {
   red[threadIdx.x] = v;
   __syncthreads();
-  if (threadIdx.x < nrhs) {
+  if (threadIdx.x < c.nrhs) {
     double s = 0.0;
-    for (int t = threadIdx.x; t < blockDim.x; t += nrhs) s += red[t];
-    out_block[threadIdx.x] = s;
+    for (int t = threadIdx.x; t < blockDim.x; t += c.nrhs) s += red[t];
+    part_k[size_t(threadIdx.x) * c.blocks + blockIdx.x] = s;
   }
   __syncthreads();
 }
 
-// r = b - A x (free rows), z = D^-1 r, p = z; partials: r.z and r.r
-__global__ void pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *A,
-                                const double *Bv, const double *X, const int32_t *fixed,
-                                double *R, double *Z, double *P, double *dinv, double *part) {
+// True in every thread of the block that finished last; that block then sees
+// every other block's partials.
+__device__ inline bool last_block(unsigned *counter) {
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
+// Sum over blocks of part[kind][j] for j = threadIdx.x / L, L = blockDim / nrhs
+// lanes per column: lane l takes blocks l, l + L, ..., then the lane sums are
+// added in lane order.  Valid in the threads with l == 0.
+__device__ inline double grid_col_sum(const double *part_k, const Cfg &c, double *red) {
+  const int L = blockDim.x / c.nrhs;
+  const int j = threadIdx.x / L, l = threadIdx.x % L;
+  double a = 0.0;
+  const double *src = part_k + size_t(j) * c.blocks;
+  for (int b = l; b < c.blocks; b += L) a += __ldcg(src + b);
+  red[threadIdx.x] = a;
+  __syncthreads();
+  double s = 0.0;
+  if (l == 0)
+    for (int q = 0; q < L; ++q) s += red[threadIdx.x + q];
+  __syncthreads();
+  return s;
+}
+
+// Step scalars in the last block.  mode 0: initial (rz, rr0, done); mode 1:
+// alpha = rz / pAp (0 for a converged column); mode 2: beta, rr, done.
+__device__ void finish_scalars(int mode, const Cfg &c, const double *part, double *sc, int *done,
+                               unsigned *counter, double tol, double *red) {
+  __shared__ int s_all;
+  if (threadIdx.x == 0) s_all = 1;
+  const double sa = grid_col_sum(part + size_t(mode == 1 ? 2 : 0) * c.nrhs * c.blocks, c, red);
+  const double sb = mode == 1 ? 0.0 : grid_col_sum(part + size_t(c.nrhs) * c.blocks, c, red);
+  const int L = blockDim.x / c.nrhs;
+  if (threadIdx.x % L == 0) {
+    double *s = sc + size_t(threadIdx.x / L) * 5;
+    if (mode == 0) {
+      s[0] = sa;
+      s[1] = sb;
+      s[2] = 0.0;
+      s[3] = 0.0;
+      s[4] = sb;
+      if (sb > 0.0) atomicAnd(&s_all, 0);
+    } else if (mode == 1) {
+      s[2] = (sa > 0.0 && s[4] > tol * tol * s[1]) ? s[0] / sa : 0.0;
+    } else {
+      s[3] = (s[0] > 0.0) ? sa / s[0] : 0.0;
+      s[0] = sa;
+      s[4] = sb;
+      if (!(sb <= tol * tol * s[1])) atomicAnd(&s_all, 0);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (mode != 1) *done = s_all;
+    *counter = 0u;
+  }
+}
+
+// r = b - A x (free rows), z = D^-1 r, p_prev = 0; partials r.z and r.r
+__global__ void __launch_bounds__(kThreads, 2)
+pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *A,
+                const double *Bv, const double *X, const int32_t *fixed, double *R, double *Z,
+                double *P, double *dinv, double *part, double *sc, int *done, unsigned *counter,
+                double tol) {
   extern __shared__ double red[];
-  const int stride = gridDim.x * blockDim.x;
+  const int j = threadIdx.x % c.nrhs, rpb = blockDim.x / c.nrhs;
+  const int step = gridDim.x * rpb;
   double rz = 0.0, rr = 0.0;
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < int64_t(c.n) * c.nrhs;
-       idx += stride) {
-    const int row = int(idx / c.nrhs), j = int(idx % c.nrhs);
+  for (int row = blockIdx.x * rpb + threadIdx.x / c.nrhs; row < c.n; row += step) {
+    const size_t idx = size_t(row) * c.nrhs + j;
     double r = 0.0, di = 0.0;
     if (!fixed || !fixed[row]) {
       double ax = 0.0, diag = 0.0;
@@ -65,106 +146,57 @@ __global__ void pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col
     const double z = r * di;
     R[idx] = r;
     Z[idx] = z;
-    P[idx] = z;
+    P[idx] = 0.0;
     rz += r * z;
     rr += r * r;
   }
-  block_col_reduce(rz, red, c.nrhs, part + size_t(blockIdx.x) * 3 * c.nrhs);
-  block_col_reduce(rr, red, c.nrhs, part + size_t(blockIdx.x) * 3 * c.nrhs + c.nrhs);
+  block_col_reduce(rz, red, c, part);
+  block_col_reduce(rr, red, c, part + size_t(c.nrhs) * c.blocks);
+  if (last_block(counter)) finish_scalars(0, c, part, sc, done, counter, tol, red);
 }
 
-// Ap = A p (free rows; p is zero on fixed rows); partial p.Ap
-__global__ void pcg_spmv_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *A,
-                                const int32_t *fixed, const double *P, double *AP,
-                                const int *done, double *part) {
+// p = z + beta p_prev, Ap = A p (free rows; p is zero on fixed rows); partial p.Ap
+__global__ void __launch_bounds__(kThreads, 2)
+pcg_spmv_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *A,
+                const int32_t *fixed, const double *Z, const double *Pprev, double *P, double *AP,
+                double *part, double *sc, int *done, unsigned *counter, double tol) {
   extern __shared__ double red[];
   if (*done) return;
-  const int stride = gridDim.x * blockDim.x;
+  const int j = threadIdx.x % c.nrhs, rpb = blockDim.x / c.nrhs;
+  const int step = gridDim.x * rpb;
+  const double beta = sc[size_t(j) * 5 + 3];
   double pap = 0.0;
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < int64_t(c.n) * c.nrhs;
-       idx += stride) {
-    const int row = int(idx / c.nrhs), j = int(idx % c.nrhs);
+  for (int row = blockIdx.x * rpb + threadIdx.x / c.nrhs; row < c.n; row += step) {
+    const size_t idx = size_t(row) * c.nrhs + j;
     double ap = 0.0;
     if (!fixed || !fixed[row]) {
-      for (int p = rowptr[row]; p < rowptr[row + 1]; ++p)
-        ap = fma(A[p], P[size_t(col[p]) * c.nrhs + j], ap);
+      for (int p = rowptr[row]; p < rowptr[row + 1]; ++p) {
+        const size_t q = size_t(col[p]) * c.nrhs + j;
+        ap = fma(A[p], fma(beta, Pprev[q], Z[q]), ap);
+      }
     }
+    const double pi = fma(beta, Pprev[idx], Z[idx]);
+    P[idx] = pi;
     AP[idx] = ap;
-    pap += P[idx] * ap;
+    pap += pi * ap;
   }
-  block_col_reduce(pap, red, c.nrhs, part + size_t(blockIdx.x) * 3 * c.nrhs + 2 * c.nrhs);
-}
-
-// scalars: mode 0 -> initial (rz, rr0); mode 1 -> alpha = rz / pAp; mode 2 -> beta, convergence
-// The per-block partials of a column are summed by L = kScalarThreads / nrhs
-// lanes (lane l takes blocks l, l + L, ...), then the L lane sums in lane
-// order: a fixed order, so the result is reproducible.
-constexpr int kScalarThreads = 1024;
-
-__global__ void __launch_bounds__(kScalarThreads)
-pcg_scalar_kernel(Cfg c, int mode, const double *part, double *sc, int *done, double tol) {
-  // sc layout per column: [rz, rr0, alpha, beta, rr]
-  __shared__ double s_a[kScalarThreads], s_b[kScalarThreads];
-  __shared__ int s_all;
-  const int t = threadIdx.x;
-  const int L = kScalarThreads / c.nrhs;
-  const int j = t / L, l = t % L;
-  if (t == 0) s_all = 1;
-  // partial kinds: 0 r.z, 1 r.r (modes 0, 2); 2 p.Ap (mode 1)
-  const int ka = mode == 1 ? 2 : 0, kb = 1;
-  double a = 0.0, b = 0.0;
-  if (j < c.nrhs) {
-    for (int blk = l; blk < c.blocks; blk += L) {
-      a += part[size_t(blk) * 3 * c.nrhs + size_t(ka) * c.nrhs + j];
-      if (mode != 1) b += part[size_t(blk) * 3 * c.nrhs + size_t(kb) * c.nrhs + j];
-    }
-  }
-  s_a[t] = a;
-  s_b[t] = b;
-  __syncthreads();
-  if (j < c.nrhs && l == 0) {
-    double sa = 0.0, sb = 0.0;
-    for (int q = 0; q < L; ++q) {
-      sa += s_a[t + q];
-      sb += s_b[t + q];
-    }
-    double *s = sc + size_t(j) * 5;
-    if (mode == 0) {
-      const double rz = sa, rr = sb;
-      s[0] = rz;
-      s[1] = rr;
-      s[4] = rr;
-      if (!(rr > 0.0)) s[2] = 0.0;
-      const bool conv = !(rr > 0.0);
-      if (!conv) atomicAnd(&s_all, 0);
-    } else if (mode == 1) {
-      const double pap = sa;
-      s[2] = (pap > 0.0 && s[4] > tol * tol * s[1]) ? s[0] / pap : 0.0;
-    } else {
-      const double rz = sa, rr = sb;
-      s[3] = (s[0] > 0.0) ? rz / s[0] : 0.0;
-      s[0] = rz;
-      s[4] = rr;
-      const bool conv = rr <= tol * tol * s[1];
-      if (!conv) atomicAnd(&s_all, 0);
-    }
-  }
-  __syncthreads();
-  if (t == 0 && mode != 1) *done = s_all;
+  block_col_reduce(pap, red, c, part + size_t(2) * c.nrhs * c.blocks);
+  if (last_block(counter)) finish_scalars(1, c, part, sc, done, counter, tol, red);
 }
 
 // x += alpha p, r -= alpha Ap, z = D^-1 r; partials r.z, r.r
-__global__ void pcg_axpy_kernel(Cfg c, const double *sc, const double *dinv, double *X, double *R,
-                                double *Z, const double *P, const double *AP, const int *done,
-                                double *part) {
+__global__ void __launch_bounds__(kThreads, 2)
+pcg_axpy_kernel(Cfg c, const double *dinv, double *X, double *R, double *Z, const double *P,
+                const double *AP, double *part, double *sc, int *done, unsigned *counter,
+                double tol) {
   extern __shared__ double red[];
   if (*done) return;
-  const int stride = gridDim.x * blockDim.x;
+  const int j = threadIdx.x % c.nrhs, rpb = blockDim.x / c.nrhs;
+  const int step = gridDim.x * rpb;
+  const double alpha = sc[size_t(j) * 5 + 2];
   double rz = 0.0, rr = 0.0;
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < int64_t(c.n) * c.nrhs;
-       idx += stride) {
-    const int row = int(idx / c.nrhs), j = int(idx % c.nrhs);
-    const double alpha = sc[size_t(j) * 5 + 2];
+  for (int row = blockIdx.x * rpb + threadIdx.x / c.nrhs; row < c.n; row += step) {
+    const size_t idx = size_t(row) * c.nrhs + j;
     X[idx] = fma(alpha, P[idx], X[idx]);
     const double r = fma(-alpha, AP[idx], R[idx]);
     const double z = r * dinv[row];
@@ -173,45 +205,87 @@ __global__ void pcg_axpy_kernel(Cfg c, const double *sc, const double *dinv, dou
     rz += r * z;
     rr += r * r;
   }
-  block_col_reduce(rz, red, c.nrhs, part + size_t(blockIdx.x) * 3 * c.nrhs);
-  block_col_reduce(rr, red, c.nrhs, part + size_t(blockIdx.x) * 3 * c.nrhs + c.nrhs);
-}
-
-__global__ void pcg_dir_kernel(Cfg c, const double *sc, const double *Z, double *P, const int *done) {
-  if (*done) return;
-  const int stride = gridDim.x * blockDim.x;
-  for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < int64_t(c.n) * c.nrhs;
-       idx += stride) {
-    const int j = int(idx % c.nrhs);
-    P[idx] = fma(sc[size_t(j) * 5 + 3], P[idx], Z[idx]);
-  }
+  block_col_reduce(rz, red, c, part);
+  block_col_reduce(rr, red, c, part + size_t(c.nrhs) * c.blocks);
+  if (last_block(counter)) finish_scalars(2, c, part, sc, done, counter, tol, red);
 }
 
 Cfg make_cfg(int n, int nrhs) {
   Cfg c;
   c.n = n;
   c.nrhs = nrhs;
-  c.threads = (256 / nrhs) * nrhs;
-  int64_t want = (int64_t(n) * nrhs + c.threads - 1) / c.threads;
-  c.blocks = int(std::min<int64_t>(std::max<int64_t>(want, 1), 148 * 8));
+  c.threads = (kThreads / nrhs) * nrhs;
+  const int rpb = c.threads / nrhs;
+  const int want = (n + rpb - 1) / rpb;
+  c.blocks = std::min(std::max(want, 1), kGridBlocks);
   return c;
 }
 
 struct PcgLayout {
-  double *R, *Z, *P, *AP, *dinv, *part, *sc;
+  double *R, *Z, *P[2], *AP, *dinv, *part, *sc;
   int *done;
+  unsigned *counter;
 };
 
 void carve(qd::Arena &ar, const Cfg &c, PcgLayout &L) {
   const size_t nv = size_t(c.n) * c.nrhs;
   L.R = ar.take<double>(nv);
   L.Z = ar.take<double>(nv);
-  L.P = ar.take<double>(nv);
+  L.P[0] = ar.take<double>(nv);
+  L.P[1] = ar.take<double>(nv);
   L.AP = ar.take<double>(nv);
   L.dinv = ar.take<double>(c.n);
   L.part = ar.take<double>(size_t(c.blocks) * 3 * c.nrhs);
   L.sc = ar.take<double>(size_t(c.nrhs) * 5);
   L.done = ar.take<int>(4);
+  L.counter = ar.take<unsigned>(4);
+}
+
+// The iteration on a carved layout.  The block counter is zeroed first; every
+// other scratch word is written before it is read.
+int run_pcg(const Cfg &c, const PcgLayout &L, const int32_t *d_rowptr, const int32_t *d_col,
+            const double *d_A, const double *d_B, double *d_X, const int32_t *d_fixed,
+            double tol, int max_iter, int32_t *h_iters, double *h_relres, cudaStream_t s) {
+  const size_t smem = size_t(c.threads) * sizeof(double);
+  QD_CUDA_TRY(cudaMemsetAsync(L.counter, 0, 4 * sizeof(unsigned), s));
+  pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
+                                                    L.R, L.Z, L.P[0], L.dinv, L.part, L.sc,
+                                                    L.done, L.counter, tol);
+  QD_CHECK_LAUNCH();
+  int it = 0, done = 0;
+  const int check = 16;
+  for (it = 0; it < max_iter; ++it) {
+    const double *Pprev = L.P[it & 1];
+    double *P = L.P[(it + 1) & 1];
+    pcg_spmv_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_fixed, L.Z,
+                                                      Pprev, P, L.AP, L.part, L.sc, L.done,
+                                                      L.counter, tol);
+    QD_CHECK_LAUNCH();
+    pcg_axpy_kernel<<<c.blocks, c.threads, smem, s>>>(c, L.dinv, d_X, L.R, L.Z, P, L.AP, L.part,
+                                                      L.sc, L.done, L.counter, tol);
+    QD_CHECK_LAUNCH();
+    if ((it + 1) % check == 0 || it + 1 == max_iter) {
+      QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
+      QD_CUDA_TRY(cudaStreamSynchronize(s));
+      if (done) {
+        ++it;
+        break;
+      }
+    }
+  }
+  double sc[kMaxRhs * 5];
+  QD_CUDA_TRY(cudaMemcpyAsync(sc, L.sc, size_t(c.nrhs) * 5 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QD_CUDA_TRY(cudaStreamSynchronize(s));
+  double worst = 0.0;
+  for (int j = 0; j < c.nrhs; ++j) {
+    const double rr0 = sc[size_t(j) * 5 + 1], rr = sc[size_t(j) * 5 + 4];
+    worst = std::max(worst, rr0 > 0.0 ? std::sqrt(rr / rr0) : 0.0);
+  }
+  if (h_iters) *h_iters = it;
+  if (h_relres) *h_relres = worst;
+  return done ? QD_OK : QD_ERR_NOT_CONVERGED;
 }
 
 }  // namespace
@@ -244,50 +318,8 @@ extern "C" int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const 
   qd::Arena ar(d_work, work_bytes);
   PcgLayout L;
   carve(ar, c, L);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t smem = size_t(c.threads) * sizeof(double);
-  pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
-                                                    L.R, L.Z, L.P, L.dinv, L.part);
-  QD_CHECK_LAUNCH();
-  pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
-  QD_CHECK_LAUNCH();
-  int it = 0, done = 0;
-  const int check = 16;
-  for (it = 0; it < max_iter; ++it) {
-    pcg_spmv_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_fixed, L.P,
-                                                      L.AP, L.done, L.part);
-    QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
-    QD_CHECK_LAUNCH();
-    pcg_axpy_kernel<<<c.blocks, c.threads, smem, s>>>(c, L.sc, L.dinv, d_X, L.R, L.Z, L.P, L.AP,
-                                                      L.done, L.part);
-    QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
-    QD_CHECK_LAUNCH();
-    pcg_dir_kernel<<<c.blocks, c.threads, 0, s>>>(c, L.sc, L.Z, L.P, L.done);
-    QD_CHECK_LAUNCH();
-    if ((it + 1) % check == 0 || it + 1 == max_iter) {
-      QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
-      QD_CUDA_TRY(cudaStreamSynchronize(s));
-      if (done) {
-        ++it;
-        break;
-      }
-    }
-  }
-  std::vector<double> sc(size_t(c.nrhs) * 5);
-  QD_CUDA_TRY(cudaMemcpyAsync(sc.data(), L.sc, sc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-  QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
-  QD_CUDA_TRY(cudaStreamSynchronize(s));
-  double worst = 0.0;
-  for (int j = 0; j < c.nrhs; ++j) {
-    const double rr0 = sc[size_t(j) * 5 + 1], rr = sc[size_t(j) * 5 + 4];
-    const double rel = rr0 > 0.0 ? std::sqrt(rr / rr0) : 0.0;
-    worst = std::max(worst, rel);
-  }
-  if (h_iters) *h_iters = it;
-  if (h_relres) *h_relres = worst;
-  return done ? QD_OK : QD_ERR_NOT_CONVERGED;
+  return run_pcg(c, L, d_rowptr, d_col, d_A, d_B, d_X, d_fixed, tol, max_iter, h_iters,
+                 h_relres, static_cast<cudaStream_t>(stream));
 }
 
 // Y = alpha * A X for nrhs row-major columns (generic CSR product, FP64).
@@ -374,50 +406,10 @@ extern "C" int qd_pcg_solve_static(int32_t n, int nrhs, const int32_t *d_rowptr,
   qd::Arena ar(scratch, kStaticScratchBytes);
   PcgLayout L;
   carve(ar, c, L);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t smem = size_t(c.threads) * sizeof(double);
-  // Every scratch word (residual, search direction, partial sums, step scalars
-  // and the done flag) is written before it is read in this call, so the
-  // contents left by an earlier call need no clearing.
-  pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
-                                                    L.R, L.Z, L.P, L.dinv, L.part);
-  QD_CHECK_LAUNCH();
-  pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 0, L.part, L.sc, L.done, tol);
-  QD_CHECK_LAUNCH();
-  int it = 0, done = 0;
-  for (it = 0; it < max_iter; ++it) {
-    pcg_spmv_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_fixed, L.P,
-                                                      L.AP, L.done, L.part);
-    QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 1, L.part, L.sc, L.done, tol);
-    QD_CHECK_LAUNCH();
-    pcg_axpy_kernel<<<c.blocks, c.threads, smem, s>>>(c, L.sc, L.dinv, d_X, L.R, L.Z, L.P, L.AP,
-                                                      L.done, L.part);
-    QD_CHECK_LAUNCH();
-    pcg_scalar_kernel<<<1, kScalarThreads, 0, s>>>(c, 2, L.part, L.sc, L.done, tol);
-    QD_CHECK_LAUNCH();
-    pcg_dir_kernel<<<c.blocks, c.threads, 0, s>>>(c, L.sc, L.Z, L.P, L.done);
-    QD_CHECK_LAUNCH();
-    if ((it + 1) % 16 == 0 || it + 1 == max_iter) {
-      QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
-      QD_CUDA_TRY(cudaStreamSynchronize(s));
-      if (done) {
-        ++it;
-        break;
-      }
-    }
-  }
-  double sc[kMaxRhs * 5];
-  QD_CUDA_TRY(cudaMemcpyAsync(sc, L.sc, size_t(c.nrhs) * 5 * sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
-  QD_CUDA_TRY(cudaMemcpyAsync(&done, L.done, sizeof(int), cudaMemcpyDeviceToHost, s));
-  QD_CUDA_TRY(cudaStreamSynchronize(s));
-  double worst = 0.0;
-  for (int j = 0; j < c.nrhs; ++j) {
-    const double rr0 = sc[size_t(j) * 5 + 1], rr = sc[size_t(j) * 5 + 4];
-    worst = std::max(worst, rr0 > 0.0 ? std::sqrt(rr / rr0) : 0.0);
-  }
-  if (h_iters) *h_iters = it;
-  if (h_relres) *h_relres = worst;
-  return done ? QD_OK : QD_ERR_NOT_CONVERGED;
+  // The block counter is zeroed at the start of the call and every other
+  // scratch word (residual, search directions, partial sums, step scalars,
+  // done flag) is written before it is read, so the contents left by an
+  // earlier call need no clearing.
+  return run_pcg(c, L, d_rowptr, d_col, d_A, d_B, d_X, d_fixed, tol, max_iter, h_iters,
+                 h_relres, static_cast<cudaStream_t>(stream));
 }
