@@ -243,6 +243,90 @@ def sc_measurement(dev):
                                    f"2 bias points x 2 iterations, {t_cpu:.1f} s"}}
 
 
+GOLDEN_C2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                         "c2_nearest20.npz")
+
+
+def cap_spmm_bytes(n, nnz, b, s):
+    """Algorithmic bytes of one qd_cap_spmm launch: column index and the three
+    matrix values per nonzero (s bytes each), row pointers, the block of b
+    complex vectors read once and AX, MX written (2 s bytes per complex)."""
+    return nnz * (4 + 3 * s) + 4 * (n + 1) + 3 * n * b * 2 * s
+
+
+def cap_measurement(dev):
+    """Open system (P2 400x200 cells on 200x100 nm, 318,801 DOFs, CAP -i 50 meV
+    (d/10 nm)^2): the 20 eigenvalues nearest -0.05 eV, in the mixed form (FP32
+    vector phase, then FP64) and the plain FP64 form, each checked against the
+    committed oracle eigenvalues; the product kernel timed alone against the
+    HBM peak; beside them the oracle's shift-invert eigs on the same pencil at
+    quarter size (P2 200x100 cells) on the host."""
+    import torch
+    from qdsim_b200 import cap as CP, workloads as W
+    d = W.c2_dot(0)
+    t0 = time.perf_counter()
+    solver = CP.CAPSolver(d.mesh, d.c, d.V, d.W, device=dev)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    prob = solver.prob
+    gold = np.load(GOLDEN_C2)["E"] if os.path.exists(GOLDEN_C2) else None
+    solver.solve(k=20, sigma=-0.05, nev=40, b=48, precision="mixed", max_iter=3)   # warm-up
+    out = {"workload": "open system, P2 400x200 cells on 200x100 nm, CAP W=50 meV in a 10 nm "
+                       "layer, 20 eigenvalues nearest -0.05 eV (lowest 40 by real part, block 48)",
+           "dofs": prob.n, "nnz": int(prob.fem.nnz), "setup_s": t_setup}
+    for prec in ("mixed", "fp64"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = solver.solve(k=20, sigma=-0.05, nev=40, b=48, precision=prec, tol=1e-9)
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        r = {"seconds": secs, "iterations": res.info["iterations"],
+             "iters_fp32": res.info["iters_fp32"], "iters_fp64": res.info["iters_fp64"],
+             "complete": res.info["complete"], "max_residual": res.info["max_residual"]}
+        if gold is not None:
+            err = np.array([np.min(np.abs(res.E - g)) / abs(g) for g in gold])
+            good = int((err <= 1e-9).sum()) if res.info["complete"] else 0
+            r.update(max_rel_err_vs_oracle=float(err.max()), converged_pairs=good,
+                     eigenpairs_per_s=good / secs)
+        out[prec] = r
+    if "eigenpairs_per_s" in out["mixed"] and out["fp64"].get("eigenpairs_per_s"):
+        out["mixed_over_plain"] = out["mixed"]["eigenpairs_per_s"] / out["fp64"]["eigenpairs_per_s"]
+    # the product kernel alone, b = 48 complex columns
+    peak = FALLBACK_HBM
+    if os.path.exists(PEAKS):
+        with open(PEAKS) as f:
+            peak = float(json.load(f).get("hbm_gbs", FALLBACK_HBM))
+    kern = {}
+    for ct, s, tag in ((torch.complex64, 4, "fp32"), (torch.complex128, 8, "fp64")):
+        X = torch.randn(prob.n, 48, dtype=ct, device=dev)
+        AX, MX = torch.empty_like(X), torch.empty_like(X)
+        for _ in range(3):
+            prob.spmm(X, AX, MX)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            prob.spmm(X, AX, MX)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        gbs = cap_spmm_bytes(prob.n, prob.fem.nnz, 48, s) / (ms * 1e-3) / 1e9
+        kern[tag] = {"ms": ms, "GBps": gbs, "frac": gbs / peak}
+        del X, AX, MX
+    out["cap_spmm_b48"] = kern
+    # host: the oracle's shift-invert eigs at quarter size
+    from oracle import fem as O
+    dq = W.c2_dot(0, nx=200, ny=100)
+    om = O.structured_mesh(2, 200, 100, 200.0, 100.0)
+    a = O.assemble(om, dq.c, dq.V, dq.W)
+    t0 = time.perf_counter()
+    O.eig_nearest_complex(a.H - 1j * a.Wm, a.M, 20, -0.05)
+    t_cpu = time.perf_counter() - t0
+    out["cpu_port"] = {"seconds": t_cpu, "eigenpairs_per_s": 20 / t_cpu, "dofs": a.n,
+                       "sample": "oracle shift-invert eigs (complex splu + ARPACK) on the same "
+                                 "pencil at quarter size, P2 200x100 cells"}
+    return out
+
+
 def algorithmic_bytes(hb, counts, k_block):
     """Algorithmic bytes per kernel kind, from the per-dot launch counts.
 
@@ -491,6 +575,10 @@ def main():
             del sdb, sub
             result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
             result["sc_junction"] = sc_measurement(dev)
+            try:
+                result["cap_open_system"] = cap_measurement(dev)
+            except Exception as e:   # recorded; the headline line stands
+                result["cap_open_system"] = {"error": repr(e)}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -297,6 +297,19 @@ int qd_pcg_solve_static(int32_t n, int nrhs, const int32_t *d_rowptr, const int3
 int qd_csr_spmv(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_col,
                 const double *d_A, const double *d_X, double *d_Y, double alpha, void *stream);
 
+/* Open-system (CAP) pencil products: AX = (H + i Himag) X and MX = M X for b
+ * complex vectors (1 <= b <= 64), row-major with re/im interleaved,
+ * X[row * ldx + c] and AX/MX[row * ldy + c] (leading dimensions in complex
+ * elements, >= b).  H, Himag and M share one CSR pattern (qd_assemble's
+ * outputs); Himag may be NULL (Hermitian pencil).  vec_fp32 selects
+ * float/float2 for the matrix values and vectors, else double/double2.
+ * Replaces the complex SpMV inside scipy's shift-invert eigs, which the
+ * oracle of the complex eigenvalue configuration runs, and the dense complex
+ * solve of backend/src/schrodinger.cpp:699-818. */
+int qd_cap_spmm(int32_t n, int b, int vec_fp32, const int32_t *d_rowptr, const int32_t *d_col,
+                const void *d_H, const void *d_Himag, const void *d_M, const void *d_X, int ldx,
+                void *d_AX, void *d_MX, int ldy, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Adjoint (Hellmann-Feynman) gradients of L = sum_s w_s E_s with respect to
  * nodal V and the per-element kinetic coefficient c.  With M-normalised
