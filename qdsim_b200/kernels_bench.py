@@ -1,0 +1,91 @@
+"""Run one kernel family on a named workload and report its CUDA-event time.
+
+    python -m qdsim_b200.kernels_bench cap_spmm [--prec fp64|fp32] [--b 48] [--launches 10]
+    python -m qdsim_b200.kernels_bench pcg [--iters 32]
+
+``cap_spmm``: ``qd_cap_spmm`` on the open-system pencil of P2 400x200 cells on
+200x100 nm (318,801 DOFs, 3.65M nonzeros) for a block of b complex columns;
+prints ms per launch and GB/s of algorithmic bytes.  ``pcg``: the Jacobi-PCG
+of the p-n junction's Poisson step (P1 300x100 cells, 30,401 nodes, 64
+right-hand sides) for a fixed number of iterations; prints ms per iteration.
+The launch sequence is fixed, so a profiler can select launches by index.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+import torch
+
+
+def cap_spmm(prec: str, b: int, launches: int, dev):
+    from .cap import CAPProblem
+    from .workloads import c2_dot
+    d = c2_dot(0)
+    prob = CAPProblem(d.mesh, d.c, d.V, d.W, device=dev)
+    ct, s = (torch.complex64, 4) if prec == "fp32" else (torch.complex128, 8)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    X = torch.view_as_complex(torch.randn(prob.n, b, 2, generator=g)).to(dev, ct)
+    AX, MX = torch.empty_like(X), torch.empty_like(X)
+    prob.spmm(X, AX, MX)                        # launch 0 (warm-up)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        prob.spmm(X, AX, MX)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    nnz = prob.fem.nnz
+    alg = nnz * (4 + 3 * s) + 4 * (prob.n + 1) + 3 * prob.n * b * 2 * s
+    return {"kernel": "cap_spmm_kernel", "prec": prec, "b": b, "rows": prob.n, "nnz": int(nnz),
+            "ms_per_launch": ms, "algorithmic_bytes": int(alg), "GBps": alg / (ms * 1e-3) / 1e9}
+
+
+def pcg(iters: int, dev):
+    from . import _native as N
+    from .poisson import PoissonProblem
+    from .workloads import c5_junction
+    j = c5_junction(64)
+    prob = PoissonProblem(j.mesh, j.eps_r, device=dev)
+    rng = np.random.default_rng(0)
+    rho = 1.6e5 * rng.standard_normal((j.mesh.num_nodes, 64))
+    out = {}
+    for tag, it in (("warm-up", 2), ("timed", iters)):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        try:
+            prob.solve(rho, 0.0, np.asarray(j.biases), tol=1e-300, max_iter=it)
+        except N.QDError as e:
+            if e.status != N.QD_ERR_NOT_CONVERGED:
+                raise
+        e1.record()
+        torch.cuda.synchronize()
+        out[tag] = e0.elapsed_time(e1)
+    n, nnz = j.mesh.num_nodes, prob.fem.nnz
+    alg = nnz * 12 + 4 * (n + 1) + 11 * n * 8 * 64
+    ms = out["timed"] / iters
+    return {"kernels": ["pcg_spmv_kernel", "pcg_axpy_kernel"], "nodes": n, "nnz": int(nnz),
+            "nrhs": 64, "iterations": iters, "ms_per_iteration": ms,
+            "algorithmic_bytes_per_iteration": int(alg), "GBps": alg / (ms * 1e-3) / 1e9}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("case", choices=["cap_spmm", "pcg"])
+    ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--b", type=int, default=48)
+    ap.add_argument("--launches", type=int, default=10)
+    ap.add_argument("--iters", type=int, default=32)
+    a = ap.parse_args(argv)
+    if not torch.cuda.is_available():
+        raise SystemExit("a CUDA device is required")
+    dev = torch.device("cuda:0")
+    r = cap_spmm(a.prec, a.b, a.launches, dev) if a.case == "cap_spmm" else pcg(a.iters, dev)
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()
