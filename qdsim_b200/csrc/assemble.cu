@@ -5,10 +5,12 @@
 // 46-336, 442-745) and the host triplet scatter of
 // GPUAccelerator::assemble_matrices (backend/src/gpu_accelerator.cpp:439-642).
 //
-// Each warp owns one reduced row r.  Lanes first stage the row's incident
-// elements (geometry, coefficient, nodal V/W) in shared memory, then each lane
-// owns one CSR slot of the row and sums that slot's contributions in the fixed
-// (element id, local column) order given by the host plan.  No atomics, so the
+// Each reduced row r is owned by a segment of 8 (P1), 16 (P2) or 32 (P3)
+// lanes, so a warp advances 4, 2 or 1 rows at once.  The segment first stages
+// the row's incident elements (geometry, coefficient, nodal V/W) in shared
+// memory, then each lane owns CSR slots of the row and sums each slot's
+// contributions in the fixed (element id, local column) order given by the
+// host plan.  No atomics, so the
 // result is bitwise reproducible; every slot is written exactly once and the
 // row's slots are contiguous, so stores are coalesced.
 //
@@ -31,18 +33,27 @@ std::atomic<uint64_t> g_launches{0};
 namespace {
 
 constexpr int kMaxAdj = 16;   // incident elements per row (pattern builder enforces)
-constexpr int kWarps = 8;
+
+// Lanes per row and threads per block by element order: a P1 row has at most
+// 7 slots in a structured mesh, a P2 row 19, a P3 row 37, so P1 rows get 8
+// lanes (four rows per warp), P2 rows 16 (two per warp), P3 rows a warp.
+template <int K> struct RowShape;
+template <> struct RowShape<3> { static constexpr int LPR = 8, THREADS = 128; };
+template <> struct RowShape<6> { static constexpr int LPR = 16, THREADS = 256; };
+template <> struct RowShape<10> { static constexpr int LPR = 32, THREADS = 256; };
 
 template <int K>
-struct __align__(8) RowStage {
+struct __align__(16) RowStage {
   double cA[kMaxAdj], A[kMaxAdj], g00[kMaxAdj], g01[kMaxAdj], g11[kMaxAdj];
   double V[kMaxAdj][K];
   double W[kMaxAdj][K];
   int a[kMaxAdj];
 };
 
-template <int K>
-__global__ void __launch_bounds__(kWarps * 32)
+// HAS_W: a CAP amplitude is given (Himag is assembled); without it the W
+// staging and the W sums are compiled out.
+template <int K, bool HAS_W>
+__global__ void __launch_bounds__(RowShape<K>::THREADS)
 assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
                      const int32_t *__restrict__ elems, const double *__restrict__ cvec,
                      const double *__restrict__ V, const double *__restrict__ W,
@@ -53,21 +64,35 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
                      int32_t *__restrict__ status) {
   constexpr int KK = K * K;
   constexpr int NT = 4 * KK + K * KK;
-  __shared__ double s_tab[NT];
-  __shared__ RowStage<K> s_stage[kWarps];
-  for (int i = threadIdx.x; i < NT; i += blockDim.x) s_tab[i] = c_tab[TabBase<K>::v + i];
+  constexpr int LPR = RowShape<K>::LPR;
+  constexpr int RPB = RowShape<K>::THREADS / LPR;   // rows in flight per block
+  __shared__ __align__(16) double s_tab[NT];
+  __shared__ RowStage<K> s_stage[RPB];
+  // Mr, Sxx, Sxy, Syy as stored; the potential table transposed to T[ab][l]
+  // so that a contribution reads its K weights contiguously
+  for (int i = threadIdx.x; i < NT; i += blockDim.x) {
+    if (i < 4 * KK) {
+      s_tab[i] = c_tab[TabBase<K>::v + i];
+    } else {
+      const int l = (i - 4 * KK) / KK, ab = (i - 4 * KK) % KK;
+      s_tab[4 * KK + ab * K + l] = c_tab[TabBase<K>::v + i];
+    }
+  }
   __syncthreads();
   const double *Mr = s_tab, *Sxx = s_tab + KK, *Sxy = s_tab + 2 * KK, *Syy = s_tab + 3 * KK;
   const double *T = s_tab + 4 * KK;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  RowStage<K> &st = s_stage[warp];
-  const unsigned FULL = 0xffffffffu;
+  const int seg = threadIdx.x / LPR, lane = threadIdx.x % LPR;
+  RowStage<K> &st = s_stage[seg];
+  // rows of one warp are independent: every shuffle and warp barrier names
+  // only the lanes of this row's segment
+  const unsigned mask = LPR == 32 ? 0xffffffffu
+                                  : ((1u << (LPR & 31)) - 1u) << ((threadIdx.x & 31) & ~(LPR - 1));
 
-  for (int32_t r = blockIdx.x * kWarps + warp; r < n; r += gridDim.x * kWarps) {
+  for (int32_t r = blockIdx.x * RPB + seg; r < n; r += gridDim.x * RPB) {
     const int t0 = adjptr[r];
     const int m = adjptr[r + 1] - t0;
-    if (lane < m) {
-      const int packed = adj[t0 + lane];
+    for (int t = lane; t < m; t += LPR) {
+      const int packed = adj[t0 + t];
       const int e = packed >> 4;
       const double2 p0 = nodes[elems[e * K + 0]];
       const double2 p1 = nodes[elems[e * K + 1]];
@@ -77,46 +102,46 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
       const double A = 0.5 * fabs(det);
       const double inv2 = 1.0 / (det * det);
       const double ce = cvec[e];
-      st.g00[lane] = (jd * jd + jb * jb) * inv2;
-      st.g01[lane] = -(jd * jc + jb * ja) * inv2;
-      st.g11[lane] = (jc * jc + ja * ja) * inv2;
-      st.cA[lane] = ce * A;
-      st.A[lane] = A;
-      st.a[lane] = packed & 15;
+      st.g00[t] = (jd * jd + jb * jb) * inv2;
+      st.g01[t] = -(jd * jc + jb * ja) * inv2;
+      st.g11[t] = (jc * jc + ja * ja) * inv2;
+      st.cA[t] = ce * A;
+      st.A[t] = A;
+      st.a[t] = packed & 15;
       if (!(det != 0.0) || !isfinite(det) || !isfinite(ce)) atomicOr(status, 1);
       if (mode != QD_ASM_FEM) {
         const double ve = V[e];
-        st.V[lane][0] = ve;
+        st.V[t][0] = ve;
         if (!isfinite(ve)) atomicOr(status, 2);
       }
     }
     if (mode == QD_ASM_FEM) {
-      for (int idx = lane; idx < m * K; idx += 32) {
+      for (int idx = lane; idx < m * K; idx += LPR) {
         const int t = idx / K, l = idx - t * K;
         const int e = adj[t0 + t] >> 4;
         const int g = elems[e * K + l];
         const double v = V[g];
         st.V[t][l] = v;
-        st.W[t][l] = W ? W[g] : 0.0;
+        if (HAS_W) st.W[t][l] = W[g];
         if (!isfinite(v)) atomicOr(status, 2);
       }
     }
-    __syncwarp();
+    __syncwarp(mask);
     const int rp = rowptr[r];
     const int L = rowptr[r + 1] - rp;
     const int cbase = cptr[r];
     int carry = 0;
-    for (int s0 = 0; s0 < L; s0 += 32) {
+    for (int s0 = 0; s0 < L; s0 += LPR) {
       const int s = s0 + lane;
       const int cnt = (s < L) ? int(slotcnt[rp + s]) : 0;
       int incl = cnt;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(FULL, incl, o);
+      for (int o = 1; o < LPR; o <<= 1) {
+        const int y = __shfl_up_sync(mask, incl, o, LPR);
         if (lane >= o) incl += y;
       }
       const int start = carry + incl - cnt;
-      carry += __shfl_sync(FULL, incl, 31);
+      carry += __shfl_sync(mask, incl, LPR - 1, LPR);
       if (s < L) {
         double h = 0.0, mm = 0.0, wi = 0.0;
         for (int q = 0; q < cnt; ++q) {
@@ -128,12 +153,32 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
           double hk;
           if (mode == QD_ASM_FEM) {
             hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]);
+            const double *tw = T + ab * K;
             double vs = 0.0, ws = 0.0;
+            if constexpr (K % 2 == 0) {
+              const double2 *t2 = reinterpret_cast<const double2 *>(tw);
+              const double2 *v2 = reinterpret_cast<const double2 *>(st.V[t]);
 #pragma unroll
-            for (int l = 0; l < K; ++l) {
-              const double tl = T[l * KK + ab];
-              vs += st.V[t][l] * tl;
-              ws += st.W[t][l] * tl;
+              for (int l = 0; l < K / 2; ++l) {
+                const double2 tl = t2[l], vl = v2[l];
+                vs += vl.x * tl.x;
+                vs += vl.y * tl.y;
+              }
+              if (HAS_W) {
+                const double2 *w2 = reinterpret_cast<const double2 *>(st.W[t]);
+#pragma unroll
+                for (int l = 0; l < K / 2; ++l) {
+                  const double2 tl = t2[l], wl = w2[l];
+                  ws += wl.x * tl.x;
+                  ws += wl.y * tl.y;
+                }
+              }
+            } else {
+#pragma unroll
+              for (int l = 0; l < K; ++l) {
+                vs += st.V[t][l] * tw[l];
+                if (HAS_W) ws += st.W[t][l] * tw[l];
+              }
             }
             hk += At * vs;
             wi -= At * ws;
@@ -152,7 +197,7 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
         if (Him) Him[rp + s] = wi;
       }
     }
-    __syncwarp();
+    __syncwarp(mask);
   }
 }
 
@@ -163,12 +208,18 @@ int launch_assemble(int mode, int32_t n, const double *nodes, const int32_t *ele
                     const uint8_t *contrib, const uint8_t *slotcnt, double *H, double *M,
                     double *Him, int32_t *status, cudaStream_t s) {
   if (n == 0) return QD_OK;
-  int64_t blocks = (int64_t(n) + kWarps - 1) / kWarps;
+  constexpr int RPB = RowShape<K>::THREADS / RowShape<K>::LPR;
+  int64_t blocks = (int64_t(n) + RPB - 1) / RPB;
   if (blocks > 148 * 64) blocks = 148 * 64;
   qd::prof_begin(qd::PK_ASSEMBLE, s);
-  assemble_rows_kernel<K><<<int(blocks), kWarps * 32, 0, s>>>(
-      mode, n, reinterpret_cast<const double2 *>(nodes), elems, c, V, W, rowptr, adjptr, adj,
-      cptr, contrib, slotcnt, H, M, Him, status);
+  if (W && mode == QD_ASM_FEM)
+    assemble_rows_kernel<K, true><<<int(blocks), RowShape<K>::THREADS, 0, s>>>(
+        mode, n, reinterpret_cast<const double2 *>(nodes), elems, c, V, W, rowptr, adjptr, adj,
+        cptr, contrib, slotcnt, H, M, Him, status);
+  else
+    assemble_rows_kernel<K, false><<<int(blocks), RowShape<K>::THREADS, 0, s>>>(
+        mode, n, reinterpret_cast<const double2 *>(nodes), elems, c, V, W, rowptr, adjptr, adj,
+        cptr, contrib, slotcnt, H, M, Him, status);
   qd::prof_end(qd::PK_ASSEMBLE, s);
   QD_CHECK_LAUNCH();
   return QD_OK;

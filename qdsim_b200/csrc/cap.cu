@@ -23,28 +23,31 @@ template <typename T> struct Vec2;
 template <> struct Vec2<float> { using type = float2; };
 template <> struct Vec2<double> { using type = double2; };
 
-constexpr int kRowsPerBlock = 8;   // one warp per row
-constexpr unsigned kFull = 0xffffffffu;
+constexpr int kLanes = 16;          // lanes per row: two rows per warp
+constexpr int kRowsPerBlock = 16;   // 256 threads
 
-// One warp per row; lane l owns columns l, l + 32, ... (NCH chunks).  The
-// row's CSR entries are loaded 32 at a time, one per lane, and broadcast by
-// shuffles, so every lane's vector loads are coalesced across the warp.
-template <typename T, int NCH>
-__global__ void __launch_bounds__(kRowsPerBlock * 32)
+// kLanes lanes per row; lane l owns columns l, l + 16, ... (C of them, so a
+// 48-column block keeps every lane busy).  The row's CSR entries are loaded 16
+// at a time, one per lane, and broadcast by shuffles within the half-warp,
+// so each half-warp's vector loads are 16 consecutive complex values.
+template <typename T, int C>
+__global__ void __launch_bounds__(kRowsPerBlock * kLanes, 4)
 cap_spmm_kernel(int32_t n, int b, int ldx, int ldy, const int32_t *__restrict__ rowptr,
                 const int32_t *__restrict__ col, const T *__restrict__ H,
                 const T *__restrict__ G, const T *__restrict__ M,
                 const typename Vec2<T>::type *__restrict__ X, typename Vec2<T>::type *AX,
                 typename Vec2<T>::type *MX) {
   using V = typename Vec2<T>::type;
-  const int row = blockIdx.x * kRowsPerBlock + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;   // warp-uniform
-  T ar[NCH], ai[NCH], mr[NCH], mi[NCH];
+  const int row = blockIdx.x * kRowsPerBlock + (threadIdx.x / kLanes);
+  const int lane = threadIdx.x % kLanes;
+  // the two rows of a warp are independent: shuffles stay inside each half
+  const unsigned mask = 0xffffu << (threadIdx.x & 16);
+  const bool live = row < n;
+  T ar[C], ai[C], mr[C], mi[C];
 #pragma unroll
-  for (int c = 0; c < NCH; ++c) ar[c] = ai[c] = mr[c] = mi[c] = T(0);
-  const int p0 = rowptr[row], p1 = rowptr[row + 1];
-  for (int base = p0; base < p1; base += 32) {
+  for (int c = 0; c < C; ++c) ar[c] = ai[c] = mr[c] = mi[c] = T(0);
+  const int p0 = live ? rowptr[row] : 0, p1 = live ? rowptr[row + 1] : 0;
+  for (int base = p0; base < p1; base += kLanes) {
     const int p = base + lane;
     int cj = 0;
     T h = T(0), g = T(0), m = T(0);
@@ -54,16 +57,16 @@ cap_spmm_kernel(int32_t n, int b, int ldx, int ldy, const int32_t *__restrict__ 
       g = G ? G[p] : T(0);
       m = M[p];
     }
-    const int cnt = min(32, p1 - base);
+    const int cnt = min(kLanes, p1 - base);
     for (int q = 0; q < cnt; ++q) {
-      const int j = __shfl_sync(kFull, cj, q);
-      const T hq = __shfl_sync(kFull, h, q);
-      const T gq = __shfl_sync(kFull, g, q);
-      const T mq = __shfl_sync(kFull, m, q);
+      const int j = __shfl_sync(mask, cj, q, kLanes);
+      const T hq = __shfl_sync(mask, h, q, kLanes);
+      const T gq = __shfl_sync(mask, g, q, kLanes);
+      const T mq = __shfl_sync(mask, m, q, kLanes);
       const V *xr = X + size_t(j) * ldx;
 #pragma unroll
-      for (int c = 0; c < NCH; ++c) {
-        const int cc = c * 32 + lane;
+      for (int c = 0; c < C; ++c) {
+        const int cc = c * kLanes + lane;
         if (cc < b) {
           const V x = xr[cc];
           // (h + i g)(xr + i xi) = (h xr - g xi) + i (h xi + g xr)
@@ -75,9 +78,10 @@ cap_spmm_kernel(int32_t n, int b, int ldx, int ldy, const int32_t *__restrict__ 
       }
     }
   }
+  if (!live) return;
 #pragma unroll
-  for (int c = 0; c < NCH; ++c) {
-    const int cc = c * 32 + lane;
+  for (int c = 0; c < C; ++c) {
+    const int cc = c * kLanes + lane;
     if (cc < b) {
       V a, mm;
       a.x = ar[c];
@@ -100,12 +104,13 @@ int launch(int32_t n, int b, int ldx, int ldy, const int32_t *rowptr, const int3
           *m = static_cast<const T *>(M);
   const V *x = static_cast<const V *>(X);
   V *ax = static_cast<V *>(AX), *mx = static_cast<V *>(MX);
-  if (b <= 32)
-    cap_spmm_kernel<T, 1><<<blocks, kRowsPerBlock * 32, 0, s>>>(n, b, ldx, ldy, rowptr, col, h,
-                                                                 g, m, x, ax, mx);
-  else
-    cap_spmm_kernel<T, 2><<<blocks, kRowsPerBlock * 32, 0, s>>>(n, b, ldx, ldy, rowptr, col, h,
-                                                                 g, m, x, ax, mx);
+  const dim3 grid(blocks), block(kRowsPerBlock * kLanes);
+  switch ((b + kLanes - 1) / kLanes) {
+    case 1: cap_spmm_kernel<T, 1><<<grid, block, 0, s>>>(n, b, ldx, ldy, rowptr, col, h, g, m, x, ax, mx); break;
+    case 2: cap_spmm_kernel<T, 2><<<grid, block, 0, s>>>(n, b, ldx, ldy, rowptr, col, h, g, m, x, ax, mx); break;
+    case 3: cap_spmm_kernel<T, 3><<<grid, block, 0, s>>>(n, b, ldx, ldy, rowptr, col, h, g, m, x, ax, mx); break;
+    default: cap_spmm_kernel<T, 4><<<grid, block, 0, s>>>(n, b, ldx, ldy, rowptr, col, h, g, m, x, ax, mx); break;
+  }
   QD_CHECK_LAUNCH();
   return QD_OK;
 }

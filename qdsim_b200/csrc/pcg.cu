@@ -42,60 +42,83 @@ struct Cfg {
 // partials: part[(kind * nrhs + j) * blocks + block]; kinds 0 r.z, 1 r.r, 2 p.Ap
 // step scalars per column: sc[j * 5 + {0 rz, 1 rr0, 2 alpha, 3 beta, 4 rr}]
 
-// Column sums of this block's per-thread values into part[kind] (threads
-// t, t + nrhs, ... in order).
-__device__ inline void block_col_reduce(double v, double *red, const Cfg &c, double *part_k) {
-  red[threadIdx.x] = v;
+// Column sums of this block's per-thread values v0 (and v1 when NV == 2) into
+// part[k0] (and part[k0 + 1]): threads t, t + nrhs, ... in order.
+template <int NV>
+__device__ inline void block_col_reduce(double v0, double v1, double *red, const Cfg &c,
+                                        double *part_k0) {
+  red[threadIdx.x] = v0;
+  if (NV == 2) red[blockDim.x + threadIdx.x] = v1;
   __syncthreads();
   if (threadIdx.x < c.nrhs) {
-    double s = 0.0;
-    for (int t = threadIdx.x; t < blockDim.x; t += c.nrhs) s += red[t];
-    part_k[size_t(threadIdx.x) * c.blocks + blockIdx.x] = s;
+    double s0 = 0.0, s1 = 0.0;
+    for (int t = threadIdx.x; t < blockDim.x; t += c.nrhs) {
+      s0 += red[t];
+      if (NV == 2) s1 += red[blockDim.x + t];
+    }
+    part_k0[size_t(threadIdx.x) * c.blocks + blockIdx.x] = s0;
+    if (NV == 2) part_k0[size_t(c.nrhs + threadIdx.x) * c.blocks + blockIdx.x] = s1;
   }
   __syncthreads();
 }
 
 // True in every thread of the block that finished last; that block then sees
-// every other block's partials.
+// every other block's partials.  The barrier orders this block's partial
+// writes before thread 0's fence, which makes them visible device-wide
+// before the counter moves.
 __device__ inline bool last_block(unsigned *counter) {
   __shared__ unsigned s_last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
   __syncthreads();
   if (s_last) __threadfence();
   return s_last;
 }
 
-// Sum over blocks of part[kind][j] for j = threadIdx.x / L, L = blockDim / nrhs
-// lanes per column: lane l takes blocks l, l + L, ..., then the lane sums are
-// added in lane order.  Valid in the threads with l == 0.
-__device__ inline double grid_col_sum(const double *part_k, const Cfg &c, double *red) {
-  const int L = blockDim.x / c.nrhs;
-  const int j = threadIdx.x / L, l = threadIdx.x % L;
-  double a = 0.0;
-  const double *src = part_k + size_t(j) * c.blocks;
-  for (int b = l; b < c.blocks; b += L) a += __ldcg(src + b);
-  red[threadIdx.x] = a;
-  __syncthreads();
-  double s = 0.0;
-  if (l == 0)
-    for (int q = 0; q < L; ++q) s += red[threadIdx.x + q];
-  __syncthreads();
-  return s;
-}
-
 // Step scalars in the last block.  mode 0: initial (rz, rr0, done); mode 1:
 // alpha = rz / pAp (0 for a converged column); mode 2: beta, rr, done.
+// Column j = threadIdx.x / L is summed by L = blockDim / nrhs lanes: lane l
+// takes blocks l, l + L, ... in order (kU loads of each kind in flight), then
+// the lane sums are added in lane order.
+constexpr int kU = 4;
+
 __device__ void finish_scalars(int mode, const Cfg &c, const double *part, double *sc, int *done,
                                unsigned *counter, double tol, double *red) {
   __shared__ int s_all;
   if (threadIdx.x == 0) s_all = 1;
-  const double sa = grid_col_sum(part + size_t(mode == 1 ? 2 : 0) * c.nrhs * c.blocks, c, red);
-  const double sb = mode == 1 ? 0.0 : grid_col_sum(part + size_t(c.nrhs) * c.blocks, c, red);
   const int L = blockDim.x / c.nrhs;
-  if (threadIdx.x % L == 0) {
-    double *s = sc + size_t(threadIdx.x / L) * 5;
+  const int j = threadIdx.x / L, l = threadIdx.x % L;
+  const bool two = mode != 1;
+  const double *pa = part + (size_t(mode == 1 ? 2 : 0) * c.nrhs + j) * c.blocks;
+  const double *pb = part + (size_t(c.nrhs) + j) * c.blocks;
+  double a = 0.0, b = 0.0;
+  for (int b0 = l; b0 < c.blocks; b0 += kU * L) {
+    double va[kU], vb[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int k = b0 + u * L;
+      va[u] = k < c.blocks ? __ldcg(pa + k) : 0.0;
+      vb[u] = (two && k < c.blocks) ? __ldcg(pb + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      a += va[u];
+      b += vb[u];
+    }
+  }
+  red[threadIdx.x] = a;
+  red[blockDim.x + threadIdx.x] = b;
+  __syncthreads();
+  double sa = 0.0, sb = 0.0;
+  if (l == 0)
+    for (int q = 0; q < L; ++q) {
+      sa += red[threadIdx.x + q];
+      sb += red[blockDim.x + threadIdx.x + q];
+    }
+  if (l == 0) {
+    double *s = sc + size_t(j) * 5;
     if (mode == 0) {
       s[0] = sa;
       s[1] = sb;
@@ -150,8 +173,7 @@ pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *
     rz += r * z;
     rr += r * r;
   }
-  block_col_reduce(rz, red, c, part);
-  block_col_reduce(rr, red, c, part + size_t(c.nrhs) * c.blocks);
+  block_col_reduce<2>(rz, rr, red, c, part);
   if (last_block(counter)) finish_scalars(0, c, part, sc, done, counter, tol, red);
 }
 
@@ -180,7 +202,7 @@ pcg_spmv_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *
     AP[idx] = ap;
     pap += pi * ap;
   }
-  block_col_reduce(pap, red, c, part + size_t(2) * c.nrhs * c.blocks);
+  block_col_reduce<1>(pap, 0.0, red, c, part + size_t(2) * c.nrhs * c.blocks);
   if (last_block(counter)) finish_scalars(1, c, part, sc, done, counter, tol, red);
 }
 
@@ -205,8 +227,7 @@ pcg_axpy_kernel(Cfg c, const double *dinv, double *X, double *R, double *Z, cons
     rz += r * z;
     rr += r * r;
   }
-  block_col_reduce(rz, red, c, part);
-  block_col_reduce(rr, red, c, part + size_t(c.nrhs) * c.blocks);
+  block_col_reduce<2>(rz, rr, red, c, part);
   if (last_block(counter)) finish_scalars(2, c, part, sc, done, counter, tol, red);
 }
 
@@ -246,7 +267,7 @@ void carve(qd::Arena &ar, const Cfg &c, PcgLayout &L) {
 int run_pcg(const Cfg &c, const PcgLayout &L, const int32_t *d_rowptr, const int32_t *d_col,
             const double *d_A, const double *d_B, double *d_X, const int32_t *d_fixed,
             double tol, int max_iter, int32_t *h_iters, double *h_relres, cudaStream_t s) {
-  const size_t smem = size_t(c.threads) * sizeof(double);
+  const size_t smem = 2 * size_t(c.threads) * sizeof(double);
   QD_CUDA_TRY(cudaMemsetAsync(L.counter, 0, 4 * sizeof(unsigned), s));
   pcg_init_kernel<<<c.blocks, c.threads, smem, s>>>(c, d_rowptr, d_col, d_A, d_B, d_X, d_fixed,
                                                     L.R, L.Z, L.P[0], L.dinv, L.part, L.sc,
