@@ -472,6 +472,13 @@ def main():
 
     # ---- roofline of the dominant kernel ------------------------------------
     bytes_kind = algorithmic_bytes(hb, counts, args.block)
+    # assembly: nodes (x, y), connectivity, per-element c, nodal V in; H, M out
+    a = hb.arrays
+    n_nodes, n_el = a["nodes"].shape[0], a["c"].shape[0]
+    k_nodes = a["elems"].size // max(n_el, 1)
+    asm_bytes = (n_nodes * 16 + n_el * k_nodes * 4 + n_el * 8 + n_nodes * 8
+                 + 16 * float(np.sum(hb.nnz_per_dot)))
+    bytes_kind["assemble"] = asm_bytes * float(prof_n[KIND_NAMES.index("assemble")])
     dom = int(np.argmax(prof_ms))
     dom_name = KIND_NAMES[dom]
     peaks = {}
