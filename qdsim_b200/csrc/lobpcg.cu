@@ -470,16 +470,42 @@ cudaError_t smem_attr(size_t bytes) {
   return e;
 }
 
-template <int B> struct GramCfg {
+// Gram tasks: one upper-triangle 4x4 block (bi <= bj) of S^T HS or of S^T MS
+// per thread (NT2 = 2 NT tasks), RG row groups.  One matrix per thread keeps
+// the FP64 accumulators at 16 values, so two CTAs fit on an SM.
+template <typename TV, int B> struct GramCfg {
   static constexpr int m = 3 * B;
   static constexpr int NB = m / 4;
   static constexpr int NT = NB * (NB + 1) / 2;            // upper-triangle 4x4 blocks
-  static constexpr int RG = (256 / NT) > 0 ? (256 / NT) : 1;
-  static constexpr int THREADS = ((NT * RG + 31) / 32) * 32;
+  static constexpr int NT2 = 2 * NT;                      // of S^T HS, then of S^T MS
+  static constexpr int TARGET = sizeof(TV) == 8 ? 256 : 384;
+  static constexpr int RG = (TARGET / NT2) > 0 ? (TARGET / NT2) : 1;
+  static constexpr int THREADS = ((NT2 * RG + 31) / 32) * 32;
 };
 
 // The Gram kernel streams the 9 vector blocks X W P HX HW HP MX MW MP of each
 // sub-tile through a 3-stage bulk-copy pipeline.
+// Four consecutive elements of a staged row in shared memory, as one 16-byte
+// (FP32) or two 16-byte (FP64) loads.  Stage tiles start 16-byte aligned, row
+// pitches are B elements (B % 4 == 0) and column groups start at multiples of
+// 4 elements, so every such group is 16-byte aligned.
+template <typename TV> __device__ inline void lds4(const TV *p, TV (&v)[4]);
+template <> __device__ inline void lds4<float>(const float *p, float (&v)[4]) {
+  const float4 a = *reinterpret_cast<const float4 *>(p);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+template <> __device__ inline void lds4<double>(const double *p, double (&v)[4]) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0];
+  const double2 b = reinterpret_cast<const double2 *>(p)[1];
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+
 template <typename TV, int B> using GramPipe = qd::BlockPipe<TV, B, 9, (sizeof(TV) == 8 ? 32 : 64), 3>;
 
 // Each thread owns one upper-triangle 4x4 block (bi <= bj) of both S^T HS and
@@ -488,13 +514,13 @@ template <typename TV, int B> using GramPipe = qd::BlockPipe<TV, B, 9, (sizeof(T
 // are written to both (bi, bj) and (bj, bi), so the per-chunk partial holds
 // the full symmetric matrices.
 template <typename TV, int B>
-__global__ void __launch_bounds__(GramCfg<B>::THREADS)
+__global__ void __launch_bounds__(GramCfg<TV, B>::THREADS, 2)
 gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, const TV *P,
             const TV *HX, const TV *HW, const TV *HP, const TV *MX, const TV *MW, const TV *MP,
             double *partial, int *wait_err) {
-  using C = GramCfg<B>;
+  using C = GramCfg<TV, B>;
   using PP = GramPipe<TV, B>;
-  constexpr int m = C::m, NB = C::NB, NT = C::NT, RG = C::RG;
+  constexpr int m = C::m, NB = C::NB, NT = C::NT, NT2 = C::NT2, RG = C::RG;
   constexpr int BLK = PP::BLK;
   extern __shared__ __align__(128) unsigned char dsm[];
 
@@ -503,8 +529,9 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
   const int tid = threadIdx.x;
   if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
     const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][1]++;
-  const bool worker = tid < NT * RG;
-  const int task = tid % NT, rg = tid / NT;
+  const bool worker = tid < NT2 * RG;
+  const int task2 = tid % NT2, rg = tid / NT2;
+  const int which = task2 / NT, task = task2 % NT;   // which: 0 S^T HS, 1 S^T MS
   // task -> (bi, bj) with bi <= bj
   int bi = 0, rem = task;
   while (rem >= NB - bi) {
@@ -515,13 +542,12 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
   // element offsets of this thread's 4 columns inside a stage (B % 4 == 0,
   // so a group of 4 columns never straddles two blocks)
   const int offS = ((4 * bi) / B) * BLK + (4 * bi) % B;
-  const int offH = (3 + (4 * bj) / B) * BLK + (4 * bj) % B;
-  const int offM = (6 + (4 * bj) / B) * BLK + (4 * bj) % B;
-  double aH[4][4], aM[4][4];
+  const int offR = (3 + 3 * which + (4 * bj) / B) * BLK + (4 * bj) % B;
+  double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) aH[a][b] = aM[a][b] = 0.0;
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
 
   const TV *src[9] = {X, W, P, HX, HW, HP, MX, MW, MP};
   PP pipe;
@@ -532,76 +558,57 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
     if (worker && ok) {
       const int nr = pipe.rows(i);
       const TV *sb = pipe.tile(i, 0);
-      TV tH[4][4], tM[4][4];
+      TV t[4][4];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) tH[a][b] = tM[a][b] = TV(0);
+        for (int b = 0; b < 4; ++b) t[a][b] = TV(0);
       for (int row = rg; row < nr; row += RG) {
-        TV sa[4], hb[4], mb[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          sa[a] = sb[offS + row * B + a];
-          hb[a] = sb[offH + row * B + a];
-          mb[a] = sb[offM + row * B + a];
-        }
+        TV sa[4], rb[4];
+        lds4(sb + offS + row * B, sa);
+        lds4(sb + offR + row * B, rb);
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            tH[a][b] = fma(sa[a], hb[b], tH[a][b]);
-            tM[a][b] = fma(sa[a], mb[b], tM[a][b]);
-          }
+          for (int b = 0; b < 4; ++b) t[a][b] = fma(sa[a], rb[b], t[a][b]);
       }
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          aH[a][b] += double(tH[a][b]);
-          aM[a][b] += double(tM[a][b]);
-        }
+        for (int b = 0; b < 4; ++b) acc[a][b] += double(t[a][b]);
     }
     pipe.release(i, ok);
   }
   if (!pipe.finish(ok, wait_err)) return;
   double *out = partial + size_t(blockIdx.x) * 2 * m * m;
   if (RG > 1) {
-    double *red = reinterpret_cast<double *>(dsm);   // NT * 32 doubles < one stage
+    double *red = reinterpret_cast<double *>(dsm);   // NT2 * 16 doubles < one stage
     for (int g = 1; g < RG; ++g) {
       if (worker && rg == g) {
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            red[task * 32 + a * 4 + b] = aH[a][b];
-            red[task * 32 + 16 + a * 4 + b] = aM[a][b];
-          }
+          for (int b = 0; b < 4; ++b) red[task2 * 16 + a * 4 + b] = acc[a][b];
       }
       __syncthreads();
       if (worker && rg == 0) {
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            aH[a][b] += red[task * 32 + a * 4 + b];
-            aM[a][b] += red[task * 32 + 16 + a * 4 + b];
-          }
+          for (int b = 0; b < 4; ++b) acc[a][b] += red[task2 * 16 + a * 4 + b];
       }
       __syncthreads();
     }
   }
   if (worker && rg == 0) {
+    double *o = out + size_t(which) * m * m;
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
         const int i = 4 * bi + a, j = 4 * bj + b;
-        out[i * m + j] = aH[a][b];
-        out[m * m + i * m + j] = aM[a][b];
-        if (bi != bj) {
-          out[j * m + i] = aH[a][b];
-          out[m * m + j * m + i] = aM[a][b];
-        }
+        o[i * m + j] = acc[a][b];
+        if (bi != bj) o[j * m + i] = acc[a][b];
       }
   }
 }
@@ -1113,18 +1120,33 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
         const int row = e / B, j = e % B;
         ACC x = 0, p = 0;
 #pragma unroll
-        for (int q = 0; q < B; ++q) x = fma(ACC(tx[row * B + q]), sY[q * B + j], x);
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          TV t[4];
+          lds4(tx + row * B + q4, t);
 #pragma unroll
-        for (int q = 0; q < B; ++q) {
-          const ACC v = ACC(tw[row * B + q]) * sY[(B + q) * B + j];
-          x += v;
-          p += v;
+          for (int u = 0; u < 4; ++u) x = fma(ACC(t[u]), sY[(q4 + u) * B + j], x);
         }
 #pragma unroll
-        for (int q = 0; q < B; ++q) {
-          const ACC v = ACC(tp[row * B + q]) * sY[(2 * B + q) * B + j];
-          x += v;
-          p += v;
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          TV t[4];
+          lds4(tw + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const ACC v = ACC(t[u]) * sY[(B + q4 + u) * B + j];
+            x += v;
+            p += v;
+          }
+        }
+#pragma unroll
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          TV t[4];
+          lds4(tp + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const ACC v = ACC(t[u]) * sY[(2 * B + q4 + u) * B + j];
+            x += v;
+            p += v;
+          }
         }
         const size_t o = size_t(r0) * B + e;
         X[o] = TV(x);
@@ -1192,11 +1214,8 @@ ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const T
         for (int b = 0; b < 4; ++b) t[a][b] = TV(0);
       for (int row = rg; row < nr; row += RG) {
         TV x[4], y[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          x[a] = tm[row * B + a];
-          y[a] = tr[row * B + a];
-        }
+        lds4(tm + row * B, x);
+        lds4(tr + row * B, y);
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -1260,16 +1279,28 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
         const size_t o = size_t(r0) * B + e;
         TV dw = 0;
 #pragma unroll
-        for (int q = 0; q < B; ++q) dw = fma(tx[row * B + q], sC[q * B + j], dw);
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          TV t[4];
+          lds4(tx + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) dw = fma(t[u], sC[(q4 + u) * B + j], dw);
+        }
         W[o] = tw[e] - dw;
         if (with_p) {
           TV dp = 0, dhp = 0, dmp = 0;
 #pragma unroll
-          for (int q = 0; q < B; ++q) {
-            const TV c = sC[B * B + q * B + j];
-            dp = fma(tx[row * B + q], c, dp);
-            dhp = fma(thx[row * B + q], c, dhp);
-            dmp = fma(tmx[row * B + q], c, dmp);
+          for (int q4 = 0; q4 < B; q4 += 4) {
+            TV t0[4], t1[4], t2[4];
+            lds4(tx + row * B + q4, t0);
+            lds4(thx + row * B + q4, t1);
+            lds4(tmx + row * B + q4, t2);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const TV c = sC[B * B + (q4 + u) * B + j];
+              dp = fma(t0[u], c, dp);
+              dhp = fma(t1[u], c, dhp);
+              dmp = fma(t2[u], c, dmp);
+            }
           }
           P[o] = tp[e] - dp;
           HP[o] = thp[e] - dhp;
@@ -1479,7 +1510,7 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
                    const int32_t *col, const double *H, const double *M, cudaStream_t s) {
   constexpr int G = B / 4;
   constexpr int PH = sizeof(TV) == 8 ? 1 : 0;
-  using GC = GramCfg<B>;
+  using GC = GramCfg<TV, B>;
   qd::prof_begin(qd::PK_SPMM, s);
   const auto A = MatFor<TV>::make(L, H, M);
   if constexpr (sizeof(TV) == 4) {
