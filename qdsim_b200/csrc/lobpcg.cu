@@ -521,7 +521,7 @@ gram_kernel(const Chunk *chunks, const DotState *st, const TV *X, const TV *W, c
   using C = GramCfg<TV, B>;
   using PP = GramPipe<TV, B>;
   constexpr int m = C::m, NB = C::NB, NT = C::NT, NT2 = C::NT2, RG = C::RG;
-  constexpr int BLK = PP::BLK;
+  constexpr int BLK = PP::BLKP;   // block stride inside a stage
   extern __shared__ __align__(128) unsigned char dsm[];
 
   const Chunk ch = chunks[blockIdx.x];

@@ -25,7 +25,11 @@ constexpr uint64_t kPipeWaitNs = 1000000000ull;   // 1 s bound on every wait
 template <typename TV, int B, int NBLK, int SUB, int STAGES>
 struct BlockPipe {
   static constexpr int BLK = SUB * B;                 // elements of one block per stage
-  static constexpr int STAGE = NBLK * BLK;            // elements per stage
+  // Blocks of a stage are one row (B elements, 16-byte multiple) further apart
+  // than their size, so the same row of different blocks falls on different
+  // shared-memory banks when a warp reads several blocks at once.
+  static constexpr int BLKP = BLK + B;
+  static constexpr int STAGE = NBLK * BLKP;           // elements per stage
   static constexpr size_t BAR_OFF = size_t(STAGES) * STAGE * sizeof(TV);
   static constexpr size_t BYTES = BAR_OFF + 8 * STAGES;
 
@@ -52,8 +56,8 @@ struct BlockPipe {
   }
   __device__ int rows(int i) const { return min(SUB, end - (begin + i * SUB)); }
   __device__ int row0(int i) const { return begin + i * SUB; }
-  __device__ const TV *tile(int i, int a) const { return stage + (i % STAGES) * STAGE + a * BLK; }
-  __device__ TV *tile_rw(int i, int a) { return stage + (i % STAGES) * STAGE + a * BLK; }
+  __device__ const TV *tile(int i, int a) const { return stage + (i % STAGES) * STAGE + a * BLKP; }
+  __device__ TV *tile_rw(int i, int a) { return stage + (i % STAGES) * STAGE + a * BLKP; }
 
   __device__ void issue(int i) {   // thread 0
     const int s = i % STAGES;
@@ -61,7 +65,7 @@ struct BlockPipe {
     tc::mbar_arrive_expect_tx(&full[s], NBLK * bytes);
 #pragma unroll
     for (int a = 0; a < NBLK; ++a)
-      tc::bulk_g2s(stage + s * STAGE + a * BLK, src[a] + size_t(row0(i)) * B, bytes, &full[s]);
+      tc::bulk_g2s(stage + s * STAGE + a * BLKP, src[a] + size_t(row0(i)) * B, bytes, &full[s]);
   }
   __device__ bool wait(int i) {
     return tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, kPipeWaitNs);
