@@ -1109,22 +1109,30 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
   for (int i = tid; i < m * B; i += blockDim.x) sY[i] = ACC(Yg[i]);
   const TV *src[3] = {X, W, P};
   PP pipe;
-  pipe.init(dsm, src, ch.begin, ch.end);
+  pipe.init(dsm, src, ch.begin, ch.end);   // its barrier also publishes sY
+  // Elements step by a multiple of B, so each thread keeps one column j and
+  // holds that column of Y in registers (threads past the multiple idle).
+  const int nthr = (int(blockDim.x) / B) * B;
+  const int j = tid % B;
+  const bool owner = tid < nthr;
+  ACC cy[3 * B];
+#pragma unroll
+  for (int q = 0; q < 3 * B; ++q) cy[q] = sY[q * B + j];
   bool ok = true;
   for (int i = 0; i < pipe.nsub; ++i) {
     ok = pipe.wait(i) && ok;
-    if (ok) {
+    if (ok && owner) {
       const int nr = pipe.rows(i), r0 = pipe.row0(i);
       const TV *tx = pipe.tile(i, 0), *tw = pipe.tile(i, 1), *tp = pipe.tile(i, 2);
-      for (int e = tid; e < nr * B; e += blockDim.x) {
-        const int row = e / B, j = e % B;
+      for (int e = tid; e < nr * B; e += nthr) {
+        const int row = e / B;
         ACC x = 0, p = 0;
 #pragma unroll
         for (int q4 = 0; q4 < B; q4 += 4) {
           TV t[4];
           lds4(tx + row * B + q4, t);
 #pragma unroll
-          for (int u = 0; u < 4; ++u) x = fma(ACC(t[u]), sY[(q4 + u) * B + j], x);
+          for (int u = 0; u < 4; ++u) x = fma(ACC(t[u]), cy[q4 + u], x);
         }
 #pragma unroll
         for (int q4 = 0; q4 < B; q4 += 4) {
@@ -1132,7 +1140,7 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
           lds4(tw + row * B + q4, t);
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const ACC v = ACC(t[u]) * sY[(B + q4 + u) * B + j];
+            const ACC v = ACC(t[u]) * cy[B + q4 + u];
             x += v;
             p += v;
           }
@@ -1143,7 +1151,7 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
           lds4(tp + row * B + q4, t);
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const ACC v = ACC(t[u]) * sY[(2 * B + q4 + u) * B + j];
+            const ACC v = ACC(t[u]) * cy[2 * B + q4 + u];
             x += v;
             p += v;
           }
