@@ -1273,17 +1273,29 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
   for (int e = tid; e < NOUT; e += blockDim.x) sC[e] = TV(csum[size_t(ch.dot) * NOUT + e]);
   const TV *src[7] = {X, HX, MX, W, P, HP, MP};
   PP pipe;
-  pipe.init(dsm, src, ch.begin, ch.end);
+  pipe.init(dsm, src, ch.begin, ch.end);   // its barrier also publishes sC
+  // Elements step by a multiple of B, so each thread keeps one column j and
+  // holds that column of C_W and C_P in registers (threads past the multiple
+  // idle).
+  const int nthr = (int(blockDim.x) / B) * B;
+  const int j = tid % B;
+  const bool owner = tid < nthr;
+  TV cw[B], cp[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    cw[q] = sC[q * B + j];
+    cp[q] = sC[B * B + q * B + j];
+  }
   bool ok = true;
   for (int i = 0; i < pipe.nsub; ++i) {
     ok = pipe.wait(i) && ok;
-    if (ok) {
+    if (ok && owner) {
       const int nr = pipe.rows(i), r0 = pipe.row0(i);
       const TV *tx = pipe.tile(i, 0), *thx = pipe.tile(i, 1), *tmx = pipe.tile(i, 2);
       const TV *tw = pipe.tile(i, 3), *tp = pipe.tile(i, 4), *thp = pipe.tile(i, 5),
                *tmp = pipe.tile(i, 6);
-      for (int e = tid; e < nr * B; e += blockDim.x) {
-        const int row = e / B, j = e % B;
+      for (int e = tid; e < nr * B; e += nthr) {
+        const int row = e / B;
         const size_t o = size_t(r0) * B + e;
         TV dw = 0;
 #pragma unroll
@@ -1291,7 +1303,7 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
           TV t[4];
           lds4(tx + row * B + q4, t);
 #pragma unroll
-          for (int u = 0; u < 4; ++u) dw = fma(t[u], sC[(q4 + u) * B + j], dw);
+          for (int u = 0; u < 4; ++u) dw = fma(t[u], cw[q4 + u], dw);
         }
         W[o] = tw[e] - dw;
         if (with_p) {
@@ -1304,7 +1316,7 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
             lds4(tmx + row * B + q4, t2);
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-              const TV c = sC[B * B + (q4 + u) * B + j];
+              const TV c = cp[q4 + u];
               dp = fma(t0[u], c, dp);
               dhp = fma(t1[u], c, dhp);
               dmp = fma(t2[u], c, dmp);
