@@ -626,20 +626,6 @@ struct RRParams {
   double eig_scale; // floor of |theta| in the relative error estimate (0: none)
 };
 
-__device__ inline double cta_sum(double v, double *s_red) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  __syncthreads();
-  s_red[tid] = v;
-  __syncthreads();
-  for (int w = nt / 2; w > 0; w >>= 1) {
-    if (tid < w) s_red[tid] += s_red[tid + w];
-    __syncthreads();
-  }
-  const double r = s_red[0];
-  __syncthreads();
-  return r;
-}
-
 // Cyclic Jacobi eigensolver for a symmetric n x n matrix A (leading dimension
 // ld, shared memory) with round-robin pairing; V (ld) receives the
 // eigenvectors as columns, A's diagonal the eigenvalues.  A pair is rotated
