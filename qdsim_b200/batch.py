@@ -154,6 +154,58 @@ class DeviceBatch:
             raise N.QDError(N.QD_ERR_DEGENERATE, f"qd_assemble (flag {flag})")
 
 
+class SweepPipeline:
+    """Repeated assemble-and-solve of one batch shape with the host <-> device
+    copies overlapped with the solves.
+
+    Two device batches alternate.  While step s assembles and solves on the
+    current stream, step s+1's inputs are copied up into the other batch and
+    step s-1's eigenvalues and eigenvectors are copied down, both on a copy
+    stream; every step still moves all of its inputs and results.  The solve
+    call returns only when its step is done, so the other batch is free when
+    its next upload is issued.
+    """
+
+    def __init__(self, host: HostBatch, device="cuda", shift_ev=None):
+        self.device = torch.device(device)
+        self.batches = [DeviceBatch(host, self.device), DeviceBatch(host, self.device)]
+        if shift_ev is not None:
+            for b in self.batches:
+                b.set_shift(shift_ev)
+        self.copy = torch.cuda.Stream(device=self.device)
+
+    def run(self, steps, k, inputs, out_E, out_X, **solve_kw):
+        """``inputs(s)``: dict of pinned host arrays of step s (``HostBatch.pin``);
+        ``out_E(s)``, ``out_X(s)``: pinned host tensors receiving step s's E
+        ([n_dots, k]) and X ([n_rows, k]).  Returns the last step's solver info."""
+        comp = torch.cuda.current_stream(self.device)
+        ready = [torch.cuda.Event(), torch.cuda.Event()]
+        with torch.cuda.stream(self.copy):
+            self.batches[0].upload(inputs(0), non_blocking=True)
+            ready[0].record(self.copy)
+        info = None
+        for s in range(steps):
+            i = s % 2
+            if s + 1 < steps:
+                with torch.cuda.stream(self.copy):
+                    self.batches[1 - i].upload(inputs(s + 1), non_blocking=True)
+                    ready[1 - i].record(self.copy)
+            comp.wait_event(ready[i])
+            db = self.batches[i]
+            db.assemble()
+            E, X, _, _, info, _ = db.solve(k, **solve_kw)
+            done = torch.cuda.Event()
+            done.record(comp)
+            self.copy.wait_event(done)
+            with torch.cuda.stream(self.copy):
+                out_E(s).copy_(E, non_blocking=True)
+                out_X(s).copy_(X, non_blocking=True)
+            E.record_stream(self.copy)
+            X.record_stream(self.copy)
+        comp.wait_stream(self.copy)
+        return info
+
+
 def solve_dots(dots, k, device="cuda", **kw) -> EigResult:
     """Assemble and solve a list of ``workloads.Dot`` on the GPU."""
     hb = HostBatch(dots)

@@ -102,3 +102,27 @@ def test_preconditioned_sweep_dots(cuda, precision):
         E0 = O.eig_lowest(a.H, a.M, 8, O.sigma_below(V))[0]
         rel = np.abs(res.E[j] - E0) / np.abs(E0)
         assert rel.max() <= 1e-9, (j, rel, res.info)
+
+
+def test_sweep_pipeline_steps_match_batch(cuda):
+    """SweepPipeline (two alternating device batches, copies on a side stream):
+    every step's host E and X equal a plain batched solve of the same dots."""
+    import torch
+    from qdsim_b200 import batch as Bt, workloads as W
+    dots = [W.sweep_dot(i, nx=nx) for i, nx in ((0, 24), (1, 32), (2, 28))]
+    hb = Bt.HostBatch(dots)
+    kw = dict(b=12, precision="mixed", tol=1e-9, max_iter=3000)
+    ref = Bt.DeviceBatch(hb, cuda)
+    ref.upload(non_blocking=False)
+    ref.assemble()
+    E_ref, X_ref = (t.cpu().numpy() for t in ref.solve(8, **kw)[:2])
+    pinned = hb.pin()
+    steps = 3
+    outE = [torch.zeros((3, 8), dtype=torch.float64).pin_memory() for _ in range(steps)]
+    outX = [torch.zeros((hb.n, 8), dtype=torch.float64).pin_memory() for _ in range(steps)]
+    pipe = Bt.SweepPipeline(hb, cuda)
+    pipe.run(steps, 8, lambda s: pinned, lambda s: outE[s], lambda s: outX[s], **kw)
+    torch.cuda.synchronize()
+    for s in range(steps):
+        assert np.array_equal(outE[s].numpy(), E_ref), s
+        assert np.array_equal(outX[s].numpy(), X_ref), s
