@@ -76,3 +76,24 @@ def test_incomplete_window_is_reported():
                         precision="fp64", tol=1e-9, max_iter=300)
     assert not res.info["complete"]
     assert res.info["kth_distance"] > res.info["unconverged_bound"]
+
+
+def test_zero_cap_reduces_to_hermitian_levels():
+    """W -> 0: the complex-symmetric solve returns the Hermitian eigenvalues
+    (the oracle's eigsh) with zero imaginary parts."""
+    from qdsim_b200.cap import solve_nearest
+    from qdsim_b200 import workloads as W
+    from qdsim_b200.eigen import DSTPreconditioner
+    from qdsim_b200.mesh import StructuredMesh
+    d = W.c2_dot(0, nx=24, ny=12)
+    om = O.structured_mesh(2, 24, 12, 200.0, 100.0)
+    a = O.assemble(om, d.c, d.V)
+    spec = DSTPreconditioner.spec_for(StructuredMesh(2, 24, 12, 200.0, 100.0), d.c, d.V, 0.02)
+    Eh, _ = O.eig_lowest(a.H, a.M, 32, O.sigma_below(d.V))
+    res = solve_nearest(_HostPencil(a.H.astype(np.complex128), a.M, spec), k=8, sigma=-0.05,
+                        nev=32, b=40, precision="fp64", tol=1e-9, max_iter=300)
+    assert res.info["complete"], res.info
+    assert np.abs(res.E.imag).max() <= 1e-12 * np.abs(res.E).max()
+    near = Eh[np.argsort(np.abs(Eh + 0.05), kind="stable")[:8]]
+    err = np.abs(np.sort(res.E.real) - np.sort(near)) / np.abs(np.sort(near))
+    assert err.max() <= 1e-9, err

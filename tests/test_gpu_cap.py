@@ -84,3 +84,27 @@ def test_cap_nearest20_matches_oracle(cuda, precision):
     r = np.linalg.norm(Ac @ X - (a.M @ X) * res.E, axis=0) / (
         np.abs(res.E) * np.linalg.norm(a.M @ X, axis=0))
     assert r.max() < 1e-8, r.max()
+
+
+@pytest.mark.parametrize("w_scale", [0.0, 1e-5])
+def test_cap_solver_tends_to_hermitian_levels(cuda, w_scale):
+    """As W -> 0 the open-system eigenvalues tend to the Hermitian ones: at
+    W = 0 they coincide (imaginary parts zero); for a CAP scaled by 1e-5 the
+    real parts move by second order only and -Im E stays below the largest W."""
+    from qdsim_b200 import cap as CP
+    d = _c2(100, 50)
+    om = O.structured_mesh(2, 100, 50, 200.0, 100.0)
+    a = O.assemble(om, d.c, d.V)
+    Eh, _ = O.eig_lowest(a.H, a.M, 40, O.sigma_below(d.V))
+    W = d.W * w_scale
+    res = CP.CAPSolver(d.mesh, d.c, d.V, W, device=cuda).solve(
+        k=20, sigma=-0.05, nev=40, b=48, precision="fp64", tol=1e-9)
+    assert res.info["complete"], res.info
+    near = np.sort(Eh[np.argsort(np.abs(Eh + 0.05), kind="stable")[:20]])
+    got = np.sort(res.E.real)
+    if w_scale == 0.0:
+        assert np.abs(res.E.imag).max() <= 1e-12 * np.abs(res.E).max()
+        assert (np.abs(got - near) / np.abs(near)).max() <= 1e-9
+    else:
+        assert (-res.E.imag).max() <= W.max() and (-res.E.imag).min() >= -1e-3 * W.max()
+        assert (np.abs(got - near) / np.abs(near)).max() <= 1e-6
