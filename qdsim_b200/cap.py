@@ -14,9 +14,10 @@ smallest real part, then the ``k`` of them nearest the shift ``sigma``.
  - Products AX, MX from ``qd_cap_spmm`` (one CSR pass for H, Himag, M).
  - Preconditioner: the tensor-core DST preconditioner of the real kinetic
    operator, applied to the real and imaginary parts as separate columns.
- - Rayleigh-Ritz with a Hermitian M-orthonormal basis of [X P W] (SVQB on the
-   scaled Gram matrix) and the projected non-Hermitian eigenproblem solved in
-   FP64 on the host (3b x 3b); the b Ritz pairs of smallest real part are kept.
+ - Rayleigh-Ritz with a Hermitian M-orthonormal basis of [X P W] (Cholesky of
+   the diagonally scaled Gram matrix while it is well conditioned, else SVQB)
+   and the projected non-Hermitian eigenproblem solved in FP64 on the host
+   (3b x 3b, LAPACK); the b Ritz pairs of smallest real part are kept.
  - Mixed form: FP32 vectors and products until the relative residuals reach
    ``tol32`` (or stop improving), then FP64 vectors warm-started from them.
    Plain form: FP64 throughout.
@@ -34,6 +35,7 @@ from dataclasses import dataclass
 
 import numpy as np
 import torch
+from scipy.linalg import solve_triangular
 from threadpoolctl import threadpool_limits
 
 from . import _native as N
@@ -115,6 +117,23 @@ class CAPProblem:
                                        N.ptr(out), N.ptr(self._pws), self._pws.numel(),
                                        stream_ptr()), "qd_dst_precond_apply")
         return out
+
+
+def _orthonormaliser(GM, drop):
+    """B with B^H GM B = I: Cholesky of the diagonally scaled Gram matrix when
+    its smallest pivot shows the basis is well conditioned (condition number
+    below ~1e6), else SVQB, which also drops dependent directions."""
+    d = np.sqrt(np.maximum(GM.diagonal().real, 0.0))
+    if np.all(d > 0.0):
+        Gs = GM / d[:, None] / d[None, :]
+        try:
+            L = np.linalg.cholesky(0.5 * (Gs + Gs.conj().T))
+        except np.linalg.LinAlgError:
+            L = None
+        if L is not None and np.min(np.abs(L.diagonal())) ** 2 > 1e-6:
+            Linv = solve_triangular(L, np.eye(L.shape[0]), lower=True)
+            return Linv.conj().T / d[:, None]
+    return _svqb(GM, drop)
 
 
 def _svqb(GM, drop):
@@ -213,13 +232,13 @@ def _rr(blk: _Block, b, used, npc, drop):
 
 
 def _rr_small(GM, GA, b, drop, like):
-    Bm = _svqb(0.5 * (GM + GM.conj().T), drop)
+    Bm = _orthonormaliser(0.5 * (GM + GM.conj().T), drop)
     C = Bm.conj().T @ GA @ Bm
     w, V = np.linalg.eig(C)
     order = np.argsort(w.real, kind="stable")[:b]
     Y = Bm @ V[:, order]
     # Hermitian M-normalise the Ritz vectors (x^H M x = 1)
-    nrm = np.sqrt(np.maximum(np.einsum("ij,ik,kj->j", Y.conj(), GM, Y).real, 1e-300))
+    nrm = np.sqrt(np.maximum(np.sum(Y.conj() * (GM @ Y), axis=0).real, 1e-300))
     Y = Y / nrm[None, :]
     return torch.from_numpy(Y).to(like.device, like.dtype), w[order]
 
