@@ -256,7 +256,10 @@ int qd_sc_mix(int32_t nb, int64_t n_nodes, int anderson, int nhist, const double
  * hands to spsolve at :240).  Replaces PoissonSolver::solve's SimplicialLDLT
  * (backend/src/poisson.cpp:320-334) and fusedPoissonSolver
  * (backend/src/fused_gpu_kernels.cu:159-206).
- *   tol          relative residual ||b - A x|| / ||b|| per column
+ *   tol          relative residual ||b - A x|| / ||b - A x_D|| per column over
+ *                the free rows, x_D = the initial X with its free entries
+ *                zeroed (the Dirichlet values alone): a warm start X lowers
+ *                the work, not the target; h_relres reports the same ratio
  *   h_iters/h_relres  host outputs: iterations used, final max relative residual
  * ------------------------------------------------------------------------- */
 int qd_pcg_workspace_size(int32_t n, int nrhs, size_t *bytes);

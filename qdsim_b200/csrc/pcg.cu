@@ -117,15 +117,31 @@ __device__ void finish_scalars(int mode, const Cfg &c, const double *part, doubl
       sa += red[threadIdx.x + q];
       sb += red[blockDim.x + threadIdx.x + q];
     }
+  // mode 0: the reference residual ||b - A x_D||^2 (kind 2), x_D = the
+  // initial x with its free entries zeroed (the Dirichlet values alone)
+  double sref = 0.0;
+  if (mode == 0) {
+    __syncthreads();
+    const double *pc = part + (size_t(2) * c.nrhs + j) * c.blocks;
+    double cz = 0.0;
+    for (int k = l; k < c.blocks; k += L) cz += __ldcg(pc + k);
+    red[threadIdx.x] = cz;
+    __syncthreads();
+    if (l == 0)
+      for (int q = 0; q < L; ++q) sref += red[threadIdx.x + q];
+  }
   if (l == 0) {
     double *s = sc + size_t(j) * 5;
     if (mode == 0) {
+      // relative to the zero-guess residual, so that a warm start does not
+      // tighten the target (the initial residual when that one is zero)
+      const double ref = sref > 0.0 ? sref : sb;
       s[0] = sa;
-      s[1] = sb;
+      s[1] = ref;
       s[2] = 0.0;
       s[3] = 0.0;
       s[4] = sb;
-      if (sb > 0.0) atomicAnd(&s_all, 0);
+      if (!(sb <= tol * tol * ref)) atomicAnd(&s_all, 0);
     } else if (mode == 1) {
       s[2] = (sa > 0.0 && s[4] > tol * tol * s[1]) ? s[0] / sa : 0.0;
     } else {
@@ -142,7 +158,8 @@ __device__ void finish_scalars(int mode, const Cfg &c, const double *part, doubl
   }
 }
 
-// r = b - A x (free rows), z = D^-1 r, p_prev = 0; partials r.z and r.r
+// r = b - A x (free rows), z = D^-1 r, p_prev = 0; partials r.z, r.r and
+// |b - A x_D|^2 (x_D: x with its free entries zeroed)
 __global__ void __launch_bounds__(kThreads, 2)
 pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *A,
                 const double *Bv, const double *X, const int32_t *fixed, double *R, double *Z,
@@ -151,18 +168,21 @@ pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *
   extern __shared__ double red[];
   const int j = threadIdx.x % c.nrhs, rpb = blockDim.x / c.nrhs;
   const int step = gridDim.x * rpb;
-  double rz = 0.0, rr = 0.0;
+  double rz = 0.0, rr = 0.0, rr0 = 0.0;
   for (int row = blockIdx.x * rpb + threadIdx.x / c.nrhs; row < c.n; row += step) {
     const size_t idx = size_t(row) * c.nrhs + j;
-    double r = 0.0, di = 0.0;
+    double r = 0.0, r0 = 0.0, di = 0.0;
     if (!fixed || !fixed[row]) {
-      double ax = 0.0, diag = 0.0;
+      double ax = 0.0, axd = 0.0, diag = 0.0;
       for (int p = rowptr[row]; p < rowptr[row + 1]; ++p) {
         const int cj = col[p];
-        ax = fma(A[p], X[size_t(cj) * c.nrhs + j], ax);
-        if (cj == row) diag = A[p];
+        const double a = A[p], xv = X[size_t(cj) * c.nrhs + j];
+        ax = fma(a, xv, ax);
+        if (fixed && fixed[cj]) axd = fma(a, xv, axd);
+        if (cj == row) diag = a;
       }
       r = Bv[idx] - ax;
+      r0 = Bv[idx] - axd;
       di = diag != 0.0 ? 1.0 / diag : 0.0;
     }
     if (j == 0) dinv[row] = di;
@@ -172,8 +192,10 @@ pcg_init_kernel(Cfg c, const int32_t *rowptr, const int32_t *col, const double *
     P[idx] = 0.0;
     rz += r * z;
     rr += r * r;
+    rr0 += r0 * r0;
   }
   block_col_reduce<2>(rz, rr, red, c, part);
+  block_col_reduce<1>(rr0, 0.0, red, c, part + size_t(2) * c.nrhs * c.blocks);
   if (last_block(counter)) finish_scalars(0, c, part, sc, done, counter, tol, red);
 }
 
