@@ -12,7 +12,7 @@ import torch
 
 from . import _native as N
 from .eigen import DSTPreconditioner, EigResult, Workspace, lobpcg_packed
-from .fem import FEMProblem, build_pattern, dof_map_for, stream_ptr
+from .fem import build_pattern, dof_map_for, stream_ptr
 
 _SHAPE_CACHE: dict = {}
 
