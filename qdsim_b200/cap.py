@@ -261,7 +261,7 @@ def solve_nearest(prob, k: int = 20, sigma: float = -0.05, nev: int = 40, b: int
     it32 = 0
     if precision == "mixed":
         _, X, _, _, res32, it32 = lobpcg_cap(prob, b, nev, tol32, max_iter, dtype=torch.complex64,
-                                             seed=seed, eig_scale=eig_scale, stall=20)
+                                             seed=seed, eig_scale=eig_scale, stall=8)
         X0 = X.to(torch.complex128)
         info["fp32_residual"] = float(res32[:nev].max())
     elif precision != "fp64":
