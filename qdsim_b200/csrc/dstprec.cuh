@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 #include "common.h"
 #include "tc.cuh"
 
@@ -191,16 +192,40 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   int issued = 0;   // slabs whose copy and MMAs thread 0 has issued
   bool fail = false;
   // A slab: this thread's n, k chunks c = cgrp + 2j, 8 consecutive k each;
-  // slab s+1 is loaded into registers while slab s is multiplied
-  float v[4][8];
+  // slab s+1 is loaded into registers while slab s is multiplied.
+  // Row-major BF16 input (unit stride along n): a thread takes the adjacent
+  // columns pn, pn + 1 and chunks pg, pg + 4 instead, and loads both columns
+  // of a k as one 4-byte pair, so a warp's load covers a full 128-byte line.
+  constexpr bool kPair = !IN_G && std::is_same<TI, __nv_bfloat16>::value;
+  const int pn = (tid & 63) * 2, pg = tid >> 6;
+  const bool pvalid = t.n0 + pn < ncols;   // ncols = other * B is even
+  const TI *pin = in + base + size_t(t.n0 + pn);
+  float v[4][8];   // pair mode: v[2 jj + q] = chunk pg + 4 jj, column pn + q
   auto load_a = [&](int s) {
+    if constexpr (kPair) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int kc = s * kTcK + (cgrp + 2 * j) * 8;
+      for (int jj = 0; jj < 2; ++jj) {
+        const int kc = s * kTcK + (pg + 4 * jj) * 8;
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const int k = kc + e;
-        v[j][e] = (nvalid && k < dim) ? to_f32(in[in_base + size_t(k) * in_kstride]) : 0.f;
+        for (int e = 0; e < 8; ++e) {
+          const int k = kc + e;
+          float2 f = make_float2(0.f, 0.f);
+          if (pvalid && k < dim)
+            f = __bfloat1622float2(
+                *reinterpret_cast<const __nv_bfloat162 *>(pin + size_t(k) * ncols));
+          v[2 * jj][e] = f.x;
+          v[2 * jj + 1][e] = f.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int kc = s * kTcK + (cgrp + 2 * j) * 8;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int k = kc + e;
+          v[j][e] = (nvalid && k < dim) ? to_f32(in[in_base + size_t(k) * in_kstride]) : 0.f;
+        }
       }
     }
   };
@@ -217,7 +242,9 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
     uint8_t *a_st = sm + lay.a_off[0] + st * kTcABytes;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int c = cgrp + 2 * j;
+      // (chunk, column) of v[j]: as loaded above
+      const int c = kPair ? pg + 4 * (j >> 1) : cgrp + 2 * j;
+      const int nl = kPair ? pn + (j & 1) : n_loc;
       uint4 pk;
       uint32_t *w = reinterpret_cast<uint32_t *>(&pk);
 #pragma unroll
@@ -225,8 +252,8 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
         const __nv_bfloat162 h = __floats2bfloat162_rn(v[j][2 * e], v[j][2 * e + 1]);
         w[e] = *reinterpret_cast<const uint32_t *>(&h);
       }
-      *reinterpret_cast<uint4 *>(a_st + c * (kTcABytes / 8) + (n_loc >> 3) * 128 +
-                                 (n_loc & 7) * 16) = pk;
+      *reinterpret_cast<uint4 *>(a_st + c * (kTcABytes / 8) + (nl >> 3) * 128 + (nl & 7) * 16) =
+          pk;
     }
     if (s + 1 < KS) load_a(s + 1);
     tc::fence_proxy_async_smem();
