@@ -199,8 +199,9 @@ int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_r
                     const qd_lobpcg_opts *opts, void *stream);
 
 /* Apply the DST preconditioner W = T R to a batch of b-column blocks
- * (b >= 4; row-major, float if vec_fp32 else double; in-place allowed).  Same
- * descriptors as qd_lobpcg_solve; exposed for testing and reuse. */
+ * (b >= 4 and even; row-major, float if vec_fp32 else double, d_in and d_out
+ * 16-byte aligned; in-place allowed).  Same descriptors as qd_lobpcg_solve;
+ * exposed for testing and reuse. */
 int qd_dst_precond_workspace_size(int32_t n_dots, const int32_t *h_row_off, int b,
                                   const qd_dst_prec *h_prec, size_t *bytes);
 

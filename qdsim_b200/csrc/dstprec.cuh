@@ -39,7 +39,6 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
-#include <type_traits>
 #include "common.h"
 #include "tc.cuh"
 
@@ -122,6 +121,18 @@ __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) {
   return __float2bfloat16_rn(v);
 }
 
+// Two adjacent elements (8-byte / 4-byte / 16-byte aligned pair) as floats.
+__device__ __forceinline__ float2 ld_pair(const __nv_bfloat16 *p) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
+}
+__device__ __forceinline__ float2 ld_pair(const float *p) {
+  return *reinterpret_cast<const float2 *>(p);
+}
+__device__ __forceinline__ float2 ld_pair(const double *p) {
+  const double2 d = *reinterpret_cast<const double2 *>(p);
+  return make_float2(float(d.x), float(d.y));
+}
+
 // out(r, n) = sum_k S[r][k] in(k, n)  [/ (lambda_r(r) + lambda_n(n / B) + shift)]
 template <typename TI, typename TO, bool YPASS, bool IN_G, bool OUT_G, bool SCALE>
 __global__ void __launch_bounds__(kTcThreads)
@@ -178,11 +189,6 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   const uint32_t tmem = *tslot;
 
   // ---- main loop over K slabs ---------------------------------------------
-  const int n_loc = tid & (kTcN - 1);
-  const int cgrp = tid >> 7;                  // 0 / 1: chunks cgrp, cgrp+2, ...
-  const int n = t.n0 + n_loc;
-  const bool nvalid = n < ncols;
-  const size_t in_base = IN_G ? base + size_t(n / B) * dim * B + (n % B) : base + n;
   const size_t in_kstride = IN_G ? size_t(B) : size_t(ncols);
   const uint32_t sA0 = tc::smem_u32(sm + lay.a_off[0]);
   const uint32_t sB0 = tc::smem_u32(sm + lay.b_off[0]);
@@ -191,41 +197,28 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   const uint32_t bstage = lay.b_off[1] - lay.b_off[0];
   int issued = 0;   // slabs whose copy and MMAs thread 0 has issued
   bool fail = false;
-  // A slab: this thread's n, k chunks c = cgrp + 2j, 8 consecutive k each;
-  // slab s+1 is loaded into registers while slab s is multiplied.
-  // Row-major BF16 input (unit stride along n): a thread takes the adjacent
-  // columns pn, pn + 1 and chunks pg, pg + 4 instead, and loads both columns
-  // of a k as one 4-byte pair, so a warp's load covers a full 128-byte line.
-  constexpr bool kPair = !IN_G && std::is_same<TI, __nv_bfloat16>::value;
+  // A slab: the thread's adjacent columns pn, pn + 1 and K chunks pg, pg + 4
+  // (8 consecutive k each), both columns of a k loaded with one access (B is
+  // even and n0 a multiple of 128, so an even n and n + 1 are adjacent in both
+  // layouts and never straddle a group of B).  For row-major input a warp's
+  // load then covers a full 128-byte line.  Slab s+1 is loaded into registers
+  // while slab s is multiplied.
   const int pn = (tid & 63) * 2, pg = tid >> 6;
-  const bool pvalid = t.n0 + pn < ncols;   // ncols = other * B is even
-  const TI *pin = in + base + size_t(t.n0 + pn);
-  float v[4][8];   // pair mode: v[2 jj + q] = chunk pg + 4 jj, column pn + q
+  const int np = t.n0 + pn;
+  const bool pvalid = np < ncols;   // ncols = other * B is even
+  const TI *pin = in + (IN_G ? base + size_t(np / B) * dim * B + (np % B) : base + np);
+  float v[4][8];   // v[2 jj + q]: chunk pg + 4 jj, column pn + q
   auto load_a = [&](int s) {
-    if constexpr (kPair) {
 #pragma unroll
-      for (int jj = 0; jj < 2; ++jj) {
-        const int kc = s * kTcK + (pg + 4 * jj) * 8;
+    for (int jj = 0; jj < 2; ++jj) {
+      const int kc = s * kTcK + (pg + 4 * jj) * 8;
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int k = kc + e;
-          float2 f = make_float2(0.f, 0.f);
-          if (pvalid && k < dim)
-            f = __bfloat1622float2(
-                *reinterpret_cast<const __nv_bfloat162 *>(pin + size_t(k) * ncols));
-          v[2 * jj][e] = f.x;
-          v[2 * jj + 1][e] = f.y;
-        }
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int kc = s * kTcK + (cgrp + 2 * j) * 8;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int k = kc + e;
-          v[j][e] = (nvalid && k < dim) ? to_f32(in[in_base + size_t(k) * in_kstride]) : 0.f;
-        }
+      for (int e = 0; e < 8; ++e) {
+        const int k = kc + e;
+        float2 f = make_float2(0.f, 0.f);
+        if (pvalid && k < dim) f = ld_pair(pin + size_t(k) * in_kstride);
+        v[2 * jj][e] = f.x;
+        v[2 * jj + 1][e] = f.y;
       }
     }
   };
@@ -242,9 +235,7 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
     uint8_t *a_st = sm + lay.a_off[0] + st * kTcABytes;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      // (chunk, column) of v[j]: as loaded above
-      const int c = kPair ? pg + 4 * (j >> 1) : cgrp + 2 * j;
-      const int nl = kPair ? pn + (j & 1) : n_loc;
+      const int c = pg + 4 * (j >> 1), nl = pn + (j & 1);   // as loaded above
       uint4 pk;
       uint32_t *w = reinterpret_cast<uint32_t *>(&pk);
 #pragma unroll

@@ -2048,6 +2048,9 @@ extern "C" int qd_dst_precond_apply(int32_t n_dots, const int32_t *h_row_off, in
   if (n_dots <= 0 || !h_row_off || !h_prec || !d_prec_mats || !d_in || !d_out || !d_work || b < 4)
     return QD_ERR_INVALID;
   if (reinterpret_cast<uintptr_t>(d_prec_mats) % 16) return QD_ERR_INVALID;
+  // the transform passes read adjacent column pairs (up to 16 bytes at once)
+  if (b % 2 || reinterpret_cast<uintptr_t>(d_in) % 16 || reinterpret_cast<uintptr_t>(d_out) % 16)
+    return QD_ERR_INVALID;
   for (int d = 0; d < n_dots; ++d) {
     const qd_dst_prec &q = h_prec[d];
     if (q.nx > 0 && (int64_t(q.nx) * q.ny != h_row_off[d + 1] - h_row_off[d] ||
