@@ -93,26 +93,6 @@ inline size_t tc_smem_request(int rows_max) {
 }
 
 template <typename T>
-__device__ __forceinline__ float to_f32(T v) {
-  return float(v);
-}
-template <>
-__device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) {
-  return __bfloat162float(v);
-}
-template <typename T>
-__device__ __forceinline__ __nv_bfloat16 to_bf16(T v) {
-  return __float2bfloat16_rn(float(v));
-}
-template <>
-__device__ __forceinline__ __nv_bfloat16 to_bf16<double>(double v) {
-  return __double2bfloat16(v);
-}
-template <>
-__device__ __forceinline__ __nv_bfloat16 to_bf16<__nv_bfloat16>(__nv_bfloat16 v) {
-  return v;
-}
-template <typename T>
 __device__ __forceinline__ T from_f32(float v) {
   return T(v);
 }
