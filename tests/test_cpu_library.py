@@ -125,3 +125,31 @@ def test_node_adjacency_counts():
     for g in (0, 5, m.num_nodes // 2):
         for packed in adj[ptr[g]:ptr[g + 1]]:
             assert m.elems[packed >> 4, packed & 15] == g
+
+
+def test_open_system_and_dst_entry_points_reject_bad_arguments_without_gpu():
+    """Argument checks of qd_cap_spmm and qd_dst_precond_apply return before
+    any device work."""
+    from qdsim_b200 import _native as N
+    L = N.lib()
+    p = C.c_void_p(256)   # never dereferenced: every call below is rejected or empty
+    s = None
+
+    def cap(n, b, ldx, ldy, rowptr, col, H, M, X, AX, MX):
+        return L.qd_cap_spmm(n, b, 0, rowptr, col, H, None, M, X, ldx, AX, MX, ldy, s)
+
+    full = (p, p, p, p, p, p, p)
+    assert cap(10, 0, 4, 4, *full) == N.QD_ERR_INVALID       # b < 1
+    assert cap(10, 65, 65, 65, *full) == N.QD_ERR_INVALID    # b > 64
+    assert cap(10, 8, 4, 8, *full) == N.QD_ERR_INVALID       # ldx < b
+    assert cap(10, 8, 8, 4, *full) == N.QD_ERR_INVALID       # ldy < b
+    assert cap(10, 8, 8, 8, None, *full[1:]) == N.QD_ERR_INVALID
+    assert cap(0, 8, 8, 8, *full) == N.QD_OK                  # nothing to do
+    desc = np.zeros(1, dtype=N.DST_PREC_DTYPE)
+    desc[0] = (4, 3, 0, 0, 1.0, 1.0, 0.1, 0)
+    ro = np.array([0, 12], np.int32)
+    apply = lambda b, din: L.qd_dst_precond_apply(1, N.ptr(ro), b, 1, N.ptr(desc), p, din, p, p,
+                                                  1 << 20, s)
+    assert apply(5, p) == N.QD_ERR_INVALID                    # odd column count
+    assert apply(2, p) == N.QD_ERR_INVALID                    # fewer than 4 columns
+    assert apply(4, C.c_void_p(264)) == N.QD_ERR_INVALID      # vectors not 16-byte aligned
