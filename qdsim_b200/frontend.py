@@ -1,0 +1,179 @@
+"""Drop-in for the C++ backend classes the reference's Python frontend drives.
+
+``frontend/qdsim/simulator.py`` builds ``qdsim_cpp.Mesh(Lx, Ly, nx, ny,
+element_order)`` (:228-232), ``qdsim_cpp.FEMSolver(mesh, m_star, V, cap,
+sc_solver, order, use_mpi)`` with ``assemble_matrices``, ``get_H``, ``get_M``
+(:746-766) and ``qdsim_cpp.EigenSolver(fem_solver)`` with ``solve``,
+``get_eigenvalues``, ``get_eigenvectors`` (:808-818); the bindings are
+backend/src/bindings.cpp:761-985.  Importing this module as ``qdsim_cpp``
+points that path at the GPU library:
+
+    from qdsim_b200 import frontend as qdsim_cpp
+
+Semantics kept from the C++ classes (SI units in and out):
+ - ``FEMSolver`` assembles every node (backend/src/fem.cpp:116-151 applies no
+   boundary condition: natural boundaries), H = K + V + i int eta phi phi
+   with the CAP callback as +i eta (fem.cpp:974), M the consistent mass.
+ - ``EigenSolver`` solves the Hermitian part of the pencil: the C++ solver
+   symmetrises L^-1 H L^-H and calls SelfAdjointEigenSolver
+   (backend/src/solver.cpp:118-128), which drops the CAP term.  It returns the
+   k lowest eigenvalues as complex numbers with zero imaginary part and the
+   real parts of the M-normalised eigenvectors (solver.cpp:141-163).
+Internally the mesh is scaled to nm and energies to eV (c = hbar^2/(2 m*) in
+eV nm^2), as the other drop-in solvers do; eigenvalues come back in J and
+eigenvectors are M-normalised in m^2.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .batch import DeviceBatch, HostBatch
+from .fem import C0_EV_NM2, FEMProblem, M_E, Q_E
+from .mesh import StructuredMesh
+from .solvers import _block_for, _eval
+from .workloads import Dot
+
+
+class Mesh:
+    """Structured triangular mesh of [0, Lx] x [0, Ly] (meters) with nx x ny
+    cells and P1/P2/P3 elements, in the node order of backend/src/mesh.cpp."""
+
+    def __init__(self, Lx: float, Ly: float, nx: int, ny: int, element_order: int = 1):
+        if element_order not in (1, 2, 3):
+            raise ValueError("element_order must be 1, 2 or 3")
+        self._Lx, self._Ly = float(Lx), float(Ly)
+        self._si = StructuredMesh(int(element_order), int(nx), int(ny), self._Lx, self._Ly)
+        self._nm = StructuredMesh(int(element_order), int(nx), int(ny), self._Lx * 1e9,
+                                  self._Ly * 1e9)
+
+    def get_nodes(self):
+        return self._si.nodes.copy()
+
+    def get_elements(self):
+        return self._si.elems.copy()
+
+    def get_num_nodes(self) -> int:
+        return int(self._si.num_nodes)
+
+    def get_num_elements(self) -> int:
+        return int(self._si.num_elements)
+
+    def get_element_order(self) -> int:
+        return int(self._si.order)
+
+    def get_lx(self) -> float:
+        return self._Lx
+
+    def get_ly(self) -> float:
+        return self._Ly
+
+    def get_nx(self) -> int:
+        return int(self._si.nx)
+
+    def get_ny(self) -> int:
+        return int(self._si.ny)
+
+    getNumNodes = get_num_nodes
+    getNumElements = get_num_elements
+    getElementOrder = get_element_order
+
+
+class FEMSolver:
+    """H and M of a ``Mesh`` from the reference's callbacks: ``m_star(x, y)``
+    in kg (element centroids), ``V(x, y)`` and ``cap(x, y)`` in J (nodes)."""
+
+    def __init__(self, mesh: Mesh, m_star, V, cap, sc_solver=None, order=None,
+                 use_mpi: bool = False, device="cuda"):
+        if order is not None and int(order) != mesh.get_element_order():
+            raise ValueError("order must match the mesh's element order")
+        self.mesh = mesh
+        self.m_star, self.V, self.cap = m_star, V, cap
+        self.sc_solver = sc_solver
+        self.device = torch.device(device)
+        self._prob = None
+        self._mats = None
+        self._coef = None
+
+    def is_using_mpi(self) -> bool:
+        return False
+
+    def assemble_matrices(self):
+        si, nm = self.mesh._si, self.mesh._nm
+        cen = si.centroids()
+        mstar = _eval(self.m_star, cen[:, 0], cen[:, 1])
+        c = C0_EV_NM2 * (M_E / mstar)
+        V_eV = _eval(self.V, si.nodes[:, 0], si.nodes[:, 1]) / Q_E
+        eta_eV = _eval(self.cap, si.nodes[:, 0], si.nodes[:, 1]) / Q_E
+        self._coef = (c, V_eV)
+        self._prob = FEMProblem(nm, dirichlet=False, device=self.device)
+        # Himag = -int W phi phi, so W = -eta gives the reference's +i eta
+        self._mats = self._prob.assemble(c, V_eV, -eta_eV)
+
+    def _need(self):
+        if self._mats is None:
+            raise RuntimeError("call assemble_matrices() first")
+
+    def get_H(self):
+        """Complex H (J) as a scipy CSR matrix over all nodes."""
+        self._need()
+        Hr = self._prob.to_scipy(self._mats["H"])
+        Hi = self._prob.to_scipy(self._mats["Himag"])
+        return ((Hr + 1j * Hi) * Q_E).tocsr()
+
+    def get_M(self):
+        """M (m^2) as a scipy CSR matrix over all nodes."""
+        self._need()
+        return (self._prob.to_scipy(self._mats["M"]) * 1e-18).tocsr()
+
+    def adapt_mesh(self, *args, **kwargs):
+        raise NotImplementedError("adaptive mesh refinement is not part of qdsim_b200")
+
+    def get_interpolator(self):
+        raise NotImplementedError("field interpolation is not part of qdsim_b200")
+
+    def set_potential_values(self, potential_values):
+        raise NotImplementedError("field interpolation is not part of qdsim_b200")
+
+    def use_interpolated_potential(self, enable):
+        raise NotImplementedError("field interpolation is not part of qdsim_b200")
+
+
+class EigenSolver:
+    """The k lowest levels of a ``FEMSolver``'s Hermitian pencil (K + V, M)."""
+
+    def __init__(self, fem_solver: FEMSolver):
+        self.fem = fem_solver
+        self.eigenvalues = []
+        self.eigenvectors = []
+
+    def solve(self, num_eigenpairs: int = 10):
+        fem = self.fem
+        fem._need()
+        nm = fem.mesh._nm
+        c, V_eV = fem._coef
+        k = int(min(num_eigenpairs, nm.num_nodes - 1))
+        hb = HostBatch([Dot(nm, c, V_eV)], dirichlet=False)
+        db = DeviceBatch(hb, fem.device)
+        db.upload(non_blocking=False)
+        db.assemble()
+        db.check_status()
+        # natural boundaries: the lowest level can sit at zero energy, so
+        # errors are measured relative to max(|E|, 0.01 eV)
+        E, X, _, _, _, _ = db.solve(k, b=_block_for(k), precision="mixed", tol=1e-9,
+                                    max_iter=4000, allow_not_converged=False,
+                                    eig_scale=0.01)
+        E_J = E.cpu().numpy()[0] * Q_E
+        psi = X.cpu().numpy() * 1e9          # M-normalised in nm^2 -> m^2
+        self.eigenvalues = [complex(e, 0.0) for e in E_J]
+        self.eigenvectors = [np.ascontiguousarray(psi[:, i]) for i in range(k)]
+
+    def get_eigenvalues(self):
+        return list(self.eigenvalues)
+
+    def get_eigenvectors(self):
+        return [v.copy() for v in self.eigenvectors]
+
+
+__all__ = ["Mesh", "FEMSolver", "EigenSolver"]
