@@ -315,6 +315,32 @@ int qd_cap_spmm(int32_t n, int b, int vec_fp32, const int32_t *d_rowptr, const i
                 void *d_AX, void *d_MX, int ldy, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Finite-element field evaluation at arbitrary points on the structured
+ * order-p mesh of [0, Lx] x [0, Ly] with nx x ny cells (lattice node order,
+ * element 2 (cj nx + ci) + t).  Replaces FEInterpolator::interpolate,
+ * interpolateWithGradient and findElement
+ * (backend/src/fe_interpolator.cpp:54-431) and interpolate_field_kernel
+ * (backend/src/gpu_kernels.cu:352-423), which scan every element per point;
+ * here the point's cell is computed and only the 3 x 3 cells around it are
+ * tested, in element order, so the containing element is the one the scan
+ * returns (first with all barycentric coordinates >= -1e-10).
+ *   d_field     nfield fields, field f at d_field + f * field_stride
+ *               (field_stride >= number of nodes)
+ *   d_x, d_y    npts query points
+ *   d_value     [nfield * npts] values, value[f * npts + i]
+ *   d_grad_x/y  [nfield * npts] gradients, both NULL for none
+ *   d_element   [npts] containing element or -1 (NULL for none)
+ *   outside_zero  0: points outside every element take the nearest node's
+ *               value and the reference's neighbour-difference gradient
+ *               estimate (FEInterpolator); 1: value and gradient 0
+ *               (interpolate_field_kernel).
+ * Returns QD_ERR_LIMIT when node or element indices would exceed int32. */
+int qd_fe_interpolate(int order, int32_t nx, int32_t ny, double Lx, double Ly, int nfield,
+                      int64_t field_stride, const double *d_field, int64_t npts,
+                      const double *d_x, const double *d_y, double *d_value, double *d_grad_x,
+                      double *d_grad_y, int32_t *d_element, int outside_zero, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Adjoint (Hellmann-Feynman) gradients of L = sum_s w_s E_s with respect to
  * nodal V and the per-element kinetic coefficient c.  With M-normalised
  * eigenvectors, dE_s/dV_l = psi_s^T (dH/dV_l) psi_s and

@@ -60,6 +60,8 @@ SIGNATURES = {
     "qd_pcg_solve_static": (_int, [_i32, _int, _p, _p, _p, _p, _p, _p, _dbl, _int, _p, _p, _p]),
     "qd_csr_spmv": (_int, [_i32, _int, _p, _p, _p, _p, _p, _dbl, _p]),
     "qd_cap_spmm": (_int, [_i32, _int, _int, _p, _p, _p, _p, _p, _p, _int, _p, _p, _int, _p]),
+    "qd_fe_interpolate": (_int, [_int, _i32, _i32, _dbl, _dbl, _int, _i64, _p, _i64, _p, _p,
+                                 _p, _p, _p, _p, _int, _p]),
     "qd_prof_enable": (_int, [_int]),
     "qd_prof_read": (_int, [_p, _p, _int]),
     "qd_sc_potential": (_int, [_i32, _i64, _p, _p, _p, _p]),

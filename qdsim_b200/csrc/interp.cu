@@ -1,0 +1,433 @@
+// Evaluation of nodal P1/P2/P3 fields of the structured triangular mesh at
+// arbitrary points: value, optional gradient and containing element.
+//
+// Replaces FEInterpolator::interpolate / interpolateWithGradient / findElement
+// (backend/src/fe_interpolator.cpp:54-431), which search every element of the
+// mesh for each point, and interpolate_field_kernel
+// (backend/src/gpu_kernels.cu:352-423), the same linear scan per thread.  On
+// the structured mesh the containing cell follows from the coordinates: a
+// point well inside the triangle of its own cell is settled by one
+// barycentric test; a point near an edge is tested against the triangles of
+// the 3 x 3 cells around it in element-index order, and the first whose
+// barycentric coordinates are all >= -1e-10 wins.  Both give the element the
+// reference's scan over all elements returns (a triangle passing that test
+// lies within 1e-10 of a triangle height of the point, so inside that window).
+//
+// Mesh layout (qdsim_b200/mesh.py, backend/src/mesh.cpp:66-115): lattice of
+// NX = p nx + 1 by NY = p ny + 1 nodes, node = iy NX + ix at
+// (ix Lx / (p nx), iy Ly / (p ny)); cell (ci, cj) holds elements
+// 2 (cj nx + ci) + t with vertices t = 0: (v00, v10, v01), t = 1:
+// (v10, v11, v01); local node a sits at the lattice point
+// (bc_a . vertices) / p for the integer barycentric multi-index bc_a.
+//
+// Points outside every element take, as FEInterpolator does, the value of the
+// nearest node (first in node order on ties) and a gradient estimated from
+// the nodes that share an element with it (inverse-distance weighted
+// directional differences, fe_interpolator.cpp:163-270), or zero, as
+// interpolate_field_kernel does.
+#include <cuda_runtime.h>
+#include <cfloat>
+#include <cstdint>
+#include "common.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr double kInsideEps = 1e-10;
+// unique neighbours of a node over the elements that contain it: at most
+// 6 triangles x 9 other nodes for P3
+constexpr int kMaxLinked = 64;
+
+struct Geo {
+  int nx, ny, NX, NY;
+  double hx, hy;    // cell size
+  double hxl, hyl;  // lattice spacing
+  double margin;    // interior depth that rules out every other triangle
+};
+
+// integer barycentric multi-indices of the local nodes (x order)
+template <int P> struct Local;
+template <> struct Local<1> {
+  static constexpr int K = 3;
+  __host__ __device__ static int b(int a, int m) {
+    constexpr int t[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    return t[a][m];
+  }
+};
+template <> struct Local<2> {
+  static constexpr int K = 6;
+  __host__ __device__ static int b(int a, int m) {
+    constexpr int t[6][3] = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
+    return t[a][m];
+  }
+};
+template <> struct Local<3> {
+  static constexpr int K = 10;
+  __host__ __device__ static int b(int a, int m) {
+    constexpr int t[10][3] = {{3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0}, {1, 2, 0},
+                              {0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {2, 0, 1}, {1, 1, 1}};
+    return t[a][m];
+  }
+};
+
+// cell-lattice corners (in cell units) of triangle t of cell (ci, cj)
+__host__ __device__ __forceinline__ void tri_corners(int ci, int cj, int t, int cx[3], int cy[3]) {
+  if (t == 0) {
+    cx[0] = ci;     cy[0] = cj;
+    cx[1] = ci + 1; cy[1] = cj;
+    cx[2] = ci;     cy[2] = cj + 1;
+  } else {
+    cx[0] = ci + 1; cy[0] = cj;
+    cx[1] = ci + 1; cy[1] = cj + 1;
+    cx[2] = ci;     cy[2] = cj + 1;
+  }
+}
+
+// Barycentric coordinates by the signed-area formula of
+// fe_interpolator.cpp:433-457 (same association of terms); returns the
+// triangle's signed area.
+__host__ __device__ __forceinline__ double bary(const double vx[3], const double vy[3], double x, double y,
+                                       double l[3]) {
+  const double area =
+      0.5 * ((vx[1] - vx[0]) * (vy[2] - vy[0]) - (vx[2] - vx[0]) * (vy[1] - vy[0]));
+  l[0] = 0.5 * ((vx[1] * vy[2] - vx[2] * vy[1]) + (vy[1] - vy[2]) * x + (vx[2] - vx[1]) * y) / area;
+  l[1] = 0.5 * ((vx[2] * vy[0] - vx[0] * vy[2]) + (vy[2] - vy[0]) * x + (vx[0] - vx[2]) * y) / area;
+  l[2] = 0.5 * ((vx[0] * vy[1] - vx[1] * vy[0]) + (vy[0] - vy[1]) * x + (vx[1] - vx[0]) * y) / area;
+  return area;
+}
+
+// Shape values phi_a and derivatives d phi_a / d lambda_m of the Lagrange
+// basis at the local nodes (the functions of fe_interpolator.cpp:474-613).
+template <int P>
+__host__ __device__ __forceinline__ void shape(const double l[3], double phi[], double dphi[][3]);
+
+template <>
+__host__ __device__ __forceinline__ void shape<1>(const double l[3], double phi[], double dphi[][3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    phi[a] = l[a];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) dphi[a][m] = a == m ? 1.0 : 0.0;
+  }
+}
+
+template <>
+__host__ __device__ __forceinline__ void shape<2>(const double l[3], double phi[], double dphi[][3]) {
+#pragma unroll
+  for (int a = 0; a < 6; ++a)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) dphi[a][m] = 0.0;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    phi[m] = l[m] * (2.0 * l[m] - 1.0);
+    dphi[m][m] = 4.0 * l[m] - 1.0;
+  }
+  // edge nodes 3, 4, 5 on edges (0, 1), (1, 2), (2, 0)
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const int i = e, j = (e + 1) % 3;
+    phi[3 + e] = 4.0 * l[i] * l[j];
+    dphi[3 + e][i] = 4.0 * l[j];
+    dphi[3 + e][j] = 4.0 * l[i];
+  }
+}
+
+template <>
+__host__ __device__ __forceinline__ void shape<3>(const double l[3], double phi[], double dphi[][3]) {
+#pragma unroll
+  for (int a = 0; a < 10; ++a)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) dphi[a][m] = 0.0;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    phi[m] = 0.5 * l[m] * (3.0 * l[m] - 1.0) * (3.0 * l[m] - 2.0);
+    dphi[m][m] = 0.5 * (27.0 * l[m] * l[m] - 18.0 * l[m] + 2.0);
+  }
+  // edge (i, j) carries node 3 + 2e next to vertex i and 4 + 2e next to j
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const int i = e, j = (e + 1) % 3;
+    const int ni = 3 + 2 * e, nj = 4 + 2 * e;
+    phi[ni] = 4.5 * l[i] * l[j] * (3.0 * l[i] - 1.0);
+    phi[nj] = 4.5 * l[i] * l[j] * (3.0 * l[j] - 1.0);
+    dphi[ni][i] = 4.5 * l[j] * (6.0 * l[i] - 1.0);
+    dphi[ni][j] = 4.5 * l[i] * (3.0 * l[i] - 1.0);
+    dphi[nj][i] = 4.5 * l[j] * (3.0 * l[j] - 1.0);
+    dphi[nj][j] = 4.5 * l[i] * (6.0 * l[j] - 1.0);
+  }
+  phi[9] = 27.0 * l[0] * l[1] * l[2];
+  dphi[9][0] = 27.0 * l[1] * l[2];
+  dphi[9][1] = 27.0 * l[0] * l[2];
+  dphi[9][2] = 27.0 * l[0] * l[1];
+}
+
+// global node index of local node a of triangle (ci, cj, t)
+template <int P>
+__host__ __device__ __forceinline__ int local_node(const Geo &g, const int cx[3], const int cy[3], int a) {
+  int lx = 0, ly = 0;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    lx += Local<P>::b(a, m) * cx[m];
+    ly += Local<P>::b(a, m) * cy[m];
+  }
+  // corners are in cell units, so (bc . P corners) / P = bc . corners
+  return ly * g.NX + lx;
+}
+
+__host__ __device__ __forceinline__ int clamp_cell(double q, int hi) {
+  // fmax/fmin return the other operand for NaN, so NaN lands on cell 0
+  return int(fmin(fmax(floor(q), 0.0), double(hi)));
+}
+
+// Nearest lattice node to (x, y) by the squared distance, the first in node
+// order on ties, or -1 when no distance is below DBL_MAX (non-finite or
+// overflowing coordinates), as the reference's scan over all nodes.
+__host__ __device__ int nearest_node(const Geo &g, double x, double y) {
+  const int jx = clamp_cell(x / g.hxl, g.NX - 1), jy = clamp_cell(y / g.hyl, g.NY - 1);
+  double best = DBL_MAX;
+  int node = -1;
+  for (int iy = max(jy - 1, 0); iy <= min(jy + 1, g.NY - 1); ++iy) {
+    const double dy = y - double(iy) * g.hyl;
+    for (int ix = max(jx - 1, 0); ix <= min(jx + 1, g.NX - 1); ++ix) {
+      const double dx = x - double(ix) * g.hxl;
+      const double d = dx * dx + dy * dy;
+      if (d < best) {
+        best = d;
+        node = iy * g.NX + ix;
+      }
+    }
+  }
+  return node;
+}
+
+// Gradient estimate at a node from the nodes sharing an element with it, in
+// the order the reference discovers them (elements ascending, local order),
+// each counted once (fe_interpolator.cpp:186-266).
+template <int P>
+__host__ __device__ __noinline__ void node_gradient(const Geo &g, int node, int nfield, int64_t fstride,
+                                           const double *__restrict__ field, int64_t npts,
+                                           int64_t i, double *gx, double *gy) {
+  const int ix = node % g.NX, iy = node / g.NX;
+  const double x0 = double(ix) * g.hxl, y0 = double(iy) * g.hyl;
+  int linked[kMaxLinked];
+  int nl = 0;
+  const int ci0 = max((ix + P - 1) / P - 1, 0), ci1 = min(ix / P, g.nx - 1);
+  const int cj0 = max((iy + P - 1) / P - 1, 0), cj1 = min(iy / P, g.ny - 1);
+  for (int cj = cj0; cj <= cj1; ++cj)
+    for (int ci = ci0; ci <= ci1; ++ci)
+      for (int t = 0; t < 2; ++t) {
+        int cx[3], cy[3];
+        tri_corners(ci, cj, t, cx, cy);
+        int self = -1;
+        for (int a = 0; a < Local<P>::K && self < 0; ++a)
+          if (local_node<P>(g, cx, cy, a) == node) self = a;
+        if (self < 0) continue;
+        for (int a = 0; a < Local<P>::K; ++a) {
+          if (a == self) continue;
+          const int q = local_node<P>(g, cx, cy, a);
+          bool seen = false;
+          for (int s = 0; s < nl; ++s) seen = seen || linked[s] == q;
+          if (!seen && nl < kMaxLinked) linked[nl++] = q;
+        }
+      }
+  for (int f = 0; f < nfield; ++f) {
+    const double *fv = field + f * fstride;
+    const double f0 = fv[node];
+    double sx = 0.0, sy = 0.0, wsum = 0.0;
+    for (int s = 0; s < nl; ++s) {
+      const int q = linked[s];
+      const double dx = double(q % g.NX) * g.hxl - x0;
+      const double dy = double(q / g.NX) * g.hyl - y0;
+      const double dist = sqrt(dx * dx + dy * dy);
+      if (dist > 1e-10) {
+        const double w = 1.0 / dist;
+        const double df = fv[q] - f0;
+        sx += w * (df * dx / dist);
+        sy += w * (df * dy / dist);
+        wsum += w;
+      }
+    }
+    gx[f * npts + i] = wsum > 0.0 ? sx / wsum : 0.0;
+    gy[f * npts + i] = wsum > 0.0 ? sy / wsum : 0.0;
+  }
+}
+
+// Value (and gradient) of every field and the containing element at point i.
+template <int P, bool GRAD>
+__host__ __device__ __forceinline__ void interp_point(
+    const Geo &g, int nfield, int64_t fstride, const double *__restrict__ field, int64_t npts,
+    int64_t i, double x, double y, double *__restrict__ val, double *__restrict__ gx,
+    double *__restrict__ gy, int32_t *__restrict__ elem, int outside_zero) {
+  constexpr int K = Local<P>::K;
+  int found = -1, fcx[3], fcy[3];
+  double l[3], vx[3], vy[3];
+  // Fast path: the triangle of the point's own cell.  A point that lies
+  // deeper than g.margin inside it (every barycentric coordinate at least
+  // g.margin) is farther from every other triangle than their -1e-10
+  // acceptance band reaches, so this is the only element the scan finds.
+  const double qx = x / g.hx, qy = y / g.hy;
+  const int ci0 = clamp_cell(qx, g.nx - 1), cj0 = clamp_cell(qy, g.ny - 1);
+  {
+    const int t = (qx - ci0) + (qy - cj0) > 1.0 ? 1 : 0;
+    tri_corners(ci0, cj0, t, fcx, fcy);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      vx[m] = double(P * fcx[m]) * g.hxl;
+      vy[m] = double(P * fcy[m]) * g.hyl;
+    }
+    bary(vx, vy, x, y, l);
+    if (l[0] >= g.margin && l[1] >= g.margin && l[2] >= g.margin)
+      found = 2 * (cj0 * g.nx + ci0) + t;
+  }
+  // Otherwise the ordered scan of the 3 x 3 cells around it.
+  for (int cj = max(cj0 - 1, 0); cj <= min(cj0 + 1, g.ny - 1) && found < 0; ++cj)
+    for (int ci = max(ci0 - 1, 0); ci <= min(ci0 + 1, g.nx - 1) && found < 0; ++ci)
+      for (int t = 0; t < 2 && found < 0; ++t) {
+        int cx[3], cy[3];
+        tri_corners(ci, cj, t, cx, cy);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          vx[m] = double(P * cx[m]) * g.hxl;
+          vy[m] = double(P * cy[m]) * g.hyl;
+        }
+        bary(vx, vy, x, y, l);
+        if (l[0] >= -kInsideEps && l[1] >= -kInsideEps && l[2] >= -kInsideEps) {
+          found = 2 * (cj * g.nx + ci) + t;
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            fcx[m] = cx[m];
+            fcy[m] = cy[m];
+          }
+        }
+      }
+  if (elem) elem[i] = found;
+  if (found >= 0) {
+    double phi[K], dphi[K][3];
+    shape<P>(l, phi, dphi);
+    int nodes[K];
+#pragma unroll
+    for (int a = 0; a < K; ++a) nodes[a] = local_node<P>(g, fcx, fcy, a);
+    // gradients of the barycentric coordinates (fe_interpolator.cpp:542-566)
+    double glx[3] = {0, 0, 0}, gly[3] = {0, 0, 0};
+    if (GRAD) {
+      const double area =
+          0.5 * ((vx[1] - vx[0]) * (vy[2] - vy[0]) - (vx[2] - vx[0]) * (vy[1] - vy[0]));
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const int j = (m + 1) % 3, k = (m + 2) % 3;
+        glx[m] = 0.5 * (vy[j] - vy[k]) / area;
+        gly[m] = 0.5 * (vx[k] - vx[j]) / area;
+      }
+    }
+    for (int f = 0; f < nfield; ++f) {
+      const double *fv = field + f * fstride;
+      double v = 0.0, sx = 0.0, sy = 0.0;
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        const double fa = fv[nodes[a]];
+        v += fa * phi[a];
+        if (GRAD) {
+          const double bx = dphi[a][0] * glx[0] + dphi[a][1] * glx[1] + dphi[a][2] * glx[2];
+          const double by = dphi[a][0] * gly[0] + dphi[a][1] * gly[1] + dphi[a][2] * gly[2];
+          sx += fa * bx;
+          sy += fa * by;
+        }
+      }
+      val[f * npts + i] = v;
+      if (GRAD) {
+        gx[f * npts + i] = sx;
+        gy[f * npts + i] = sy;
+      }
+    }
+    return;
+  }
+  const int node = outside_zero ? -1 : nearest_node(g, x, y);
+  for (int f = 0; f < nfield; ++f) val[f * npts + i] = node >= 0 ? field[f * fstride + node] : 0.0;
+  if (GRAD) {
+    if (node >= 0) {
+      node_gradient<P>(g, node, nfield, fstride, field, npts, i, gx, gy);
+    } else {
+      for (int f = 0; f < nfield; ++f) gx[f * npts + i] = gy[f * npts + i] = 0.0;
+    }
+  }
+}
+
+template <int P, bool GRAD>
+__global__ void __launch_bounds__(kThreads)
+interp_kernel(Geo g, int nfield, int64_t fstride, const double *__restrict__ field, int64_t npts,
+              const double *__restrict__ px, const double *__restrict__ py,
+              double *__restrict__ val, double *__restrict__ gx, double *__restrict__ gy,
+              int32_t *__restrict__ elem, int outside_zero) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npts;
+       i += int64_t(gridDim.x) * blockDim.x)
+    interp_point<P, GRAD>(g, nfield, fstride, field, npts, i, px[i], py[i], val, gx, gy, elem,
+                          outside_zero);
+}
+
+// Mesh geometry of the launch (arguments already checked).
+Geo make_geo(int order, int32_t nx, int32_t ny, double Lx, double Ly) {
+  Geo g;
+  g.nx = nx;
+  g.ny = ny;
+  g.NX = order * nx + 1;
+  g.NY = order * ny + 1;
+  g.hx = Lx / nx;
+  g.hy = Ly / ny;
+  g.hxl = Lx / double(int64_t(order) * nx);
+  g.hyl = Ly / double(int64_t(order) * ny);
+  // Triangle T' accepts points within 1e-10 of its heights outside it; near
+  // a corner of angle a that band reaches 1e-10 h_max / sin(a).  A point at
+  // barycentric depth d inside T is at least d h_min from T's boundary, with
+  // h_min the height onto the hypotenuse; the band around T' reaches at most
+  // 2e-10 h_max / sin(a_min) past it.  d at twice that ratio makes T the only
+  // triangle that passes.
+  {
+    const double hyp = sqrt(g.hx * g.hx + g.hy * g.hy);
+    const double hmax = fmax(g.hx, g.hy), hmin = g.hx * g.hy / hyp;
+    const double sin_min = fmin(g.hx, g.hy) / hyp;
+    g.margin = 4.0 * kInsideEps * hmax / (hmin * sin_min);
+  }
+  return g;
+}
+
+template <int P>
+int launch(const Geo &g, int nfield, int64_t fstride, const double *field, int64_t npts,
+           const double *x, const double *y, double *val, double *gx, double *gy, int32_t *elem,
+           int outside_zero, cudaStream_t s) {
+  const int64_t want = (npts + kThreads - 1) / kThreads;
+  const unsigned blocks = unsigned(want < 148 * 16 ? want : 148 * 16);
+  if (gx)
+    interp_kernel<P, true><<<blocks, kThreads, 0, s>>>(g, nfield, fstride, field, npts, x, y, val,
+                                                       gx, gy, elem, outside_zero);
+  else
+    interp_kernel<P, false><<<blocks, kThreads, 0, s>>>(g, nfield, fstride, field, npts, x, y,
+                                                        val, nullptr, nullptr, elem, outside_zero);
+  QD_CHECK_LAUNCH();
+  return QD_OK;
+}
+
+}  // namespace
+
+extern "C" int qd_fe_interpolate(int order, int32_t nx, int32_t ny, double Lx, double Ly,
+                                 int nfield, int64_t field_stride, const double *d_field,
+                                 int64_t npts, const double *d_x, const double *d_y,
+                                 double *d_value, double *d_grad_x, double *d_grad_y,
+                                 int32_t *d_element, int outside_zero, void *stream) {
+  if (order < 1 || order > 3 || nx < 1 || ny < 1 || !(Lx > 0.0) || !(Ly > 0.0) ||
+      !(Lx < DBL_MAX) || !(Ly < DBL_MAX) || nfield < 1 || npts < 0 ||
+      (outside_zero != 0 && outside_zero != 1) || (d_grad_x == nullptr) != (d_grad_y == nullptr))
+    return QD_ERR_INVALID;
+  const int64_t NX = int64_t(order) * nx + 1, NY = int64_t(order) * ny + 1;
+  // node and element indices are int32
+  if (NX * NY > INT32_MAX || 2 * int64_t(nx) * ny > INT32_MAX) return QD_ERR_LIMIT;
+  if (field_stride < NX * NY || (npts > 0 && (!d_field || !d_x || !d_y || !d_value)))
+    return QD_ERR_INVALID;
+  if (npts == 0) return QD_OK;
+  const Geo g = make_geo(order, nx, ny, Lx, Ly);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (order) {
+    case 1: return launch<1>(g, nfield, field_stride, d_field, npts, d_x, d_y, d_value, d_grad_x, d_grad_y, d_element, outside_zero, s);
+    case 2: return launch<2>(g, nfield, field_stride, d_field, npts, d_x, d_y, d_value, d_grad_x, d_grad_y, d_element, outside_zero, s);
+    default: return launch<3>(g, nfield, field_stride, d_field, npts, d_x, d_y, d_value, d_grad_x, d_grad_y, d_element, outside_zero, s);
+  }
+}

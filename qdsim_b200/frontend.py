@@ -5,8 +5,9 @@ element_order)`` (:228-232), ``qdsim_cpp.FEMSolver(mesh, m_star, V, cap,
 sc_solver, order, use_mpi)`` with ``assemble_matrices``, ``get_H``, ``get_M``
 (:746-766) and ``qdsim_cpp.EigenSolver(fem_solver)`` with ``solve``,
 ``get_eigenvalues``, ``get_eigenvectors`` (:808-818); the bindings are
-backend/src/bindings.cpp:761-985.  Importing this module as ``qdsim_cpp``
-points that path at the GPU library:
+backend/src/bindings.cpp:761-985, ``FEInterpolator(mesh)`` among them
+(:779-809).  Importing this module as ``qdsim_cpp`` points that path at the
+GPU library:
 
     from qdsim_b200 import frontend as qdsim_cpp
 
@@ -19,6 +20,13 @@ Semantics kept from the C++ classes (SI units in and out):
    (backend/src/solver.cpp:118-128), which drops the CAP term.  It returns the
    k lowest eigenvalues as complex numbers with zero imaginary part and the
    real parts of the M-normalised eigenvectors (solver.cpp:141-163).
+ - ``FEMSolver.set_potential_values`` / ``use_interpolated_potential`` make the
+   assembly use the finite-element interpolant of the given nodal potential
+   (J) instead of the ``V`` callback (fem.cpp:441-462, :930-937).
+ - ``FEInterpolator`` evaluates nodal fields at points on the GPU
+   (``qd_fe_interpolate``): the reference's element scan becomes an O(1)
+   cell lookup with the same containing element, and points outside the mesh
+   take the nearest node's value and the reference's gradient estimate.
 Internally the mesh is scaled to nm and energies to eV (c = hbar^2/(2 m*) in
 eV nm^2), as the other drop-in solvers do; eigenvalues come back in J and
 eigenvectors are M-normalised in m^2.
@@ -31,6 +39,7 @@ import torch
 from . import _native as N
 from .batch import DeviceBatch, HostBatch
 from .fem import C0_EV_NM2, FEMProblem, M_E, Q_E
+from .interp import FieldInterpolator
 from .mesh import StructuredMesh
 from .solvers import _block_for, _eval
 from .workloads import Dot
@@ -95,6 +104,9 @@ class FEMSolver:
         self._prob = None
         self._mats = None
         self._coef = None
+        self._potential = np.zeros(mesh.get_num_nodes())
+        self._use_interp = False
+        self._interp = None
 
     def is_using_mpi(self) -> bool:
         return False
@@ -104,7 +116,10 @@ class FEMSolver:
         cen = si.centroids()
         mstar = _eval(self.m_star, cen[:, 0], cen[:, 1])
         c = C0_EV_NM2 * (M_E / mstar)
-        V_eV = _eval(self.V, si.nodes[:, 0], si.nodes[:, 1]) / Q_E
+        if self._use_interp:
+            V_eV = self._potential / Q_E
+        else:
+            V_eV = _eval(self.V, si.nodes[:, 0], si.nodes[:, 1]) / Q_E
         eta_eV = _eval(self.cap, si.nodes[:, 0], si.nodes[:, 1]) / Q_E
         self._coef = (c, V_eV)
         self._prob = FEMProblem(nm, dirichlet=False, device=self.device)
@@ -131,13 +146,82 @@ class FEMSolver:
         raise NotImplementedError("adaptive mesh refinement is not part of qdsim_b200")
 
     def get_interpolator(self):
-        raise NotImplementedError("field interpolation is not part of qdsim_b200")
+        if self._interp is None:
+            self._interp = FEInterpolator(self.mesh, device=self.device)
+        return self._interp
 
     def set_potential_values(self, potential_values):
-        raise NotImplementedError("field interpolation is not part of qdsim_b200")
+        """Nodal potential (J) for the interpolated-potential assembly; the
+        length must be the number of nodes (fem.cpp:441-449)."""
+        v = np.asarray(potential_values, dtype=np.float64).reshape(-1)
+        if v.size != self.mesh.get_num_nodes():
+            raise ValueError("potential_values must have one value per mesh node")
+        self._potential = v.copy()
 
     def use_interpolated_potential(self, enable):
-        raise NotImplementedError("field interpolation is not part of qdsim_b200")
+        self._use_interp = bool(enable)
+
+
+class FEInterpolator:
+    """Field evaluation on a ``Mesh`` (backend/src/fe_interpolator.cpp) with the
+    reference's method names; coordinates are in the mesh's units.  Every
+    evaluation is one ``qd_fe_interpolate`` launch; the ``*_vector`` /
+    ``*_points`` forms take whole arrays of points in one launch."""
+
+    def __init__(self, mesh: Mesh, device="cuda"):
+        self.mesh = mesh
+        self._fi = FieldInterpolator(mesh._si, device=device)
+        self._fz = FieldInterpolator(mesh._si, device=device, outside="zero")
+
+    def _one(self, x, y, field, gradient=False, element=False):
+        return self._fi.evaluate([float(x)], [float(y)], field, gradient=gradient,
+                                 element=element)
+
+    def interpolate(self, x, y, field) -> float:
+        return float(self._one(x, y, field)["value"][0])
+
+    def interpolate_with_gradient(self, x, y, field):
+        r = self._one(x, y, field, gradient=True)
+        return (float(r["value"][0]), float(r["grad_x"][0]), float(r["grad_y"][0]))
+
+    def interpolate_gradient(self, x, y, field):
+        _, gx, gy = self.interpolate_with_gradient(x, y, field)
+        return (gx, gy)
+
+    def find_element(self, x, y) -> int:
+        field = torch.zeros(self.mesh.get_num_nodes(), dtype=torch.float64)
+        return int(self._fz.evaluate([float(x)], [float(y)], field, element=True)["element"][0])
+
+    find_containing_element = find_element
+
+    def is_inside_domain(self, x, y) -> bool:
+        return self.find_element(x, y) >= 0
+
+    def interpolate_vector(self, x_points, y_points, field):
+        """Values at many points (numpy array), one launch."""
+        x = np.asarray(x_points, dtype=np.float64).reshape(-1)
+        y = np.asarray(y_points, dtype=np.float64).reshape(-1)
+        if x.size != y.size:
+            raise ValueError("x_points and y_points must have same length")
+        return self._fi.evaluate(x, y, field)["value"].cpu().numpy()
+
+    def interpolate_points(self, x_points, y_points, field, gradient=False, zero_outside=False):
+        """Values (and gradients) of one or more fields at many points as
+        device tensors, one launch (``FieldInterpolator.evaluate``)."""
+        fi = self._fz if zero_outside else self._fi
+        return fi.evaluate(x_points, y_points, field, gradient=gradient, element=True)
+
+    @staticmethod
+    def compute_barycentric_coordinates(x, y, vertices):
+        """(inside, [l0, l1, l2]) of (x, y) in the triangle ``vertices``
+        (fe_interpolator.cpp:433-472): signed-area formula, inside when every
+        coordinate is >= -1e-10."""
+        (x0, y0), (x1, y1), (x2, y2) = [(float(v[0]), float(v[1])) for v in vertices[:3]]
+        area = 0.5 * ((x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0))
+        lam = [0.5 * ((x1 * y2 - x2 * y1) + (y1 - y2) * x + (x2 - x1) * y) / area,
+               0.5 * ((x2 * y0 - x0 * y2) + (y2 - y0) * x + (x0 - x2) * y) / area,
+               0.5 * ((x0 * y1 - x1 * y0) + (y0 - y1) * x + (x1 - x0) * y) / area]
+        return (all(v >= -1e-10 for v in lam), lam)
 
 
 class EigenSolver:
@@ -176,4 +260,4 @@ class EigenSolver:
         return [v.copy() for v in self.eigenvectors]
 
 
-__all__ = ["Mesh", "FEMSolver", "EigenSolver"]
+__all__ = ["Mesh", "FEMSolver", "EigenSolver", "FEInterpolator"]

@@ -2,12 +2,18 @@
 
     python -m qdsim_b200.kernels_bench cap_spmm [--prec fp64|fp32] [--b 48] [--launches 10]
     python -m qdsim_b200.kernels_bench pcg [--iters 32]
+    python -m qdsim_b200.kernels_bench interp [--points 16777216] [--gradient] [--launches 10]
 
 ``cap_spmm``: ``qd_cap_spmm`` on the open-system pencil of P2 400x200 cells on
 200x100 nm (318,801 DOFs, 3.65M nonzeros) for a block of b complex columns;
 prints ms per launch and GB/s of algorithmic bytes.  ``pcg``: the Jacobi-PCG
 of the p-n junction's Poisson step (P1 300x100 cells, 30,401 nodes, 64
 right-hand sides) for a fixed number of iterations; prints ms per iteration.
+``interp``: ``qd_fe_interpolate`` of one nodal field of the P2 400x200-cell
+mesh on 200x100 nm at uniformly random points (values, optionally gradients
+and elements); prints ms per launch and GB/s of algorithmic bytes (16 B of
+coordinates in, 8 B per value out, 20 B more with gradients and elements, the
+field read once).
 The launch sequence is fixed, so a profiler can select launches by index.
 """
 from __future__ import annotations
@@ -72,18 +78,49 @@ def pcg(iters: int, dev):
             "algorithmic_bytes_per_iteration": int(alg), "GBps": alg / (ms * 1e-3) / 1e9}
 
 
+def interp(points: int, gradient: bool, launches: int, dev):
+    from .interp import FieldInterpolator
+    from .mesh import StructuredMesh
+    m = StructuredMesh(2, 400, 200, 200.0, 100.0)
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.rand(points, generator=g, device=dev, dtype=torch.float64) * m.Lx
+    y = torch.rand(points, generator=g, device=dev, dtype=torch.float64) * m.Ly
+    f = torch.randn(m.num_nodes, generator=g, device=dev, dtype=torch.float64)
+    fi = FieldInterpolator(m, device=dev)
+    fi.evaluate(x, y, f, gradient=gradient, element=gradient)   # launch 0 (warm-up)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        fi.evaluate(x, y, f, gradient=gradient, element=gradient)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    alg = points * (16 + 8 + (20 if gradient else 0)) + m.num_nodes * 8
+    return {"kernel": "interp_kernel", "order": 2, "nodes": int(m.num_nodes), "points": points,
+            "gradient": gradient, "ms_per_launch": ms, "algorithmic_bytes": int(alg),
+            "GBps": alg / (ms * 1e-3) / 1e9, "Gpoints_per_s": points / (ms * 1e-3) / 1e9}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["cap_spmm", "pcg"])
+    ap.add_argument("case", choices=["cap_spmm", "pcg", "interp"])
     ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--b", type=int, default=48)
     ap.add_argument("--launches", type=int, default=10)
     ap.add_argument("--iters", type=int, default=32)
+    ap.add_argument("--points", type=int, default=1 << 24)
+    ap.add_argument("--gradient", action="store_true")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("a CUDA device is required")
     dev = torch.device("cuda:0")
-    r = cap_spmm(a.prec, a.b, a.launches, dev) if a.case == "cap_spmm" else pcg(a.iters, dev)
+    if a.case == "cap_spmm":
+        r = cap_spmm(a.prec, a.b, a.launches, dev)
+    elif a.case == "pcg":
+        r = pcg(a.iters, dev)
+    else:
+        r = interp(a.points, a.gradient, a.launches, dev)
     print(json.dumps(r))
 
 

@@ -1,0 +1,142 @@
+"""Finite-element field interpolation without a GPU: the oracle pinned by known
+answers, the C entry point's argument checks and the frontend's host logic.
+
+The reference's FEInterpolator (backend/src/fe_interpolator.cpp) needs Eigen,
+which this image lacks, so its outputs cannot be generated here; the oracle is
+pinned instead by properties any correct implementation of that file has:
+nodal values are reproduced, polynomials of the element degree are reproduced
+with their gradients, the first element in index order wins on shared edges,
+and outside points follow the nearest-node rule and its gradient estimate,
+computed here by hand.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle.fem import structured_mesh
+from oracle.interp import Interpolator, barycentric
+
+
+def _poly(order, x, y):
+    """A polynomial of total degree ``order`` and its gradient."""
+    if order == 1:
+        return 0.3 + 1.7 * x - 0.9 * y, 1.7 + 0 * x, -0.9 + 0 * y
+    if order == 2:
+        f = 0.3 + 1.7 * x - 0.9 * y + 0.05 * x * x - 0.11 * x * y + 0.07 * y * y
+        return f, 1.7 + 0.1 * x - 0.11 * y, -0.9 - 0.11 * x + 0.14 * y
+    f = (0.3 + 1.7 * x - 0.9 * y + 0.05 * x * x - 0.11 * x * y + 0.07 * y * y
+         + 0.004 * x ** 3 - 0.003 * x * x * y + 0.002 * x * y * y - 0.001 * y ** 3)
+    gx = 1.7 + 0.1 * x - 0.11 * y + 0.012 * x * x - 0.006 * x * y + 0.002 * y * y
+    gy = -0.9 - 0.11 * x + 0.14 * y - 0.003 * x * x + 0.004 * x * y - 0.003 * y * y
+    return f, gx, gy
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_oracle_reproduces_polynomials_of_element_degree(order):
+    m = structured_mesh(order, 5, 4, 10.0, 6.0)
+    it = Interpolator(m)
+    f, _, _ = _poly(order, m.nodes[:, 0], m.nodes[:, 1])
+    rng = np.random.default_rng(order)
+    for x, y in zip(rng.uniform(0, 10, 40), rng.uniform(0, 6, 40)):
+        v, gx, gy, e = it.evaluate(x, y, f, gradient=True)
+        ev, egx, egy = _poly(order, x, y)
+        assert e >= 0
+        assert abs(v - ev) < 1e-11
+        assert abs(gx - egx) < 1e-10 and abs(gy - egy) < 1e-10
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_oracle_reproduces_nodal_values(order):
+    m = structured_mesh(order, 3, 2, 3.0, 2.0)
+    it = Interpolator(m)
+    f = np.random.default_rng(0).standard_normal(m.num_nodes)
+    for n in range(m.num_nodes):
+        v, _, _, e = it.evaluate(m.nodes[n, 0], m.nodes[n, 1], f)
+        assert e >= 0 and abs(v - f[n]) < 1e-12
+
+
+def test_oracle_first_element_wins_on_shared_edges():
+    m = structured_mesh(1, 3, 2, 3.0, 2.0)   # unit cells
+    it = Interpolator(m)
+    # on the diagonal of cell (1, 0): both triangles of the cell, t = 0 first
+    assert it.find_element(1.5, 0.5) == 2 * (0 * 3 + 1) + 0
+    # on the vertical line x = 1 inside row 0: cell 0's t = 1 precedes cell 1
+    assert it.find_element(1.0, 0.25) == 2 * (0 * 3 + 0) + 1
+    # on the horizontal line y = 1: row 0's t = 1 precedes row 1
+    assert it.find_element(2.25, 1.0) == 2 * (0 * 3 + 2) + 1
+    # interior vertex (1, 1): the first of its six triangles
+    assert it.find_element(1.0, 1.0) == 1
+    assert it.find_element(-0.5, 0.5) == -1
+
+
+def test_oracle_outside_points_take_nearest_node_and_its_estimate():
+    m = structured_mesh(1, 1, 1, 1.0, 1.0)   # nodes (0,0) (1,0) (0,1) (1,1)
+    it = Interpolator(m)
+    f = np.array([1.0, 3.0, 2.0, 7.0])
+    v, gx, gy, e = it.evaluate(-0.3, -0.2, f, gradient=True)
+    assert e == -1 and v == 1.0
+    # node 0 lies in element 0 only: neighbours 1 at (1, 0) and 2 at (0, 1),
+    # each at distance 1: grad = ((3-1) (1,0) + (2-1) (0,1)) / 2
+    assert (gx, gy) == (1.0, 0.5)
+    # node 3 at (1, 1) lies in element 1 (nodes 1, 3, 2): neighbours 1 and 2
+    v, gx, gy, _ = it.evaluate(1.4, 1.1, f, gradient=True)
+    assert v == 7.0
+    assert gx == pytest.approx(((3 - 7) * 0 + (2 - 7) * -1) / 2)
+    assert gy == pytest.approx(((3 - 7) * -1 + (2 - 7) * 0) / 2)
+    # ties go to the first node; zero mode and non-finite points give 0
+    assert it.evaluate(0.5, -1.0, f)[0] == 1.0
+    assert it.evaluate(-0.3, -0.2, f, zero_outside=True)[:3] == (0.0, 0.0, 0.0)
+    assert it.evaluate(float("nan"), 0.5, f)[0] == 0.0
+    assert it.evaluate(1e200, 0.5, f)[0] == 0.0
+
+
+def test_oracle_barycentric_formula():
+    lam = barycentric(0.25, 0.5, [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0)])
+    assert np.allclose(lam, [0.25, 0.25, 0.5])
+
+
+def test_interpolate_entry_point_rejects_bad_arguments_without_gpu():
+    """Argument checks of qd_fe_interpolate return before any device work."""
+    from qdsim_b200 import _native as N
+    L = N.lib()
+    p = C.c_void_p(256)   # never dereferenced: every call below is rejected or empty
+
+    def call(order=1, nx=4, ny=3, Lx=1.0, Ly=1.0, nfield=1, stride=20, npts=5, field=p,
+             gx=None, gy=None, outside=0):
+        return L.qd_fe_interpolate(order, nx, ny, Lx, Ly, nfield, stride, field, npts, p, p, p,
+                                   gx, gy, None, outside, None)
+
+    assert call(order=0) == N.QD_ERR_INVALID
+    assert call(order=4) == N.QD_ERR_INVALID
+    assert call(nx=0) == N.QD_ERR_INVALID
+    assert call(Lx=0.0) == N.QD_ERR_INVALID
+    assert call(Ly=float("nan")) == N.QD_ERR_INVALID
+    assert call(Lx=float("inf")) == N.QD_ERR_INVALID
+    assert call(nfield=0) == N.QD_ERR_INVALID
+    assert call(stride=19) == N.QD_ERR_INVALID           # (4+1)(3+1) = 20 nodes
+    assert call(order=2, stride=20) == N.QD_ERR_INVALID  # 9 x 7 = 63 nodes
+    assert call(gx=p) == N.QD_ERR_INVALID                 # one gradient pointer
+    assert call(outside=2) == N.QD_ERR_INVALID
+    assert call(field=None) == N.QD_ERR_INVALID
+    assert call(npts=-1) == N.QD_ERR_INVALID
+    assert call(nx=60000, ny=60000, stride=1 << 40) == N.QD_ERR_LIMIT
+    assert call(npts=0) == N.QD_OK                        # nothing to do
+
+
+def test_frontend_interpolator_host_logic():
+    from qdsim_b200 import frontend as F
+    inside, lam = F.FEInterpolator.compute_barycentric_coordinates(
+        0.25, 0.5, [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0)])
+    assert inside and np.allclose(lam, [0.25, 0.25, 0.5])
+    inside, _ = F.FEInterpolator.compute_barycentric_coordinates(
+        1.0, 1.0, [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0)])
+    assert not inside
+    mesh = F.Mesh(10e-9, 6e-9, 5, 3, 1)
+    fem = F.FEMSolver(mesh, lambda x, y: 0.067 * 9.109e-31, lambda x, y: 0.0,
+                      lambda x, y: 0.0, device="cpu")
+    with pytest.raises(ValueError):
+        fem.set_potential_values(np.zeros(5))
+    fem.set_potential_values(np.ones(mesh.get_num_nodes()))
+    fem.use_interpolated_potential(True)
+    assert fem._use_interp
