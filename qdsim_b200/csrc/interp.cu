@@ -41,6 +41,7 @@ constexpr int kMaxLinked = 64;
 struct Geo {
   int nx, ny, NX, NY;
   double hx, hy;    // cell size
+  double ihx, ihy;  // their reciprocals
   double hxl, hyl;  // lattice spacing
   double margin;    // interior depth that rules out every other triangle
 };
@@ -252,6 +253,36 @@ __host__ __device__ __noinline__ void node_gradient(const Geo &g, int node, int 
   }
 }
 
+struct Hit {
+  int element, ci, cj, t;
+  double l0, l1, l2;
+};
+
+// The triangles of the 3 x 3 cells around (ci0, cj0) in element order: the
+// first whose barycentric coordinates (signed-area formula) are all >= -1e-10,
+// with its cell, t and coordinates; element -1 when there is none.
+template <int P>
+__host__ __device__ __forceinline__ Hit scan_cells(const Geo &g, double x, double y, int ci0,
+                                                int cj0) {
+  Hit h{-1, 0, 0, 0, 0.0, 0.0, 0.0};
+  for (int cj = max(cj0 - 1, 0); cj <= min(cj0 + 1, g.ny - 1); ++cj)
+    for (int ci = max(ci0 - 1, 0); ci <= min(ci0 + 1, g.nx - 1); ++ci)
+      for (int t = 0; t < 2; ++t) {
+        int cx[3], cy[3];
+        double vx[3], vy[3], l[3];
+        tri_corners(ci, cj, t, cx, cy);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          vx[m] = double(P * cx[m]) * g.hxl;
+          vy[m] = double(P * cy[m]) * g.hyl;
+        }
+        bary(vx, vy, x, y, l);
+        if (l[0] >= -kInsideEps && l[1] >= -kInsideEps && l[2] >= -kInsideEps)
+          return Hit{2 * (cj * g.nx + ci) + t, ci, cj, t, l[0], l[1], l[2]};
+      }
+  return h;
+}
+
 // Value (and gradient) of every field and the containing element at point i.
 template <int P, bool GRAD>
 __host__ __device__ __forceinline__ void interp_point(
@@ -260,46 +291,47 @@ __host__ __device__ __forceinline__ void interp_point(
     double *__restrict__ gy, int32_t *__restrict__ elem, int outside_zero) {
   constexpr int K = Local<P>::K;
   int found = -1, fcx[3], fcy[3];
-  double l[3], vx[3], vy[3];
+  double l[3];
   // Fast path: the triangle of the point's own cell.  A point that lies
   // deeper than g.margin inside it (every barycentric coordinate at least
   // g.margin) is farther from every other triangle than their -1e-10
   // acceptance band reaches, so this is the only element the scan finds.
-  const double qx = x / g.hx, qy = y / g.hy;
-  const int ci0 = clamp_cell(qx, g.nx - 1), cj0 = clamp_cell(qy, g.ny - 1);
+  // Its barycentric coordinates come from cell-local coordinates measured
+  // from the cell's corner, (x - X0) / hx and (y - Y0) / hy, which equal the
+  // signed-area formula's up to rounding and carry no cancellation of
+  // coordinate-sized terms.
+  const int ci0 = clamp_cell(x * g.ihx, g.nx - 1), cj0 = clamp_cell(y * g.ihy, g.ny - 1);
+  int t = 0;
   {
-    const int t = (qx - ci0) + (qy - cj0) > 1.0 ? 1 : 0;
-    tri_corners(ci0, cj0, t, fcx, fcy);
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      vx[m] = double(P * fcx[m]) * g.hxl;
-      vy[m] = double(P * fcy[m]) * g.hyl;
+    const double u = (x - double(P * ci0) * g.hxl) * g.ihx;
+    const double w = (y - double(P * cj0) * g.hyl) * g.ihy;
+    t = u + w > 1.0 ? 1 : 0;
+    if (t == 0) {
+      l[0] = 1.0 - u - w;
+      l[1] = u;
+      l[2] = w;
+    } else {
+      l[0] = 1.0 - w;
+      l[1] = u + w - 1.0;
+      l[2] = 1.0 - u;
     }
-    bary(vx, vy, x, y, l);
-    if (l[0] >= g.margin && l[1] >= g.margin && l[2] >= g.margin)
+    if (l[0] >= g.margin && l[1] >= g.margin && l[2] >= g.margin) {
       found = 2 * (cj0 * g.nx + ci0) + t;
+      tri_corners(ci0, cj0, t, fcx, fcy);
+    }
   }
   // Otherwise the ordered scan of the 3 x 3 cells around it.
-  for (int cj = max(cj0 - 1, 0); cj <= min(cj0 + 1, g.ny - 1) && found < 0; ++cj)
-    for (int ci = max(ci0 - 1, 0); ci <= min(ci0 + 1, g.nx - 1) && found < 0; ++ci)
-      for (int t = 0; t < 2 && found < 0; ++t) {
-        int cx[3], cy[3];
-        tri_corners(ci, cj, t, cx, cy);
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          vx[m] = double(P * cx[m]) * g.hxl;
-          vy[m] = double(P * cy[m]) * g.hyl;
-        }
-        bary(vx, vy, x, y, l);
-        if (l[0] >= -kInsideEps && l[1] >= -kInsideEps && l[2] >= -kInsideEps) {
-          found = 2 * (cj * g.nx + ci) + t;
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            fcx[m] = cx[m];
-            fcy[m] = cy[m];
-          }
-        }
-      }
+  if (found < 0) {
+    const Hit h = scan_cells<P>(g, x, y, ci0, cj0);
+    found = h.element;
+    if (found >= 0) {
+      t = h.t;
+      l[0] = h.l0;
+      l[1] = h.l1;
+      l[2] = h.l2;
+      tri_corners(h.ci, h.cj, t, fcx, fcy);
+    }
+  }
   if (elem) elem[i] = found;
   if (found >= 0) {
     double phi[K], dphi[K][3];
@@ -307,16 +339,19 @@ __host__ __device__ __forceinline__ void interp_point(
     int nodes[K];
 #pragma unroll
     for (int a = 0; a < K; ++a) nodes[a] = local_node<P>(g, fcx, fcy, a);
-    // gradients of the barycentric coordinates (fe_interpolator.cpp:542-566)
+    // gradients of the barycentric coordinates (fe_interpolator.cpp:542-566):
+    // every triangle is one of the two right triangles of a cell, so they are
+    // +-1/hx and +-1/hy
     double glx[3] = {0, 0, 0}, gly[3] = {0, 0, 0};
     if (GRAD) {
-      const double area =
-          0.5 * ((vx[1] - vx[0]) * (vy[2] - vy[0]) - (vx[2] - vx[0]) * (vy[1] - vy[0]));
-#pragma unroll
-      for (int m = 0; m < 3; ++m) {
-        const int j = (m + 1) % 3, k = (m + 2) % 3;
-        glx[m] = 0.5 * (vy[j] - vy[k]) / area;
-        gly[m] = 0.5 * (vx[k] - vx[j]) / area;
+      if (t == 0) {
+        glx[0] = -g.ihx; gly[0] = -g.ihy;
+        glx[1] = g.ihx;
+        gly[2] = g.ihy;
+      } else {
+        gly[0] = -g.ihy;
+        glx[1] = g.ihx; gly[1] = g.ihy;
+        glx[2] = -g.ihx;
       }
     }
     for (int f = 0; f < nfield; ++f) {
@@ -353,7 +388,7 @@ __host__ __device__ __forceinline__ void interp_point(
 }
 
 template <int P, bool GRAD>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, GRAD ? 2 : 3)
 interp_kernel(Geo g, int nfield, int64_t fstride, const double *__restrict__ field, int64_t npts,
               const double *__restrict__ px, const double *__restrict__ py,
               double *__restrict__ val, double *__restrict__ gx, double *__restrict__ gy,
@@ -373,6 +408,8 @@ Geo make_geo(int order, int32_t nx, int32_t ny, double Lx, double Ly) {
   g.NY = order * ny + 1;
   g.hx = Lx / nx;
   g.hy = Ly / ny;
+  g.ihx = 1.0 / g.hx;
+  g.ihy = 1.0 / g.hy;
   g.hxl = Lx / double(int64_t(order) * nx);
   g.hyl = Ly / double(int64_t(order) * ny);
   // Triangle T' accepts points within 1e-10 of its heights outside it; near
@@ -390,18 +427,39 @@ Geo make_geo(int order, int32_t nx, int32_t ny, double Lx, double Ly) {
   return g;
 }
 
+// One wave of resident blocks (grid-stride over the points).
+template <int P, bool GRAD>
+unsigned resident_blocks() {
+  static int blocks = 0;
+  if (blocks == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, interp_kernel<P, GRAD>, kThreads,
+                                                      0) != cudaSuccess ||
+        sms <= 0 || per_sm <= 0)
+      return 148u * 4u;
+    blocks = sms * per_sm;
+  }
+  return unsigned(blocks);
+}
+
 template <int P>
 int launch(const Geo &g, int nfield, int64_t fstride, const double *field, int64_t npts,
            const double *x, const double *y, double *val, double *gx, double *gy, int32_t *elem,
            int outside_zero, cudaStream_t s) {
   const int64_t want = (npts + kThreads - 1) / kThreads;
-  const unsigned blocks = unsigned(want < 148 * 16 ? want : 148 * 16);
-  if (gx)
+  if (gx) {
+    const unsigned cap = resident_blocks<P, true>();
+    const unsigned blocks = unsigned(want < cap ? want : cap);
     interp_kernel<P, true><<<blocks, kThreads, 0, s>>>(g, nfield, fstride, field, npts, x, y, val,
                                                        gx, gy, elem, outside_zero);
-  else
+  } else {
+    const unsigned cap = resident_blocks<P, false>();
+    const unsigned blocks = unsigned(want < cap ? want : cap);
     interp_kernel<P, false><<<blocks, kThreads, 0, s>>>(g, nfield, fstride, field, npts, x, y,
                                                         val, nullptr, nullptr, elem, outside_zero);
+  }
   QD_CHECK_LAUNCH();
   return QD_OK;
 }

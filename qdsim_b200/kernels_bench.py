@@ -2,7 +2,7 @@
 
     python -m qdsim_b200.kernels_bench cap_spmm [--prec fp64|fp32] [--b 48] [--launches 10]
     python -m qdsim_b200.kernels_bench pcg [--iters 32]
-    python -m qdsim_b200.kernels_bench interp [--points 16777216] [--gradient] [--launches 10]
+    python -m qdsim_b200.kernels_bench interp [--points 16777216] [--gradient] [--sorted]
 
 ``cap_spmm``: ``qd_cap_spmm`` on the open-system pencil of P2 400x200 cells on
 200x100 nm (318,801 DOFs, 3.65M nonzeros) for a block of b complex columns;
@@ -11,9 +11,10 @@ of the p-n junction's Poisson step (P1 300x100 cells, 30,401 nodes, 64
 right-hand sides) for a fixed number of iterations; prints ms per iteration.
 ``interp``: ``qd_fe_interpolate`` of one nodal field of the P2 400x200-cell
 mesh on 200x100 nm at uniformly random points (values, optionally gradients
-and elements); prints ms per launch and GB/s of algorithmic bytes (16 B of
-coordinates in, 8 B per value out, 20 B more with gradients and elements, the
-field read once).
+and elements), in random order or sorted by cell (``--sorted``, the order of
+a resampling onto another mesh's nodes); prints ms per launch and GB/s of
+algorithmic bytes (16 B of coordinates in, 8 B per value out, 20 B more with
+gradients and elements, the field read once).
 The launch sequence is fixed, so a profiler can select launches by index.
 """
 from __future__ import annotations
@@ -78,7 +79,7 @@ def pcg(iters: int, dev):
             "algorithmic_bytes_per_iteration": int(alg), "GBps": alg / (ms * 1e-3) / 1e9}
 
 
-def interp(points: int, gradient: bool, launches: int, dev):
+def interp(points: int, gradient: bool, ordered: bool, launches: int, dev):
     from .interp import FieldInterpolator
     from .mesh import StructuredMesh
     m = StructuredMesh(2, 400, 200, 200.0, 100.0)
@@ -86,6 +87,12 @@ def interp(points: int, gradient: bool, launches: int, dev):
     x = torch.rand(points, generator=g, device=dev, dtype=torch.float64) * m.Lx
     y = torch.rand(points, generator=g, device=dev, dtype=torch.float64) * m.Ly
     f = torch.randn(m.num_nodes, generator=g, device=dev, dtype=torch.float64)
+    if ordered:
+        key = (y * (m.ny / m.Ly)).long().clamp(max=m.ny - 1) * m.nx + \
+            (x * (m.nx / m.Lx)).long().clamp(max=m.nx - 1)
+        order = torch.argsort(key)
+        x, y = x[order].contiguous(), y[order].contiguous()
+        del key, order
     fi = FieldInterpolator(m, device=dev)
     fi.evaluate(x, y, f, gradient=gradient, element=gradient)   # launch 0 (warm-up)
     torch.cuda.synchronize()
@@ -98,7 +105,7 @@ def interp(points: int, gradient: bool, launches: int, dev):
     ms = e0.elapsed_time(e1) / launches
     alg = points * (16 + 8 + (20 if gradient else 0)) + m.num_nodes * 8
     return {"kernel": "interp_kernel", "order": 2, "nodes": int(m.num_nodes), "points": points,
-            "gradient": gradient, "ms_per_launch": ms, "algorithmic_bytes": int(alg),
+            "gradient": gradient, "sorted": ordered, "ms_per_launch": ms, "algorithmic_bytes": int(alg),
             "GBps": alg / (ms * 1e-3) / 1e9, "Gpoints_per_s": points / (ms * 1e-3) / 1e9}
 
 
@@ -111,6 +118,7 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=32)
     ap.add_argument("--points", type=int, default=1 << 24)
     ap.add_argument("--gradient", action="store_true")
+    ap.add_argument("--sorted", action="store_true")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("a CUDA device is required")
@@ -120,7 +128,7 @@ def main(argv=None):
     elif a.case == "pcg":
         r = pcg(a.iters, dev)
     else:
-        r = interp(a.points, a.gradient, a.launches, dev)
+        r = interp(a.points, a.gradient, a.sorted, a.launches, dev)
     print(json.dumps(r))
 
 
