@@ -32,7 +32,7 @@
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 constexpr double kInsideEps = 1e-10;
 // unique neighbours of a node over the elements that contain it: at most
 // 6 triangles x 9 other nodes for P3
@@ -388,15 +388,32 @@ __host__ __device__ __forceinline__ void interp_point(
 }
 
 template <int P, bool GRAD>
-__global__ void __launch_bounds__(kThreads, GRAD ? 2 : 3)
+__global__ void __launch_bounds__(kThreads, GRAD ? 4 : 5)
 interp_kernel(Geo g, int nfield, int64_t fstride, const double *__restrict__ field, int64_t npts,
               const double *__restrict__ px, const double *__restrict__ py,
               double *__restrict__ val, double *__restrict__ gx, double *__restrict__ gy,
               int32_t *__restrict__ elem, int outside_zero) {
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npts;
-       i += int64_t(gridDim.x) * blockDim.x)
-    interp_point<P, GRAD>(g, nfield, fstride, field, npts, i, px[i], py[i], val, gx, gy, elem,
+  // the next point's coordinates are loaded before this point's gathers, so
+  // the two dependent memory round trips of consecutive points overlap
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double x = 0.0, y = 0.0;
+  if (i < npts) {
+    x = px[i];
+    y = py[i];
+  }
+  for (; i < npts; i += stride) {
+    const int64_t j = i + stride;
+    double xn = 0.0, yn = 0.0;
+    if (j < npts) {
+      xn = px[j];
+      yn = py[j];
+    }
+    interp_point<P, GRAD>(g, nfield, fstride, field, npts, i, x, y, val, gx, gy, elem,
                           outside_zero);
+    x = xn;
+    y = yn;
+  }
 }
 
 // Mesh geometry of the launch (arguments already checked).
