@@ -27,6 +27,10 @@ Semantics kept from the C++ classes (SI units in and out):
    (``qd_fe_interpolate``): the reference's element scan becomes an O(1)
    cell lookup with the same containing element, and points outside the mesh
    take the nearest node's value and the reference's gradient estimate.
+ - ``potential``, ``effective_mass``, ``epsilon_r`` and ``cap`` are the
+   callbacks of backend/src/physics.cpp the frontend hands to ``FEMSolver``;
+   ``potential`` resamples the electrostatic potential through the
+   ``FEInterpolator`` (one launch for all nodes when given arrays).
 Internally the mesh is scaled to nm and energies to eV (c = hbar^2/(2 m*) in
 eV nm^2), as the other drop-in solvers do; eigenvalues come back in J and
 eigenvectors are M-normalised in m^2.
@@ -224,6 +228,87 @@ class FEInterpolator:
         return (all(v >= -1e-10 for v in lam), lam)
 
 
+# the elementary charge and the potential cap of backend/src/physics.cpp:69-141
+_PHYS_Q = 1.602e-19
+_MAX_POTENTIAL_EV = 100.0
+
+
+def _field(mat, name):
+    """A material property from a Material-like object or a mapping."""
+    if isinstance(mat, dict):
+        return float(mat[name])
+    return float(getattr(mat, name))
+
+
+def _out(v, scalar):
+    return float(v) if scalar else v
+
+
+def effective_mass(x, y, qd_mat, matrix_mat, R):
+    """m_e of the dot inside the disc x^2 + y^2 <= R^2, of the matrix outside
+    (physics.cpp:39-43); arrays are evaluated elementwise."""
+    xa, ya = np.asarray(x, dtype=float), np.asarray(y, dtype=float)
+    v = np.where(xa * xa + ya * ya <= R * R, _field(qd_mat, "m_e"), _field(matrix_mat, "m_e"))
+    return _out(v, xa.ndim == 0)
+
+
+def epsilon_r(x, y, p_mat, n_mat):
+    """p-side permittivity for x < 0, n-side otherwise (physics.cpp:143-147)."""
+    xa = np.asarray(x, dtype=float)
+    v = np.where(xa < 0, _field(p_mat, "epsilon_r"), _field(n_mat, "epsilon_r"))
+    return _out(v, xa.ndim == 0)
+
+
+def cap(x, y, eta, Lx, Ly, d):
+    """Absorbing-potential amplitude, quadratic in the distance past
+    |x| = Lx/2 - d or |y| = Ly/2 - d, the larger of the two
+    (physics.cpp:244-254)."""
+    xa, ya = np.abs(np.asarray(x, dtype=float)), np.abs(np.asarray(y, dtype=float))
+    ex = np.where(xa > Lx / 2 - d, eta * ((xa - Lx / 2) / d) ** 2, 0.0)
+    ey = np.where(ya > Ly / 2 - d, eta * ((ya - Ly / 2) / d) ** 2, 0.0)
+    return _out(np.maximum(ex, ey), xa.ndim == 0)
+
+
+def potential(x, y, qd_mat, matrix_mat, R, type, phi, interpolator=None):
+    """Dot potential plus the electrostatic potential phi resampled at (x, y)
+    (physics.cpp:69-141), in J.  The dot term is -min(Delta_E_c, 100 eV)
+    inside the disc ("square") or as a Gaussian of width R ("gaussian"); the
+    electrostatic term is the finite-element interpolation of the nodal phi
+    (volts, read as eV), clipped to +-100, or phi[0] clipped when there is no
+    interpolator.  With a ``FEInterpolator`` of this module, arrays of points
+    are resampled in one GPU launch."""
+    xa, ya = np.asarray(x, dtype=float), np.asarray(y, dtype=float)
+    scalar = xa.ndim == 0
+    xa, ya = np.atleast_1d(xa), np.atleast_1d(ya)
+    depth = min(_field(qd_mat, "Delta_E_c"), _MAX_POTENTIAL_EV)
+    r2 = xa * xa + ya * ya
+    if type == "square":
+        v_qd = np.where(r2 <= R * R, -depth, 0.0)
+    elif type == "gaussian":
+        v_qd = -depth * np.exp(-r2 / (2 * R * R))
+    else:
+        v_qd = np.zeros_like(xa)
+    ph = np.asarray(phi, dtype=float).reshape(-1)
+    v_el = np.zeros_like(xa)
+    first = (min(abs(ph[0]), _MAX_POTENTIAL_EV) * (1.0 if ph[0] >= 0 else -1.0)
+             if ph.size else 0.0)
+    if ph.size and interpolator is not None:
+        try:
+            if isinstance(interpolator, FEInterpolator):
+                v_el = np.asarray(interpolator.interpolate_vector(xa, ya, ph), dtype=float)
+            else:
+                v_el = np.array([interpolator.interpolate(a, b, ph) for a, b in zip(xa, ya)],
+                                dtype=float)
+            v_el = np.where(np.abs(v_el) > _MAX_POTENTIAL_EV,
+                            np.where(v_el >= 0, _MAX_POTENTIAL_EV, -_MAX_POTENTIAL_EV), v_el)
+        except Exception:
+            v_el = np.full_like(xa, first)
+    elif ph.size:
+        v_el = np.full_like(xa, first)
+    v = v_qd * _PHYS_Q + v_el * _PHYS_Q
+    return float(v[0]) if scalar else v
+
+
 class EigenSolver:
     """The k lowest levels of a ``FEMSolver``'s Hermitian pencil (K + V, M)."""
 
@@ -260,4 +345,5 @@ class EigenSolver:
         return [v.copy() for v in self.eigenvectors]
 
 
-__all__ = ["Mesh", "FEMSolver", "EigenSolver", "FEInterpolator"]
+__all__ = ["Mesh", "FEMSolver", "EigenSolver", "FEInterpolator", "potential",
+           "effective_mass", "epsilon_r", "cap"]

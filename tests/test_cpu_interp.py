@@ -140,3 +140,50 @@ def test_frontend_interpolator_host_logic():
     fem.set_potential_values(np.ones(mesh.get_num_nodes()))
     fem.use_interpolated_potential(True)
     assert fem._use_interp
+
+
+def test_frontend_physics_callbacks():
+    """The reference's physics callbacks (backend/src/physics.cpp) on scalars
+    and arrays; the electrostatic part of ``potential`` through a stand-in
+    interpolator (its GPU evaluation is covered by the GPU tests of
+    FEInterpolator)."""
+    from qdsim_b200 import frontend as F
+    q = 1.602e-19
+    dot, host = {"m_e": 0.041, "Delta_E_c": 0.3}, {"m_e": 0.067, "Delta_E_c": 0.0}
+    assert F.effective_mass(0.5, 0.5, dot, host, 1.0) == 0.041
+    assert F.effective_mass(1.0, 0.5, dot, host, 1.0) == 0.067
+    np.testing.assert_array_equal(F.effective_mass(np.array([0.0, 2.0]), np.zeros(2), dot, host,
+                                                   1.0), [0.041, 0.067])
+    assert F.epsilon_r(-1.0, 0.0, {"epsilon_r": 12.9}, {"epsilon_r": 13.1}) == 12.9
+    assert F.epsilon_r(0.0, 0.0, {"epsilon_r": 12.9}, {"epsilon_r": 13.1}) == 13.1
+    # quadratic in (|x| - Lx/2) / d past |x| = Lx/2 - d, the larger of x and y
+    assert F.cap(3.0, 0.0, 2.0, 10.0, 10.0, 1.0) == 0.0
+    assert F.cap(4.5, 0.0, 2.0, 10.0, 10.0, 1.0) == pytest.approx(2.0 * 0.25)
+    assert F.cap(4.5, 4.8, 2.0, 10.0, 10.0, 1.0) == pytest.approx(2.0 * 0.25)
+    # dot term alone
+    assert F.potential(0.0, 0.0, dot, host, 1.0, "square", []) == pytest.approx(-0.3 * q)
+    assert F.potential(2.0, 0.0, dot, host, 1.0, "square", []) == 0.0
+    assert F.potential(1.0, 0.0, dot, host, 1.0, "gaussian", []) == pytest.approx(
+        -0.3 * np.exp(-0.5) * q)
+    deep = {"Delta_E_c": 500.0}
+    assert F.potential(0.0, 0.0, deep, host, 1.0, "square", []) == pytest.approx(-100.0 * q)
+    # no interpolator: phi[0] clipped to +-100
+    assert F.potential(5.0, 0.0, dot, host, 1.0, "square", [250.0, 1.0]) == pytest.approx(100 * q)
+    assert F.potential(5.0, 0.0, dot, host, 1.0, "square", [-0.2]) == pytest.approx(-0.2 * q)
+
+    class Stand:
+        def interpolate(self, x, y, field):
+            return field[0] * x + 300.0 * (y > 10)
+
+    x = np.array([0.0, 0.5, 3.0, 3.0])
+    y = np.array([0.0, 0.0, 0.0, 20.0])
+    v = F.potential(x, y, dot, host, 1.0, "square", [0.1, 9.0], Stand())
+    want = (np.array([-0.3, -0.3, 0.0, 0.0]) + np.array([0.0, 0.05, 0.3, 100.0])) * q
+    np.testing.assert_allclose(v, want, rtol=1e-12)
+
+    class Broken:
+        def interpolate(self, x, y, field):
+            raise RuntimeError("no element")
+
+    assert F.potential(3.0, 0.0, dot, host, 1.0, "square", [-0.25], Broken()) == \
+        pytest.approx(-0.25 * q)
