@@ -169,13 +169,16 @@ class FEMSolver:
 class FEInterpolator:
     """Field evaluation on a ``Mesh`` (backend/src/fe_interpolator.cpp) with the
     reference's method names; coordinates are in the mesh's units.  Every
-    evaluation is one ``qd_fe_interpolate`` launch; the ``*_vector`` /
-    ``*_points`` forms take whole arrays of points in one launch."""
+    evaluation is one ``qd_fe_interpolate`` launch, and a host field is
+    copied to the device on each call: the per-point methods suit a few
+    points, while ``interpolate_vector`` / ``interpolate_points`` take whole
+    arrays of points (and device fields) in one launch."""
 
     def __init__(self, mesh: Mesh, device="cuda"):
         self.mesh = mesh
         self._fi = FieldInterpolator(mesh._si, device=device)
         self._fz = FieldInterpolator(mesh._si, device=device, outside="zero")
+        self._zeros = None
 
     def _one(self, x, y, field, gradient=False, element=False):
         return self._fi.evaluate([float(x)], [float(y)], field, gradient=gradient,
@@ -193,8 +196,11 @@ class FEInterpolator:
         return (gx, gy)
 
     def find_element(self, x, y) -> int:
-        field = torch.zeros(self.mesh.get_num_nodes(), dtype=torch.float64)
-        return int(self._fz.evaluate([float(x)], [float(y)], field, element=True)["element"][0])
+        if self._zeros is None:
+            self._zeros = torch.zeros(self.mesh.get_num_nodes(), dtype=torch.float64,
+                                      device=self._fz.device)
+        r = self._fz.evaluate([float(x)], [float(y)], self._zeros, element=True)
+        return int(r["element"][0])
 
     find_containing_element = find_element
 
