@@ -21,10 +21,13 @@ search:
   (``backend/src/gpu_kernels.cu:352-423``) does.
 
 Parity pin: ``fe_interpolator.cpp`` needs Eigen, which this image lacks, so
-the reference cannot be compiled here; the restatement is pinned by known
-answers instead (nodal values reproduced, polynomials of the element degree
-reproduced with their gradients, hand-computed outside-point estimates) in
-``tests/test_cpu_interp.py``.
+it cannot be compiled here.  The restatement is pinned (``tests/test_cpu_interp.py``)
+against golden vectors of the reference's own Python P1 interpolator
+(``frontend/qdsim/fe_interpolator.py``; ``tests/golden/make_interp_golden.py``)
+for interior values, gradients and elements and for outside-point values, and
+by known answers for P2/P3 and the C++-only rules: nodal values reproduced,
+polynomials of the element degree reproduced with their gradients, the first
+element winning on shared edges, hand-computed outside-point estimates.
 
 Mesh: ``oracle.fem.structured_mesh`` (lattice node order; P1 identical to
 ``backend/src/mesh.cpp:66-92``).

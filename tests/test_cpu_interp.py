@@ -1,13 +1,14 @@
 """Finite-element field interpolation without a GPU: the oracle pinned by known
 answers, the C entry point's argument checks and the frontend's host logic.
 
-The reference's FEInterpolator (backend/src/fe_interpolator.cpp) needs Eigen,
-which this image lacks, so its outputs cannot be generated here; the oracle is
-pinned instead by properties any correct implementation of that file has:
-nodal values are reproduced, polynomials of the element degree are reproduced
-with their gradients, the first element in index order wins on shared edges,
-and outside points follow the nearest-node rule and its gradient estimate,
-computed here by hand.
+The reference's C++ FEInterpolator (backend/src/fe_interpolator.cpp) needs
+Eigen, which this image lacks.  The oracle is pinned by golden vectors of the
+reference's own Python P1 interpolator (tests/golden/interp_p1.npz) and by
+properties any correct implementation of the C++ file has: nodal values are
+reproduced, polynomials of the element degree are reproduced with their
+gradients, the first element in index order wins on shared edges, and outside
+points follow the nearest-node rule and its gradient estimate, computed here
+by hand.
 """
 import ctypes as C
 
@@ -89,6 +90,35 @@ def test_oracle_outside_points_take_nearest_node_and_its_estimate():
     assert it.evaluate(-0.3, -0.2, f, zero_outside=True)[:3] == (0.0, 0.0, 0.0)
     assert it.evaluate(float("nan"), 0.5, f)[0] == 0.0
     assert it.evaluate(1e200, 0.5, f)[0] == 0.0
+
+
+def test_oracle_matches_reference_python_interpolator_golden():
+    """The reference's own P1 interpolator (frontend/qdsim/fe_interpolator.py
+    with its quadtree), run by tests/golden/make_interp_golden.py: values,
+    gradients and elements at points strictly inside one element, and the
+    nearest-node values of points outside the mesh, except at the interior
+    points its quadtree misses (recorded in the fixture)."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "interp_p1.npz"))
+    m = structured_mesh(1, int(d["nx"]), int(d["ny"]), float(d["Lx"]), float(d["Ly"]))
+    it = Interpolator(m)
+    n_in = int(d["n_inside"])
+    val, gx, gy, el = it.evaluate_many(d["x"], d["y"], d["field"], gradient=True)
+    ok = ~d["quadtree_miss"]
+    ok_in = ok[:n_in]
+    np.testing.assert_array_equal(el[ok], d["element"][ok])
+    np.testing.assert_allclose(val[0][ok], d["value"][ok], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(gx[0, :n_in][ok_in], d["grad_x"][ok_in], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(gy[0, :n_in][ok_in], d["grad_y"][ok_in], rtol=0, atol=1e-12)
+    assert (el[:n_in] >= 0).all() and (el[n_in:] < 0).all()
+    assert ok_in.sum() >= 390 and ok[n_in:].all()
+    # a recorded fact about the reference: where its quadtree missed, the
+    # element it returned does not contain the point, and the oracle's does
+    for i in np.flatnonzero(~ok):
+        v = m.nodes[m.elems[d["element"][i], :3]]
+        assert barycentric(d["x"][i], d["y"][i], v).min() < -1e-3
+        v = m.nodes[m.elems[el[i], :3]]
+        assert barycentric(d["x"][i], d["y"][i], v).min() >= -1e-10
 
 
 def test_oracle_barycentric_formula():
