@@ -206,6 +206,84 @@ class SweepPipeline:
         return info
 
 
+# ---------------------------------------------------------------------------
+# Sharding a fixed set of dots (or bias points) over ranks
+# ---------------------------------------------------------------------------
+
+# CSR nonzeros per row of the P1 / P2 / P3 stiffness pattern on the structured
+# mesh (the average over a 60 x 30-cell mesh), the cost model's row weight
+_NNZ_PER_ROW = {1: 6.8, 2: 11.3, 3: 16.8}
+
+
+def dot_cost(dot) -> float:
+    """Predicted solve cost of a dot: its stiffness nonzeros.  With the DST
+    preconditioner the LOBPCG iteration count hardly depends on the grid, so
+    nonzeros x iterations is proportional to the nonzeros."""
+    m = dot.mesh
+    return float(m.num_nodes) * _NNZ_PER_ROW[int(m.order)]
+
+
+def partition_by_cost(costs, parts: int):
+    """Longest-processing-time-first split of items with ``costs`` into
+    ``parts`` groups: items in decreasing cost (ties by index), each to the
+    group with the least load so far (the lowest-numbered on ties).  The
+    heaviest group is within 4/3 of the best possible split.  Returns one
+    sorted index array per group; every rank computes the same split."""
+    costs = np.asarray(costs, dtype=np.float64).reshape(-1)
+    if parts < 1:
+        raise ValueError("parts must be at least 1")
+    if not np.all(np.isfinite(costs)) or (costs < 0).any():
+        raise ValueError("costs must be finite and non-negative")
+    order = np.argsort(-costs, kind="stable")
+    load = np.zeros(parts)
+    groups = [[] for _ in range(parts)]
+    for i in order:
+        g = int(np.argmin(load))
+        groups[g].append(int(i))
+        load[g] += costs[i]
+    return [np.array(sorted(g), dtype=np.int64) for g in groups]
+
+
+def shard_dots(dots, rank: int, world: int):
+    """(indices, dots) of this rank's share of ``dots``, split by
+    ``partition_by_cost`` on ``dot_cost``; the shards are disjoint and cover
+    every dot, and no data moves between ranks during the solves."""
+    if not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    idx = partition_by_cost([dot_cost(d) for d in dots], world)[rank]
+    return idx, [dots[i] for i in idx]
+
+
+def gather_by_index(local, indices, n_items: int, group=None):
+    """Reassemble per-item host results from every rank's shard: ``local``
+    holds this rank's rows for ``indices``; the rows of all ranks are
+    all-gathered (small host objects over the process group) and returned in
+    item order, shape (n_items, ...).  Without an initialised process group
+    the local rows are returned in item order."""
+    local = np.asarray(local)
+    indices = np.asarray(indices, dtype=np.int64)
+    if local.shape[0] != indices.size:
+        raise ValueError("one row of results per index")
+    import torch.distributed as dist
+    parts = [(indices, local)]
+    if dist.is_available() and dist.is_initialized():
+        parts = [None] * dist.get_world_size(group)
+        dist.all_gather_object(parts, (indices, local), group=group)
+    out = None
+    seen = np.zeros(n_items, dtype=bool)
+    for idx, rows in parts:
+        rows = np.asarray(rows)
+        if out is None:
+            out = np.zeros((n_items,) + rows.shape[1:], dtype=rows.dtype)
+        if seen[idx].any():
+            raise ValueError("an item appears in more than one shard")
+        out[idx] = rows
+        seen[idx] = True
+    if not seen.all():
+        raise ValueError("the shards do not cover every item")
+    return out
+
+
 def solve_dots(dots, k, device="cuda", **kw) -> EigResult:
     """Assemble and solve a list of ``workloads.Dot`` on the GPU."""
     hb = HostBatch(dots)
