@@ -254,6 +254,44 @@ def cap_spmm_bytes(n, nnz, b, s):
     return nnz * (4 + 3 * s) + 4 * (n + 1) + 3 * n * b * 2 * s
 
 
+def interp_measurement(dev):
+    """Field interpolation (qd_fe_interpolate): one nodal field of the P2
+    400x200-cell mesh on 200x100 nm (321,201 nodes) at 16.8M uniformly random
+    points, in random order and sorted by cell, values alone and with
+    gradients and elements; CUDA-event time per launch against the HBM peak
+    (algorithmic bytes: 16 B of coordinates in, 8 B per value out, 20 B more
+    with gradients and elements, the field once).  Beside it a size-independent
+    check: a quadratic field is reproduced exactly by the P2 interpolant."""
+    import torch
+    from qdsim_b200 import kernels_bench as KB
+    from qdsim_b200.interp import FieldInterpolator
+    from qdsim_b200.mesh import StructuredMesh
+    peak = FALLBACK_HBM
+    if os.path.exists(PEAKS):
+        with open(PEAKS) as f:
+            peak = float(json.load(f).get("hbm_gbs", FALLBACK_HBM))
+    out = {"workload": "one field of the P2 400x200-cell mesh (321,201 nodes) at 16,777,216 "
+                       "uniformly random points", "points": 1 << 24}
+    for grad in (False, True):
+        for ordered in (False, True):
+            r = KB.interp(1 << 24, grad, ordered, 10, dev)
+            key = ("gradients" if grad else "values") + ("_sorted" if ordered else "_random")
+            out[key] = {"ms": r["ms_per_launch"], "Gpoints_per_s": r["Gpoints_per_s"],
+                        "GBps": r["GBps"], "frac": r["GBps"] / peak}
+    m = StructuredMesh(2, 400, 200, 200.0, 100.0)
+    g = torch.Generator(device=dev).manual_seed(1)
+    x = torch.rand(1 << 22, generator=g, device=dev, dtype=torch.float64) * m.Lx
+    y = torch.rand(1 << 22, generator=g, device=dev, dtype=torch.float64) * m.Ly
+    nd = torch.as_tensor(m.nodes, device=dev)
+
+    def quad(a, b):
+        return 0.3 + 1.7 * a - 0.9 * b + 0.5 * a * a - 1.1 * a * b + 0.7 * b * b
+
+    v = FieldInterpolator(m, device=dev).evaluate(x, y, quad(nd[:, 0] / m.Lx, nd[:, 1] / m.Ly))
+    out["max_err_quadratic_field"] = float((v["value"] - quad(x / m.Lx, y / m.Ly)).abs().max())
+    return out
+
+
 def cap_measurement(dev):
     """Open system (P2 400x200 cells on 200x100 nm, 318,801 DOFs, CAP -i 50 meV
     (d/10 nm)^2): the 20 eigenvalues nearest -0.05 eV, in the mixed form (FP32
@@ -606,6 +644,10 @@ def main():
                 result["cap_open_system"] = cap_measurement(dev)
             except Exception as e:   # recorded; the headline line stands
                 result["cap_open_system"] = {"error": repr(e)}
+            try:
+                result["field_interpolation"] = interp_measurement(dev)
+            except Exception as e:   # recorded; the headline line stands
+                result["field_interpolation"] = {"error": repr(e)}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
