@@ -191,6 +191,24 @@ class FEInterpolator:
         r = self._one(x, y, field, gradient=True)
         return (float(r["value"][0]), float(r["grad_x"][0]), float(r["grad_y"][0]))
 
+    def interpolate_complex(self, x, y, values, component="real"):
+        """A complex nodal field at (x, y), as the Cython wrapper's
+        ``interpolate_complex`` (qdsim_cython/core/interpolator.pyx:107-150):
+        ``"real"`` / ``"imag"`` interpolate that part, ``"abs"`` gives the
+        modulus of the interpolated value.  Both parts are evaluated in one
+        launch (two fields)."""
+        if component not in ("real", "imag", "abs"):
+            raise ValueError(f"Unknown component: {component}")
+        z = np.asarray(values, dtype=np.complex128).reshape(-1)
+        parts = np.stack([z.real, z.imag])
+        v = self._fi.evaluate([float(x)], [float(y)], parts)["value"]
+        re, im = float(v[0, 0]), float(v[1, 0])
+        if component == "real":
+            return re
+        if component == "imag":
+            return im
+        return float(np.hypot(re, im))
+
     def interpolate_gradient(self, x, y, field):
         _, gx, gy = self.interpolate_with_gradient(x, y, field)
         return (gx, gy)

@@ -217,3 +217,33 @@ def test_frontend_physics_callbacks():
 
     assert F.potential(3.0, 0.0, dot, host, 1.0, "square", [-0.25], Broken()) == \
         pytest.approx(-0.25 * q)
+
+
+def test_frontend_complex_interpolation_host_logic():
+    """interpolate_complex splits the field into real and imaginary rows of one
+    evaluation and combines them; the evaluation is replaced by the oracle."""
+    import torch
+    from qdsim_b200 import frontend as F
+    mesh = F.Mesh(12e-9, 8e-9, 6, 4, 2)
+    fi = F.FEInterpolator(mesh, device="cpu")
+    om = structured_mesh(2, 6, 4, 12e-9, 8e-9)
+    it = Interpolator(om)
+    calls = []
+
+    def fake(x, y, field, gradient=False, element=False, stream=None):
+        calls.append(np.asarray(field).shape)
+        v = it.evaluate_many(np.asarray(x), np.asarray(y), field)[0]
+        return {"value": torch.as_tensor(v)}
+
+    fi._fi.evaluate = fake
+    rng = np.random.default_rng(3)
+    z = rng.standard_normal(mesh.get_num_nodes()) + 1j * rng.standard_normal(mesh.get_num_nodes())
+    x, y = 5.3e-9, 2.9e-9
+    re = it.evaluate(x, y, z.real)[0]
+    im = it.evaluate(x, y, z.imag)[0]
+    assert fi.interpolate_complex(x, y, z, "real") == pytest.approx(re, abs=1e-14)
+    assert fi.interpolate_complex(x, y, z, "imag") == pytest.approx(im, abs=1e-14)
+    assert fi.interpolate_complex(x, y, z, "abs") == pytest.approx(abs(re + 1j * im), abs=1e-14)
+    assert calls == [(2, mesh.get_num_nodes())] * 3
+    with pytest.raises(ValueError):
+        fi.interpolate_complex(x, y, z, "phase")
