@@ -321,9 +321,11 @@ int qd_cap_spmm(int32_t n, int b, int vec_fp32, const int32_t *d_rowptr, const i
  * interpolateWithGradient and findElement
  * (backend/src/fe_interpolator.cpp:54-431) and interpolate_field_kernel
  * (backend/src/gpu_kernels.cu:352-423), which scan every element per point;
- * here the point's cell is computed and only the 3 x 3 cells around it are
- * tested, in element order, so the containing element is the one the scan
- * returns (first with all barycentric coordinates >= -1e-10).
+ * here the point's cell is computed: a point well inside its own cell's
+ * triangle is settled by that one test, any other point by testing the
+ * triangles of the 3 x 3 cells around it in element order, so the containing
+ * element is the one the scan returns (the first with all barycentric
+ * coordinates >= -1e-10).
  *   d_field     nfield fields, field f at d_field + f * field_stride
  *               (field_stride >= number of nodes)
  *   d_x, d_y    npts query points
