@@ -287,6 +287,46 @@ def accuracy_report(hb, E, X, Rn, rel, k, n_check=2):
     return out
 
 
+def c1_measurement(dev, repeats=5):
+    """Single dot (P1 100x50 cells on 100x50 nm, seeded Gaussian well, 10
+    lowest levels): one assembly and one eigensolve on the GPU, each timed
+    over ``repeats`` calls after a warm-up, the levels checked against the
+    oracle; beside it the oracle's assembly + shift-invert eigsh on the host."""
+    import torch
+    from oracle import fem as O
+    from qdsim_b200 import eigen as G, fem as F, mesh as Mh
+    om, c, V = O.dot_config_c1(seed=0)
+    t0 = time.perf_counter()
+    ref = O.assemble(om, c, V)
+    E0, _ = O.eig_lowest(ref.H, ref.M, 10, O.sigma_below(V))
+    t_host = time.perf_counter() - t0
+    m = Mh.StructuredMesh(om.order, om.nx, om.ny, om.Lx, om.Ly)
+    prob = F.FEMProblem(m, device=dev)
+    a = prob.assemble(c, V)
+    G.solve_batch([(prob.d_rowptr, prob.d_col, a["H"], a["M"])], 10, b=16,
+                  precision="mixed", tol=1e-9, max_iter=3000)          # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        a = prob.assemble(c, V)
+    torch.cuda.synchronize()
+    t_asm = (time.perf_counter() - t0) / repeats
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        res = G.solve_batch([(prob.d_rowptr, prob.d_col, a["H"], a["M"])], 10, b=16,
+                            precision="mixed", tol=1e-9, max_iter=3000)
+    torch.cuda.synchronize()
+    t_solve = (time.perf_counter() - t0) / repeats
+    err = np.abs(res.E[0] - E0) / np.abs(E0)
+    good = int((err <= 1e-9).sum())
+    return {"workload": "P1 100x50 cells on 100x50 nm, Gaussian well, 10 lowest levels",
+            "dofs": int(prob.n), "assemble_s": t_asm, "solve_s": t_solve,
+            "iterations": int(res.iters[0]), "converged_pairs": good,
+            "max_rel_err_vs_oracle": float(err.max()),
+            "eigenpairs_per_s": good / (t_asm + t_solve),
+            "host_oracle_s": t_host, "note": "host-timed, one dot per call (no batching)"}
+
+
 def interp_measurement(dev):
     """Field interpolation (qd_fe_interpolate): one nodal field of the P2
     400x200-cell mesh on 200x100 nm (321,201 nodes) at 16.8M uniformly random
@@ -684,6 +724,10 @@ def main():
                 result["cap_open_system"] = cap_measurement(dev)
             except Exception as e:   # recorded; the headline line stands
                 result["cap_open_system"] = {"error": repr(e)}
+            try:
+                result["single_dot_c1"] = c1_measurement(dev)
+            except Exception as e:   # recorded; the headline line stands
+                result["single_dot_c1"] = {"error": repr(e)}
             try:
                 result["field_interpolation"] = interp_measurement(dev)
             except Exception as e:   # recorded; the headline line stands
