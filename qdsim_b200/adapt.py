@@ -1,0 +1,214 @@
+"""Adaptive refinement of the triangular meshes (host side).
+
+Restates the reference's refinement step, ``FEMSolver::adapt_mesh``
+(backend/src/fem.cpp:470-542):
+- ``refinement_flags`` marks the elements whose least-squares gradient of a
+  nodal field exceeds a threshold (``AdaptiveMesh::computeRefinementFlags``,
+  backend/src/adaptive_mesh.cpp:431-494). The gradient is fitted over the
+  element's K nodes, (c, gx, gy) = pinv([1 x y]) psi_e.
+- ``refine`` red-refines them (four children by the edge midpoints, in the
+  reference's child order, adaptive_mesh.cpp:105-117).
+
+The reference then tries to close the hanging nodes by refining neighbours
+again, but indexes the old elements' flags with the new elements' numbers
+(:354-395), so its result is not a conforming mesh. Here the closure is the
+standard red-green one:
+- a triangle with two or three split edges is red-refined too, until no
+  triangle has more than one split edge;
+- a triangle with one split edge is bisected from that edge's midpoint to the
+  opposite vertex.
+The result is conforming, and every child keeps its parent's orientation.
+
+The refined mesh is a ``TriMesh``: the vertex mesh is refined, then the P2/P3
+nodes are generated on it (edge nodes at 1/2, or at 1/3 and 2/3; the P3
+centroid) in the local node order of the structured meshes. Its boundary
+nodes are those on edges that belong to one element only. ``TriMesh`` has the
+attributes ``FEMProblem`` and ``HostBatch`` read, so the GPU assembly
+(explicit coordinates) and the eigensolve run on it unchanged; the DST
+preconditioner, which needs the lattice, is not used on it.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+
+from .mesh import LOCAL_NODES, nodes_per_element
+
+_EDGES = ((0, 1), (1, 2), (2, 0))
+
+
+class TriMesh:
+    """Unstructured triangular mesh of order 1, 2 or 3 over the rectangle
+    [0, Lx] x [0, Ly]: ``nodes`` (N, 2), ``elems`` (E, K) in the local node
+    order of ``StructuredMesh``, ``boundary`` (N,) flags."""
+
+    def __init__(self, order: int, nodes, elems, boundary, Lx: float, Ly: float,
+                 nx: int, ny: int):
+        self.order = int(order)
+        self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        self.elems = np.ascontiguousarray(elems, dtype=np.int32)
+        self.boundary = np.ascontiguousarray(boundary, dtype=bool)
+        self.Lx, self.Ly = float(Lx), float(Ly)
+        # the cell counts of the mesh this one was refined from (the
+        # reference's Mesh keeps reporting them)
+        self.nx, self.ny = int(nx), int(ny)
+        if self.elems.shape[1] != nodes_per_element(self.order):
+            raise ValueError("elems do not match the element order")
+        self._key = None
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.nodes.shape[0])
+
+    @property
+    def num_elements(self) -> int:
+        return int(self.elems.shape[0])
+
+    def centroids(self) -> np.ndarray:
+        return self.nodes[self.elems[:, :3]].mean(axis=1)
+
+    def shape_key(self):
+        if self._key is None:
+            h = hashlib.sha1(self.elems.tobytes()).hexdigest()
+            self._key = ("tri", self.order, self.num_nodes, self.num_elements, h)
+        return self._key
+
+
+def refinement_flags(mesh, psi, threshold: float) -> np.ndarray:
+    """Elements whose least-squares gradient of the nodal field ``psi``
+    exceeds ``threshold`` (adaptive_mesh.cpp:431-494): per element, A = [1 x y]
+    over its K nodes, (c, gx, gy) = pinv(A) psi_e, flagged when
+    |(gx, gy)| > threshold."""
+    psi = np.asarray(psi, dtype=np.float64).reshape(-1)
+    if psi.size != mesh.num_nodes:
+        raise ValueError("psi must have one value per mesh node")
+    el = mesh.elems
+    xy = mesh.nodes[el]                                  # (E, K, 2)
+    A = np.concatenate([np.ones(el.shape + (1,)), xy], axis=2)
+    g = np.einsum("ejk,ek->ej", np.linalg.pinv(A)[:, 1:3, :], psi[el])
+    return np.sqrt(g[:, 0] ** 2 + g[:, 1] ** 2) > threshold
+
+
+def _vertex_mesh(mesh):
+    """Vertex coordinates and vertex triangles of a mesh of any order."""
+    tri = mesh.elems[:, :3]
+    verts, inv = np.unique(tri.ravel(), return_inverse=True)
+    return mesh.nodes[verts], inv.reshape(tri.shape).astype(np.int64)
+
+
+def _edge_ids(tri, nv):
+    """Unique edge ids (E, 3) of the local edges, numbered in order of first
+    appearance (element order, local edge order), and each edge's vertices."""
+    a = tri[:, [0, 1, 2]]
+    b = tri[:, [1, 2, 0]]
+    keys = (np.minimum(a, b) * nv + np.maximum(a, b)).ravel()
+    uniq, first, inv = np.unique(keys, return_index=True, return_inverse=True)
+    rank = np.empty(uniq.size, dtype=np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(uniq.size)
+    ids = rank[inv].reshape(tri.shape)
+    ends = np.empty((uniq.size, 2), dtype=np.int64)
+    ends[rank] = np.stack([uniq // nv, uniq % nv], axis=1)
+    return ids, ends
+
+
+def _refine_vertex_mesh(V, T, flags):
+    """Red-green refinement of the vertex mesh (V, T) for the flagged
+    triangles.  Returns the new vertices (old ones first, then the edge
+    midpoints in order of first appearance) and triangles (each parent's
+    children in the parent's place)."""
+    nv = V.shape[0]
+    eid, ends = _edge_ids(T, nv)
+    red = np.asarray(flags, dtype=bool).copy()
+    split = np.zeros(ends.shape[0], dtype=bool)
+    split[eid[red].ravel()] = True
+    while True:                            # red closure: two or more split edges
+        cnt = split[eid].sum(axis=1)
+        more = (~red) & (cnt >= 2)
+        if not more.any():
+            break
+        red |= more
+        split[eid[more].ravel()] = True
+    green = (~red) & (split[eid].sum(axis=1) == 1)
+    mid = np.full(ends.shape[0], -1, dtype=np.int64)
+    order = np.flatnonzero(split)          # edge ids are already first-appearance ranks
+    mid[order] = nv + np.arange(order.size)
+    newV = np.concatenate([V, 0.5 * (V[ends[order, 0]] + V[ends[order, 1]])])
+    out = []
+    for e in range(T.shape[0]):
+        n0, n1, n2 = T[e]
+        if red[e]:
+            m01, m12, m20 = mid[eid[e, 0]], mid[eid[e, 1]], mid[eid[e, 2]]
+            out += [(n0, m01, m20), (n1, m12, m01), (n2, m20, m12), (m01, m12, m20)]
+        elif green[e]:
+            j = int(np.flatnonzero(split[eid[e]])[0])
+            a, b, c = T[e][j], T[e][(j + 1) % 3], T[e][(j + 2) % 3]
+            m = mid[eid[e, j]]
+            out += [(a, m, c), (m, b, c)]
+        else:
+            out.append((n0, n1, n2))
+    return newV, np.asarray(out, dtype=np.int64)
+
+
+def _lift(V, T, order):
+    """Elements of ``order`` on the vertex mesh (V, T): vertices first, then
+    the edge nodes (per edge in order of first appearance; for P3 the node
+    nearer the lower-numbered vertex first), then the P3 centroids."""
+    nv = V.shape[0]
+    eid, ends = _edge_ids(T, nv)
+    ne = ends.shape[0]
+    # boundary: edges of one element only, with all their nodes
+    counts = np.bincount(eid.ravel(), minlength=ne)
+    bedge = counts == 1
+    if order == 1:
+        bnd = np.zeros(nv, dtype=bool)
+        bnd[ends[bedge].ravel()] = True
+        return V, T, bnd
+    p = order
+    per_edge = p - 1
+    u, v = V[ends[:, 0]], V[ends[:, 1]]
+    edge_nodes = [((p - s) * u + s * v) / p for s in range(1, p)]   # s-th from the lower end
+    E_nodes = np.stack(edge_nodes, axis=1).reshape(ne * per_edge, 2)
+    nodes = [V, E_nodes]
+    if p == 3:
+        nodes.append(V[T].mean(axis=1))
+    nodes = np.concatenate(nodes)
+    K = nodes_per_element(p)
+    el = np.zeros((T.shape[0], K), dtype=np.int64)
+    el[:, :3] = T
+    for a, bc in enumerate(LOCAL_NODES[p]):
+        if a < 3:
+            continue
+        nz = [m for m in range(3) if bc[m] > 0]
+        if len(nz) == 3:                               # P3 centroid
+            el[:, a] = nv + ne * per_edge + np.arange(T.shape[0])
+            continue
+        i, j = nz                                      # local edge between vertices i and j
+        k = {(0, 1): 0, (1, 2): 1, (0, 2): 2}[(i, j)]
+        e = eid[:, k]
+        lo = ends[e, 0]
+        # distance (in steps of 1/p) of this node from the edge's lower end
+        steps_from_i = bc[j]                          # bc[j] / p of the way from i to j
+        s = np.where(T[:, i] == lo, steps_from_i, p - steps_from_i)
+        el[:, a] = nv + e * per_edge + (s - 1)
+    bnd = np.zeros(nodes.shape[0], dtype=bool)
+    be = np.flatnonzero(bedge)
+    bnd[ends[be].ravel()] = True
+    for s in range(per_edge):
+        bnd[nv + be * per_edge + s] = True
+    return nodes, el, bnd
+
+
+def refine(mesh, flags) -> TriMesh:
+    """The mesh after refining the flagged elements (red-green closure, see
+    the module docstring), as a ``TriMesh`` of the same order."""
+    flags = np.asarray(flags, dtype=bool).reshape(-1)
+    if flags.size != mesh.num_elements:
+        raise ValueError("one flag per element")
+    V, T = _vertex_mesh(mesh)
+    V2, T2 = _refine_vertex_mesh(V, T, flags)
+    nodes, el, bnd = _lift(V2, T2, mesh.order)
+    return TriMesh(mesh.order, nodes, el, bnd, mesh.Lx, mesh.Ly, mesh.nx, mesh.ny)
+
+
+__all__ = ["TriMesh", "refinement_flags", "refine"]

@@ -27,6 +27,9 @@ Semantics kept from the C++ classes (SI units in and out):
    (``qd_fe_interpolate``): the reference's element scan becomes an O(1)
    cell lookup with the same containing element, and points outside the mesh
    take the nearest node's value and the reference's gradient estimate.
+ - ``FEMSolver.adapt_mesh`` refines the mesh where the eigenvector varies
+   fastest (``qdsim_b200.adapt``: the reference's gradient flags, red-green
+   refinement) and reassembles on the refined, unstructured mesh.
  - ``potential``, ``effective_mass``, ``epsilon_r`` and ``cap`` are the
    callbacks of backend/src/physics.cpp the frontend hands to ``FEMSolver``;
    ``potential`` resamples the electrostatic potential through the
@@ -37,12 +40,15 @@ eigenvectors are M-normalised in m^2.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 
 from . import _native as N
 from .batch import DeviceBatch, HostBatch
 from .fem import C0_EV_NM2, FEMProblem, M_E, Q_E
+from .adapt import TriMesh, refine, refinement_flags
 from .interp import FieldInterpolator
 from .mesh import StructuredMesh
 from .solvers import _block_for, _eval
@@ -88,6 +94,13 @@ class Mesh:
     def get_ny(self) -> int:
         return int(self._si.ny)
 
+    def is_refined(self) -> bool:
+        """True once ``FEMSolver.adapt_mesh`` has replaced the structured mesh."""
+        return isinstance(self._si, TriMesh)
+
+    def _replace(self, si, nm):
+        self._si, self._nm = si, nm
+
     getNumNodes = get_num_nodes
     getNumElements = get_num_elements
     getElementOrder = get_element_order
@@ -120,7 +133,9 @@ class FEMSolver:
         cen = si.centroids()
         mstar = _eval(self.m_star, cen[:, 0], cen[:, 1])
         c = C0_EV_NM2 * (M_E / mstar)
-        if self._use_interp:
+        # the interpolated potential applies while it matches the mesh
+        # (fem.cpp:934); after a refinement the V callback is used again
+        if self._use_interp and self._potential.size == si.num_nodes:
             V_eV = self._potential / Q_E
         else:
             V_eV = _eval(self.V, si.nodes[:, 0], si.nodes[:, 1]) / Q_E
@@ -146,8 +161,35 @@ class FEMSolver:
         self._need()
         return (self._prob.to_scipy(self._mats["M"]) * 1e-18).tocsr()
 
-    def adapt_mesh(self, *args, **kwargs):
-        raise NotImplementedError("adaptive mesh refinement is not part of qdsim_b200")
+    def adapt_mesh(self, eigenvector, threshold, cache_dir=""):
+        """Refine the mesh where the nodal ``eigenvector`` varies fastest and
+        reassemble (fem.cpp:470-542): elements whose least-squares gradient
+        (in the mesh's units) exceeds ``threshold`` are red-refined, with a
+        conforming red-green closure (``qdsim_b200.adapt``).  With a
+        ``cache_dir`` the refined mesh is stored as mesh_<norm>.npz (<norm> the
+        eigenvector's 2-norm, six decimals) and reused when that file exists.
+        The refined mesh is unstructured: the interpolator is not available on
+        it, and the eigensolve runs without the DST preconditioner."""
+        psi = np.real(np.asarray(eigenvector)).astype(np.float64).reshape(-1)
+        si, nm = self.mesh._si, self.mesh._nm
+        cache = (os.path.join(cache_dir, f"mesh_{np.linalg.norm(psi):.6f}.npz")
+                 if cache_dir else None)
+        if cache is not None and os.path.exists(cache):
+            z = np.load(cache)
+            args = (int(z["order"]), z["nodes"], z["elems"], z["boundary"])
+            si2 = TriMesh(*args, float(z["Lx"]), float(z["Ly"]), int(z["nx"]), int(z["ny"]))
+            nm2 = TriMesh(args[0], args[1] * 1e9, args[2], args[3], si2.Lx * 1e9,
+                          si2.Ly * 1e9, si2.nx, si2.ny)
+        else:
+            flags = refinement_flags(si, psi, threshold)
+            si2, nm2 = refine(si, flags), refine(nm, flags)
+            if cache is not None:
+                os.makedirs(cache_dir, exist_ok=True)
+                np.savez(cache, order=si2.order, nodes=si2.nodes, elems=si2.elems,
+                         boundary=si2.boundary, Lx=si2.Lx, Ly=si2.Ly, nx=si2.nx, ny=si2.ny)
+        self.mesh._replace(si2, nm2)
+        self._interp = None
+        self.assemble_matrices()
 
     def get_interpolator(self):
         if self._interp is None:

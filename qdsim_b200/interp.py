@@ -33,6 +33,10 @@ class FieldInterpolator:
     def __init__(self, mesh: StructuredMesh, device="cuda", outside: str = "nearest"):
         if outside not in ("nearest", "zero"):
             raise ValueError("outside must be 'nearest' or 'zero'")
+        if not isinstance(mesh, StructuredMesh):
+            raise NotImplementedError(
+                "point location uses the structured lattice; refined (unstructured) meshes "
+                "are not supported")
         self.mesh = mesh
         self.device = torch.device(device)
         self.outside = outside
