@@ -170,3 +170,33 @@ def test_frontend_adapt_mesh_host_logic(tmp_path, monkeypatch):
     # the interpolator needs the lattice
     with pytest.raises(NotImplementedError):
         fem.get_interpolator()
+
+
+def test_adaptive_step_improves_levels_with_fewer_elements():
+    """One adapt step on a dot (the oracle's assembly and eigensolve on the
+    refined mesh): the lowest levels move toward those of a mesh four times
+    finer, with fewer elements than refining everything."""
+    Lx, Ly, nx, ny = 40.0, 30.0, 16, 12
+
+    def levels(mesh, k=3):
+        om = O.Mesh(mesh.order, mesh.nx, mesh.ny, mesh.Lx, mesh.Ly, mesh.nodes,
+                    mesh.elems, mesh.boundary)
+        x, y = mesh.nodes[:, 0], mesh.nodes[:, 1]
+        V = -0.4 * np.exp(-((x - 17.0) ** 2 + (y - 14.0) ** 2) / (2 * 3.0 ** 2))
+        c = np.full(mesh.num_elements, O.C0_EV_NM2 / 0.067)
+        a = O.assemble(om, c, V)
+        E, X = O.eig_lowest(a.H, a.M, k, O.sigma_below(V))
+        psi = np.zeros(mesh.num_nodes)
+        psi[a.dm >= 0] = X[a.dm[a.dm >= 0], 0]
+        return E, psi
+
+    coarse = StructuredMesh(1, nx, ny, Lx, Ly)
+    E_c, psi = levels(coarse)
+    E_f, _ = levels(StructuredMesh(1, 4 * nx, 4 * ny, Lx, Ly))
+    g = OA.element_gradients(coarse.nodes, coarse.elems, np.abs(psi))
+    gn = np.sqrt((g ** 2).sum(1))
+    flags = A.refinement_flags(coarse, np.abs(psi), float(np.quantile(gn, 0.6)))
+    tm = A.refine(coarse, flags)
+    E_a, _ = levels(tm)
+    assert tm.num_elements < 4 * coarse.num_elements
+    assert (np.abs(E_a - E_f) < 0.6 * np.abs(E_c - E_f)).all(), (E_c, E_a, E_f)
