@@ -200,3 +200,22 @@ def test_adaptive_step_improves_levels_with_fewer_elements():
     E_a, _ = levels(tm)
     assert tm.num_elements < 4 * coarse.num_elements
     assert (np.abs(E_a - E_f) < 0.6 * np.abs(E_c - E_f)).all(), (E_c, E_a, E_f)
+
+
+def test_host_batch_accepts_a_refined_mesh():
+    """The host half of the eigensolve path on a refined mesh: HostBatch
+    builds its pattern and arrays for a TriMesh (natural boundaries, as the
+    frontend's EigenSolver uses, so no lattice preconditioner is asked for)."""
+    from qdsim_b200 import batch as B
+    from qdsim_b200.workloads import Dot
+    m = StructuredMesh(2, 10, 6, 12.0, 8.0)
+    tm = A.refine(m, A.refinement_flags(m, _field(m.nodes), 0.2))
+    c = np.full(tm.num_elements, 0.5)
+    V = -0.1 * _field(tm.nodes)
+    hb = B.HostBatch([Dot(tm, c, V)], dirichlet=False)
+    assert hb.n == tm.num_nodes and hb.prec_specs is None
+    assert hb.arrays["elems"].shape == tm.elems.shape
+    assert int(hb.arrays["rowptr"][-1]) == hb.nnz
+    # the same topology twice hits the pattern cache (shape_key of the TriMesh)
+    hb2 = B.HostBatch([Dot(tm, c, V), Dot(tm, c, V)], dirichlet=False)
+    assert hb2.nnz == 2 * hb.nnz
