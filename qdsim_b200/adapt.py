@@ -12,12 +12,17 @@ Restates the reference's refinement step, ``FEMSolver::adapt_mesh``
 The reference then tries to close the hanging nodes by refining neighbours
 again, but indexes the old elements' flags with the new elements' numbers
 (:354-395), so its result is not a conforming mesh. Here the closure is the
-standard red-green one:
+standard red-green one with green removal:
 - a triangle with two or three split edges is red-refined too, until no
   triangle has more than one split edge;
 - a triangle with one split edge is bisected from that edge's midpoint to the
-  opposite vertex.
-The result is conforming, and every child keeps its parent's orientation.
+  opposite vertex (a green pair, whose parent the mesh remembers);
+- green pairs are merged back into their parents before the next refinement,
+  so a green triangle is never bisected again;
+- a red triangle on half of a hanging edge makes the coarse triangle across
+  it red too, so neighbours differ by at most one level.
+The result is conforming, every child keeps its parent's orientation, and
+shapes and vertex valences stay bounded over repeated refinements.
 
 The refined mesh is a ``TriMesh``: the vertex mesh is refined, then the P2/P3
 nodes are generated on it (edge nodes at 1/2, or at 1/3 and 2/3; the P3
@@ -44,7 +49,7 @@ class TriMesh:
     order of ``StructuredMesh``, ``boundary`` (N,) flags."""
 
     def __init__(self, order: int, nodes, elems, boundary, Lx: float, Ly: float,
-                 nx: int, ny: int):
+                 nx: int, ny: int, green_pair=None, green_parent=None):
         self.order = int(order)
         self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
         self.elems = np.ascontiguousarray(elems, dtype=np.int32)
@@ -55,6 +60,14 @@ class TriMesh:
         self.nx, self.ny = int(nx), int(ny)
         if self.elems.shape[1] != nodes_per_element(self.order):
             raise ValueError("elems do not match the element order")
+        # green pairs of the last refinement: pair id per element (-1 none)
+        # and each pair's parent triangle (vertex node numbers)
+        self.green_pair = (np.full(self.num_elements, -1, dtype=np.int64) if green_pair is None
+                           else np.asarray(green_pair, dtype=np.int64))
+        self.green_parent = (np.zeros((0, 3), dtype=np.int64) if green_parent is None
+                             else np.asarray(green_parent, dtype=np.int64).reshape(-1, 3))
+        if self.green_pair.shape != (self.num_elements,):
+            raise ValueError("one green-pair entry per element")
         self._key = None
 
     @property
@@ -91,10 +104,13 @@ def refinement_flags(mesh, psi, threshold: float) -> np.ndarray:
 
 
 def _vertex_mesh(mesh):
-    """Vertex coordinates and vertex triangles of a mesh of any order."""
+    """Vertex coordinates and vertex triangles of a mesh of any order, and the
+    node -> vertex map (-1 for nodes that are not vertices)."""
     tri = mesh.elems[:, :3]
     verts, inv = np.unique(tri.ravel(), return_inverse=True)
-    return mesh.nodes[verts], inv.reshape(tri.shape).astype(np.int64)
+    vmap = np.full(mesh.num_nodes, -1, dtype=np.int64)
+    vmap[verts] = np.arange(verts.size)
+    return mesh.nodes[verts], inv.reshape(tri.shape).astype(np.int64), vmap
 
 
 def _edge_ids(tri, nv):
@@ -112,42 +128,136 @@ def _edge_ids(tri, nv):
     return ids, ends
 
 
-def _refine_vertex_mesh(V, T, flags):
+def _refine_vertex_mesh(V, T, flags, pair=None, parents=None, extra_hang=None):
     """Red-green refinement of the vertex mesh (V, T) for the flagged
-    triangles.  Returns the new vertices (old ones first, then the edge
-    midpoints in order of first appearance) and triangles (each parent's
-    children in the parent's place)."""
+    triangles, with green removal.
+
+    ``pair[e]`` names the green pair triangle e belongs to (-1 for none) and
+    ``parents[p]`` that pair's parent triangle (a, b, c), bisected on (a, b).
+
+    1. Every green pair is replaced by its parent (flagged when either half
+       is), which leaves a red-only mesh whose hanging edges are the parents'
+       bisected edges, each with its existing midpoint.
+    2. Closure, until stable:
+       - a triangle is red when flagged;
+       - a triangle is red when two or more of its edges are split (hanging,
+         or an edge of a red triangle);
+       - a red triangle lying on half of a hanging edge makes the coarse
+         triangle across that edge red too, so neighbours never differ by
+         more than one level.
+    3. Red triangles get four children, in the reference's order. A hanging
+       edge reuses its midpoint. A triangle with exactly one split edge is
+       bisected to its opposite vertex (a new green pair).
+
+    Only red triangles are ever subdivided further, so shapes and vertex
+    valences stay bounded over repeated refinements. Returns the new vertices
+    (old ones first, then the new midpoints in order of first appearance),
+    the triangles (each parent's children in the parent's place) and the new
+    green pairs and parents."""
+    V = np.asarray(V, dtype=np.float64)
     nv = V.shape[0]
+    T = np.asarray(T, dtype=np.int64)
+    flags = np.asarray(flags, dtype=bool)
+    hang = dict(extra_hang or {})           # hanging edge -> its midpoint vertex
+    if pair is not None and (np.asarray(pair) >= 0).any():
+        pair = np.asarray(pair, dtype=np.int64)
+        parents = np.asarray(parents, dtype=np.int64)
+        nT, nF, seen = [], [], set()
+        for e in range(T.shape[0]):
+            pid = int(pair[e])
+            if pid < 0:
+                nT.append(T[e])
+                nF.append(bool(flags[e]))
+                continue
+            if pid in seen:
+                continue
+            seen.add(pid)
+            pa, pb, pc = (int(v) for v in parents[pid])
+            m = ({int(v) for v in T[e]} - {pa, pb, pc}).pop()
+            hang[(min(pa, pb), max(pa, pb))] = m
+            nT.append((pa, pb, pc))
+            nF.append(bool(flags[pair == pid].any()))
+        T = np.asarray(nT, dtype=np.int64)
+        flags = np.asarray(nF, dtype=bool)
     eid, ends = _edge_ids(T, nv)
-    red = np.asarray(flags, dtype=bool).copy()
-    split = np.zeros(ends.shape[0], dtype=bool)
-    split[eid[red].ravel()] = True
-    while True:                            # red closure: two or more split edges
-        cnt = split[eid].sum(axis=1)
-        more = (~red) & (cnt >= 2)
+    ne = ends.shape[0]
+    keyid = {(int(u), int(v)): i for i, (u, v) in enumerate(ends)}
+    is_hang = np.zeros(ne, dtype=bool)
+    owner = np.full(ne, -1, dtype=np.int64)  # half of a hanging edge -> coarse triangle
+    tri_of = np.full(ne, -1, dtype=np.int64)
+    tri_of[eid.ravel()] = np.repeat(np.arange(T.shape[0]), 3)
+    for (u, v), m in hang.items():
+        h = keyid[(u, v)]
+        is_hang[h] = True
+        for half in ((min(u, m), max(u, m)), (min(m, v), max(m, v))):
+            if half in keyid:
+                owner[keyid[half]] = tri_of[h]
+    red = flags.copy()
+    while True:
+        split = is_hang.copy()
+        split[eid[red].ravel()] = True
+        more = (~red) & (split[eid].sum(axis=1) >= 2)
+        coarse = owner[eid[red].ravel()]
+        coarse = coarse[coarse >= 0]
+        more[coarse[~red[coarse]]] = True
         if not more.any():
             break
         red |= more
-        split[eid[more].ravel()] = True
     green = (~red) & (split[eid].sum(axis=1) == 1)
-    mid = np.full(ends.shape[0], -1, dtype=np.int64)
-    order = np.flatnonzero(split)          # edge ids are already first-appearance ranks
-    mid[order] = nv + np.arange(order.size)
-    newV = np.concatenate([V, 0.5 * (V[ends[order, 0]] + V[ends[order, 1]])])
-    out = []
+    mid = np.full(ne, -1, dtype=np.int64)
+    fresh = []
+    for ed in np.flatnonzero(split):        # edge ids are first-appearance ranks
+        k = (int(ends[ed, 0]), int(ends[ed, 1]))
+        if k in hang:
+            mid[ed] = hang[k]
+        else:
+            mid[ed] = nv + len(fresh)
+            fresh.append(ed)
+    fresh = np.asarray(fresh, dtype=np.int64)
+    newV = np.concatenate([V, 0.5 * (V[ends[fresh, 0]] + V[ends[fresh, 1]])])
+    mids = {(int(ends[ed, 0]), int(ends[ed, 1])): int(mid[ed]) for ed in np.flatnonzero(split)}
+    out, out_pair, out_parents = [], [], []
     for e in range(T.shape[0]):
         n0, n1, n2 = T[e]
         if red[e]:
             m01, m12, m20 = mid[eid[e, 0]], mid[eid[e, 1]], mid[eid[e, 2]]
             out += [(n0, m01, m20), (n1, m12, m01), (n2, m20, m12), (m01, m12, m20)]
+            out_pair += [-1] * 4
         elif green[e]:
             j = int(np.flatnonzero(split[eid[e]])[0])
             a, b, c = T[e][j], T[e][(j + 1) % 3], T[e][(j + 2) % 3]
             m = mid[eid[e, j]]
             out += [(a, m, c), (m, b, c)]
+            out_pair += [len(out_parents)] * 2
+            out_parents.append((a, b, c))
         else:
             out.append((n0, n1, n2))
-    return newV, np.asarray(out, dtype=np.int64)
+            out_pair.append(-1)
+    return (newV, np.asarray(out, dtype=np.int64), np.asarray(out_pair, dtype=np.int64),
+            np.asarray(out_parents, dtype=np.int64).reshape(-1, 3), mids)
+
+
+def _refine_conforming(V, T, flags, pair, parents):
+    """One refinement step, then closure passes until no edge of the mesh has
+    a midpoint used on its other side.  A coarse triangle and a finer one on
+    half of its hanging edge can both be refined in one step; the coarse
+    triangle's child then keeps a full edge that the fine side split, and the
+    next pass (no new flags) closes it like any other split edge."""
+    V, T, pair, parents, known = _refine_vertex_mesh(V, T, flags, pair, parents)
+    while True:
+        a = T[:, [0, 1, 2]]
+        b = T[:, [1, 2, 0]]
+        lo, hi = np.minimum(a, b).ravel(), np.maximum(a, b).ravel()
+        residual = {}
+        for u, v in zip(lo.tolist(), hi.tolist()):
+            m = known.get((u, v))
+            if m is not None:
+                residual[(u, v)] = m
+        if not residual:
+            return V, T, pair, parents
+        V, T, pair, parents, more = _refine_vertex_mesh(
+            V, T, np.zeros(T.shape[0], dtype=bool), pair, parents, extra_hang=residual)
+        known.update(more)
 
 
 def _lift(V, T, order):
@@ -205,10 +315,16 @@ def refine(mesh, flags) -> TriMesh:
     flags = np.asarray(flags, dtype=bool).reshape(-1)
     if flags.size != mesh.num_elements:
         raise ValueError("one flag per element")
-    V, T = _vertex_mesh(mesh)
-    V2, T2 = _refine_vertex_mesh(V, T, flags)
+    V, T, vmap = _vertex_mesh(mesh)
+    pair = getattr(mesh, "green_pair", None)
+    parents = getattr(mesh, "green_parent", None)
+    if parents is not None:
+        parents = vmap[parents]
+    V2, T2, pair2, parents2 = _refine_conforming(V, T, flags, pair, parents)
     nodes, el, bnd = _lift(V2, T2, mesh.order)
-    return TriMesh(mesh.order, nodes, el, bnd, mesh.Lx, mesh.Ly, mesh.nx, mesh.ny)
+    # vertices keep their numbers in the lifted mesh (they come first)
+    return TriMesh(mesh.order, nodes, el, bnd, mesh.Lx, mesh.Ly, mesh.nx, mesh.ny,
+                   green_pair=pair2, green_parent=parents2)
 
 
 __all__ = ["TriMesh", "refinement_flags", "refine"]

@@ -177,16 +177,19 @@ class FEMSolver:
         if cache is not None and os.path.exists(cache):
             z = np.load(cache)
             args = (int(z["order"]), z["nodes"], z["elems"], z["boundary"])
-            si2 = TriMesh(*args, float(z["Lx"]), float(z["Ly"]), int(z["nx"]), int(z["ny"]))
+            green = dict(green_pair=z["green_pair"], green_parent=z["green_parent"])
+            si2 = TriMesh(*args, float(z["Lx"]), float(z["Ly"]), int(z["nx"]), int(z["ny"]),
+                          **green)
             nm2 = TriMesh(args[0], args[1] * 1e9, args[2], args[3], si2.Lx * 1e9,
-                          si2.Ly * 1e9, si2.nx, si2.ny)
+                          si2.Ly * 1e9, si2.nx, si2.ny, **green)
         else:
             flags = refinement_flags(si, psi, threshold)
             si2, nm2 = refine(si, flags), refine(nm, flags)
             if cache is not None:
                 os.makedirs(cache_dir, exist_ok=True)
                 np.savez(cache, order=si2.order, nodes=si2.nodes, elems=si2.elems,
-                         boundary=si2.boundary, Lx=si2.Lx, Ly=si2.Ly, nx=si2.nx, ny=si2.ny)
+                         boundary=si2.boundary, Lx=si2.Lx, Ly=si2.Ly, nx=si2.nx, ny=si2.ny,
+                         green_pair=si2.green_pair, green_parent=si2.green_parent)
         self.mesh._replace(si2, nm2)
         self._interp = None
         self.assemble_matrices()

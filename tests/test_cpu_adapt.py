@@ -219,3 +219,32 @@ def test_host_batch_accepts_a_refined_mesh():
     # the same topology twice hits the pattern cache (shape_key of the TriMesh)
     hb2 = B.HostBatch([Dot(tm, c, V), Dot(tm, c, V)], dirichlet=False)
     assert hb2.nnz == 2 * hb.nnz
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_repeated_refinement_stays_conforming_and_shape_regular(order):
+    """Green triangles are never bisected again (green removal): over
+    repeated refinements the mesh stays conforming, the smallest angle does
+    not shrink after the first step, and vertex valences stay within the 16
+    elements per node the pattern builder accepts."""
+    cur = StructuredMesh(order, 10, 6, 12.0, 8.0)
+    first_min = None
+    for step in range(4):
+        cur = A.refine(cur, A.refinement_flags(cur, _field(cur.nodes), 0.15))
+        _check_conforming(cur)
+        tri = cur.elems[:, :3]
+        ar = _areas(cur.nodes, tri)
+        assert (ar > 0).all() and np.isclose(ar.sum(), 96.0, rtol=1e-12)
+        assert np.unique(cur.elems).size == cur.num_nodes
+        P = cur.nodes[tri]
+        ang = []
+        for k in range(3):
+            u, v = P[:, (k + 1) % 3] - P[:, k], P[:, (k + 2) % 3] - P[:, k]
+            c = np.sum(u * v, 1) / np.linalg.norm(u, axis=1) / np.linalg.norm(v, axis=1)
+            ang.append(np.degrees(np.arccos(np.clip(c, -1, 1))))
+        amin = float(np.min(ang))
+        first_min = amin if first_min is None else first_min
+        assert amin >= first_min - 1e-9
+        assert np.bincount(tri.ravel()).max() <= 16
+        dm, n = dof_map_for(cur, True)
+        build_pattern(cur.elems, dm, n, cur.num_nodes)
