@@ -45,7 +45,6 @@ import os
 import numpy as np
 import torch
 
-from . import _native as N
 from .batch import DeviceBatch, HostBatch
 from .fem import C0_EV_NM2, FEMProblem, M_E, Q_E
 from .adapt import TriMesh, refine, refinement_flags
