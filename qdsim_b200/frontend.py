@@ -296,6 +296,46 @@ class FEInterpolator:
         return (all(v >= -1e-10 for v in lam), lam)
 
 
+class AdaptiveMesh:
+    """The static refinement helpers bound as ``qdsim_cpp.AdaptiveMesh``
+    (backend/src/bindings.cpp:1590-1608) on this module's ``Mesh``."""
+
+    @staticmethod
+    def compute_refinement_flags(mesh: Mesh, psi, threshold):
+        """Elements whose least-squares gradient of the nodal ``psi`` (per
+        metre) exceeds ``threshold`` (adaptive_mesh.cpp:431-494)."""
+        return [bool(f) for f in refinement_flags(mesh._si, psi, threshold)]
+
+    @staticmethod
+    def refine_mesh(mesh: Mesh, refine_flags):
+        """Refine the flagged elements of ``mesh`` in place (conforming
+        red-green refinement, ``qdsim_b200.adapt.refine``)."""
+        flags = np.asarray(refine_flags, dtype=bool)
+        mesh._replace(refine(mesh._si, flags), refine(mesh._nm, flags))
+
+    @staticmethod
+    def compute_triangle_quality(mesh: Mesh, elem_idx: int) -> float:
+        """4 sqrt(3) area / (sum of squared edge lengths): 1 for an
+        equilateral triangle (adaptive_mesh.cpp:1323-1337)."""
+        p = mesh._si.nodes[mesh._si.elems[int(elem_idx), :3]]
+        l1 = float(np.linalg.norm(p[1] - p[0]))
+        l2 = float(np.linalg.norm(p[2] - p[1]))
+        l3 = float(np.linalg.norm(p[0] - p[2]))
+        sp = 0.5 * (l1 + l2 + l3)
+        area = np.sqrt(max(sp * (sp - l1) * (sp - l2) * (sp - l3), 0.0))
+        return float(4.0 * np.sqrt(3.0) * area / (l1 * l1 + l2 * l2 + l3 * l3))
+
+    @staticmethod
+    def is_mesh_conforming(mesh: Mesh) -> bool:
+        """False when an edge is shared by more than two triangles, the test
+        the reference makes (adaptive_mesh.cpp:1339-1362)."""
+        tri = mesh._si.elems[:, :3].astype(np.int64)
+        a, b = tri, np.roll(tri, -1, axis=1)
+        n = int(tri.max()) + 1
+        keys = (np.minimum(a, b) * n + np.maximum(a, b)).ravel()
+        return bool(np.unique(keys, return_counts=True)[1].max() <= 2)
+
+
 # the elementary charge and the potential cap of backend/src/physics.cpp:69-141
 _PHYS_Q = 1.602e-19
 _MAX_POTENTIAL_EV = 100.0
@@ -413,5 +453,5 @@ class EigenSolver:
         return [v.copy() for v in self.eigenvectors]
 
 
-__all__ = ["Mesh", "FEMSolver", "EigenSolver", "FEInterpolator", "potential",
+__all__ = ["Mesh", "FEMSolver", "EigenSolver", "FEInterpolator", "AdaptiveMesh", "potential",
            "effective_mass", "epsilon_r", "cap"]

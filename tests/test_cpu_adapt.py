@@ -248,3 +248,21 @@ def test_repeated_refinement_stays_conforming_and_shape_regular(order):
         assert np.bincount(tri.ravel()).max() <= 16
         dm, n = dof_map_for(cur, True)
         build_pattern(cur.elems, dm, n, cur.num_nodes)
+
+
+def test_frontend_adaptive_mesh_helpers():
+    """qdsim_cpp.AdaptiveMesh's static helpers on the frontend Mesh."""
+    from qdsim_b200 import frontend as F
+    mesh = F.Mesh(12e-9, 8e-9, 10, 6, 1)
+    psi = _field(mesh.get_nodes() * 1e9)
+    flags = F.AdaptiveMesh.compute_refinement_flags(mesh, psi, 0.2e9)
+    assert isinstance(flags, list) and 0 < sum(flags) < mesh.get_num_elements()
+    np.testing.assert_array_equal(flags, OA.refinement_flags(mesh.get_nodes(),
+                                                             mesh.get_elements(), psi, 0.2e9))
+    # right isosceles cells: quality 4 sqrt(3) (h^2/2) / (4 h^2) = sqrt(3)/2
+    sq = F.Mesh(10e-9, 10e-9, 5, 5, 1)
+    assert F.AdaptiveMesh.compute_triangle_quality(sq, 0) == pytest.approx(np.sqrt(3) / 2)
+    e0 = mesh.get_num_elements()
+    F.AdaptiveMesh.refine_mesh(mesh, flags)
+    assert mesh.is_refined() and mesh.get_num_elements() > e0
+    assert F.AdaptiveMesh.is_mesh_conforming(mesh)
