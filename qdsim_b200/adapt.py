@@ -150,10 +150,13 @@ def _refine_vertex_mesh(V, T, flags, pair=None, parents=None, extra_hang=None):
        bisected to its opposite vertex (a new green pair).
 
     Only red triangles are ever subdivided further, so shapes and vertex
-    valences stay bounded over repeated refinements. Returns the new vertices
-    (old ones first, then the new midpoints in order of first appearance),
-    the triangles (each parent's children in the parent's place) and the new
-    green pairs and parents."""
+    valences stay bounded over repeated refinements.
+
+    ``extra_hang`` adds hanging edges (edge -> existing midpoint) left by an
+    earlier pass.  Returns the new vertices (old ones first, then the new
+    midpoints in order of first appearance), the triangles (each parent's
+    children in the parent's place), the new green pairs and parents, and
+    the midpoint of every edge split in this pass."""
     V = np.asarray(V, dtype=np.float64)
     nv = V.shape[0]
     T = np.asarray(T, dtype=np.int64)
