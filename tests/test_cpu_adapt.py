@@ -266,3 +266,27 @@ def test_frontend_adaptive_mesh_helpers():
     F.AdaptiveMesh.refine_mesh(mesh, flags)
     assert mesh.is_refined() and mesh.get_num_elements() > e0
     assert F.AdaptiveMesh.is_mesh_conforming(mesh)
+
+
+def test_red_children_follow_the_reference_order():
+    """A flagged element's four children replace it in place, in the order and
+    vertex order of adaptive_mesh.cpp:105-108: (n0, m01, m20), (n1, m12, m01),
+    (n2, m20, m12), (m01, m12, m20)."""
+    m = StructuredMesh(1, 3, 3, 3.0, 3.0)
+    e = 2 * (1 * 3 + 1)                                     # the middle cell's t = 0
+    flags = np.zeros(m.num_elements, bool)
+    flags[e] = True
+    tm = A.refine(m, flags)
+    n0, n1, n2 = (m.nodes[i] for i in m.elems[e])
+    m01, m12, m20 = (n0 + n1) / 2, (n1 + n2) / 2, (n2 + n0) / 2
+    want = [(n0, m01, m20), (n1, m12, m01), (n2, m20, m12), (m01, m12, m20)]
+    # children are consecutive, where the parent was: after the outputs of
+    # the elements before it (a bisected neighbour among them yields two)
+    P = tm.nodes[tm.elems[:, :3]]
+    first = [i for i in range(tm.num_elements) if np.allclose(P[i], np.array(want[0]))]
+    assert len(first) == 1
+    for k, tri in enumerate(want):
+        np.testing.assert_allclose(P[first[0] + k], np.array(tri), atol=1e-12)
+    # two neighbours precede it (across its bottom and left edges), each
+    # bisected into two
+    assert first[0] == e + 2
