@@ -327,6 +327,46 @@ def c1_measurement(dev, repeats=5):
             "host_oracle_s": t_host, "note": "host-timed, one dot per call (no batching)"}
 
 
+def c3_measurement(dev, launches=20):
+    """Adjoint gradients on the P3 150x75-cell dot (config 3): dL/dV (nodal)
+    and dL/dc (per element) of L = E1+E2+E3+E4 + (E2-E1) from 4 states, one
+    qd_adjoint launch each, timed with CUDA events over ``launches`` launches.
+    The states are seeded random vectors of the eigenvectors' shape (the
+    launch does the same work for any values; the gradients' accuracy is the
+    GPU tests' concern).  Algorithmic bytes per launch: the states n 4 8, the
+    connectivity E 10 4, coordinates N 16 and the DOF map N 4 in; N 8 + E 8
+    out."""
+    import torch
+    from qdsim_b200 import adjoint as AD, fem as F, workloads as W
+    d = W.c3_dot(0)
+    prob = F.FEMProblem(d.mesh, device=dev)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    psi = torch.randn(prob.n, 4, generator=g, dtype=torch.float64).to(dev)
+    w = np.array([0.0, 2.0, 1.0, 1.0])
+    for _ in range(3):
+        AD.energy_gradients(prob, psi, w)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        AD.energy_gradients(prob, psi, w)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    m = d.mesh
+    alg = prob.n * 4 * 8 + m.num_elements * 10 * 4 + m.num_nodes * (16 + 4 + 8) + \
+        m.num_elements * 8
+    peak = FALLBACK_HBM
+    if os.path.exists(PEAKS):
+        with open(PEAKS) as f:
+            peak = float(json.load(f).get("hbm_gbs", FALLBACK_HBM))
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"workload": "P3 150x75 cells, 4 states, L = E1+E2+E3+E4 + (E2-E1)",
+            "nodes": int(m.num_nodes), "elements": int(m.num_elements), "ms_per_launch": ms,
+            "algorithmic_bytes": int(alg), "GBps": gbs, "frac": gbs / peak,
+            "note": "includes the host-side allocation of the two outputs per call"}
+
+
 def interp_measurement(dev):
     """Field interpolation (qd_fe_interpolate): one nodal field of the P2
     400x200-cell mesh on 200x100 nm (321,201 nodes) at 16.8M uniformly random
@@ -728,6 +768,10 @@ def main():
                 result["single_dot_c1"] = c1_measurement(dev)
             except Exception as e:   # recorded; the headline line stands
                 result["single_dot_c1"] = {"error": repr(e)}
+            try:
+                result["adjoint_c3"] = c3_measurement(dev)
+            except Exception as e:   # recorded; the headline line stands
+                result["adjoint_c3"] = {"error": repr(e)}
             try:
                 result["field_interpolation"] = interp_measurement(dev)
             except Exception as e:   # recorded; the headline line stands
