@@ -30,10 +30,11 @@ Semantics kept from the C++ classes (SI units in and out):
  - ``FEMSolver.adapt_mesh`` refines the mesh where the eigenvector varies
    fastest (``qdsim_b200.adapt``: the reference's gradient flags, red-green
    refinement) and reassembles on the refined, unstructured mesh.
- - ``potential``, ``effective_mass``, ``epsilon_r`` and ``cap`` are the
-   callbacks of backend/src/physics.cpp the frontend hands to ``FEMSolver``;
-   ``potential`` resamples the electrostatic potential through the
-   ``FEInterpolator`` (one launch for all nodes when given arrays).
+ - ``potential``, ``charge_density``, ``effective_mass``, ``epsilon_r`` and
+   ``cap`` are the callbacks of backend/src/physics.cpp the frontend hands to
+   its solvers; ``potential`` and ``charge_density`` resample nodal fields
+   through the ``FEInterpolator`` (one launch for all points when given
+   arrays).
 Internally the mesh is scaled to nm and energies to eV (c = hbar^2/(2 m*) in
 eV nm^2), as the other drop-in solvers do; eigenvalues come back in J and
 eigenvectors are M-normalised in m^2.
@@ -402,11 +403,7 @@ def potential(x, y, qd_mat, matrix_mat, R, type, phi, interpolator=None):
              if ph.size else 0.0)
     if ph.size and interpolator is not None:
         try:
-            if isinstance(interpolator, FEInterpolator):
-                v_el = np.asarray(interpolator.interpolate_vector(xa, ya, ph), dtype=float)
-            else:
-                v_el = np.array([interpolator.interpolate(a, b, ph) for a, b in zip(xa, ya)],
-                                dtype=float)
+            v_el = _resample(interpolator, xa, ya, ph)
             v_el = np.where(np.abs(v_el) > _MAX_POTENTIAL_EV,
                             np.where(v_el >= 0, _MAX_POTENTIAL_EV, -_MAX_POTENTIAL_EV), v_el)
         except Exception:
@@ -414,6 +411,38 @@ def potential(x, y, qd_mat, matrix_mat, R, type, phi, interpolator=None):
     elif ph.size:
         v_el = np.full_like(xa, first)
     v = v_qd * _PHYS_Q + v_el * _PHYS_Q
+    return float(v[0]) if scalar else v
+
+
+def _resample(interpolator, xa, ya, field):
+    """``field`` at the points through ``interpolator``: one launch for all
+    points with this module's FEInterpolator, point by point otherwise."""
+    if isinstance(interpolator, FEInterpolator):
+        return np.asarray(interpolator.interpolate_vector(xa, ya, field), dtype=float)
+    return np.array([interpolator.interpolate(a, b, field) for a, b in zip(xa, ya)],
+                    dtype=float)
+
+
+def charge_density(x, y, n, p, n_interpolator=None, p_interpolator=None):
+    """q (p - n) at (x, y) (physics.cpp:184-216): each carrier density is
+    resampled through its interpolator, or is its first entry when there is
+    no interpolator (or the interpolation fails), or 0 when empty."""
+    xa, ya = np.asarray(x, dtype=float), np.asarray(y, dtype=float)
+    scalar = xa.ndim == 0
+    xa, ya = np.atleast_1d(xa), np.atleast_1d(ya)
+
+    def density(field, interp):
+        f = np.asarray(field, dtype=float).reshape(-1)
+        if f.size == 0:
+            return np.zeros_like(xa)
+        if interp is not None:
+            try:
+                return _resample(interp, xa, ya, f)
+            except Exception:
+                pass
+        return np.full_like(xa, f[0])
+
+    v = _PHYS_Q * (density(p, p_interpolator) - density(n, n_interpolator))
     return float(v[0]) if scalar else v
 
 
@@ -454,4 +483,4 @@ class EigenSolver:
 
 
 __all__ = ["Mesh", "FEMSolver", "EigenSolver", "FEInterpolator", "AdaptiveMesh", "potential",
-           "effective_mass", "epsilon_r", "cap"]
+           "charge_density", "effective_mass", "epsilon_r", "cap"]

@@ -247,3 +247,27 @@ def test_frontend_complex_interpolation_host_logic():
     assert calls == [(2, mesh.get_num_nodes())] * 3
     with pytest.raises(ValueError):
         fi.interpolate_complex(x, y, z, "phase")
+
+
+def test_frontend_charge_density_callback():
+    """q (p - n) from resampled carrier densities (physics.cpp:184-216), with
+    a stand-in interpolator; first entries without one, 0 when empty."""
+    from qdsim_b200 import frontend as F
+    q = 1.602e-19
+
+    class Stand:
+        def interpolate(self, x, y, field):
+            return field[0] + x
+
+    assert F.charge_density(1.0, 0.0, [2.0, 9.0], [5.0]) == pytest.approx(q * (5.0 - 2.0))
+    assert F.charge_density(1.0, 0.0, [], [5.0]) == pytest.approx(q * 5.0)
+    assert F.charge_density(1.0, 0.0, [], []) == 0.0
+    v = F.charge_density(np.array([0.0, 2.0]), np.zeros(2), [1.0], [3.0], Stand(), Stand())
+    np.testing.assert_allclose(v, q * np.array([(3.0 + 0.0) - (1.0 + 0.0),
+                                                (3.0 + 2.0) - (1.0 + 2.0)]))
+
+    class Broken:
+        def interpolate(self, x, y, field):
+            raise RuntimeError("outside")
+
+    assert F.charge_density(0.5, 0.5, [4.0], [1.0], Broken(), None) == pytest.approx(q * -3.0)
