@@ -271,3 +271,23 @@ def test_frontend_charge_density_callback():
             raise RuntimeError("outside")
 
     assert F.charge_density(0.5, 0.5, [4.0], [1.0], Broken(), None) == pytest.approx(q * -3.0)
+
+
+def test_field_interpolator_rejects_bad_arguments_without_gpu():
+    """FieldInterpolator checks its arguments before any launch."""
+    from qdsim_b200.adapt import refine
+    from qdsim_b200.interp import FieldInterpolator
+    from qdsim_b200.mesh import StructuredMesh
+    m = StructuredMesh(2, 4, 3, 4.0, 3.0)
+    with pytest.raises(ValueError):
+        FieldInterpolator(m, device="cpu", outside="clamp")
+    fi = FieldInterpolator(m, device="cpu")
+    with pytest.raises(ValueError):
+        fi.evaluate([0.5, 1.0], [0.5], np.zeros(m.num_nodes))          # x and y differ
+    with pytest.raises(ValueError):
+        fi.evaluate([0.5], [0.5], np.zeros(m.num_nodes - 1))           # wrong field length
+    with pytest.raises(ValueError):
+        fi.evaluate([0.5], [0.5], np.zeros((2, 3, m.num_nodes)))       # not (N,) or (F, N)
+    tm = refine(m, np.ones(m.num_elements, bool))
+    with pytest.raises(NotImplementedError):
+        FieldInterpolator(tm, device="cpu")                            # needs the lattice
