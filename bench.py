@@ -376,7 +376,7 @@ def interp_measurement(dev):
     with gradients and elements, the field once).  Beside it a size-independent
     check: a quadratic field is reproduced exactly by the P2 interpolant."""
     import torch
-    from qdsim_b200 import kernels_bench as KB
+    import kernels_bench as KB
     from qdsim_b200.interp import FieldInterpolator
     from qdsim_b200.mesh import StructuredMesh
     peak = FALLBACK_HBM

@@ -1,8 +1,8 @@
 """Run one kernel family on a named workload and report its CUDA-event time.
 
-    python -m qdsim_b200.kernels_bench cap_spmm [--prec fp64|fp32] [--b 48] [--launches 10]
-    python -m qdsim_b200.kernels_bench pcg [--iters 32]
-    python -m qdsim_b200.kernels_bench interp [--points 16777216] [--gradient] [--sorted]
+    python kernels_bench.py cap_spmm [--prec fp64|fp32] [--b 48] [--launches 10]
+    python kernels_bench.py pcg [--iters 32]
+    python kernels_bench.py interp [--points 16777216] [--gradient] [--sorted]
 
 ``cap_spmm``: ``qd_cap_spmm`` on the open-system pencil of P2 400x200 cells on
 200x100 nm (318,801 DOFs, 3.65M nonzeros) for a block of b complex columns;
@@ -21,14 +21,18 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
+import sys
 
 import numpy as np
 import torch
 
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
 
 def cap_spmm(prec: str, b: int, launches: int, dev):
-    from .cap import CAPProblem
-    from .workloads import c2_dot
+    from qdsim_b200.cap import CAPProblem
+    from qdsim_b200.workloads import c2_dot
     d = c2_dot(0)
     prob = CAPProblem(d.mesh, d.c, d.V, d.W, device=dev)
     ct, s = (torch.complex64, 4) if prec == "fp32" else (torch.complex128, 8)
@@ -51,9 +55,9 @@ def cap_spmm(prec: str, b: int, launches: int, dev):
 
 
 def pcg(iters: int, dev):
-    from . import _native as N
-    from .poisson import PoissonProblem
-    from .workloads import c5_junction
+    from qdsim_b200 import _native as N
+    from qdsim_b200.poisson import PoissonProblem
+    from qdsim_b200.workloads import c5_junction
     j = c5_junction(64)
     prob = PoissonProblem(j.mesh, j.eps_r, device=dev)
     rng = np.random.default_rng(0)
@@ -80,8 +84,8 @@ def pcg(iters: int, dev):
 
 
 def interp(points: int, gradient: bool, ordered: bool, launches: int, dev):
-    from .interp import FieldInterpolator
-    from .mesh import StructuredMesh
+    from qdsim_b200.interp import FieldInterpolator
+    from qdsim_b200.mesh import StructuredMesh
     m = StructuredMesh(2, 400, 200, 200.0, 100.0)
     g = torch.Generator(device=dev).manual_seed(0)
     x = torch.rand(points, generator=g, device=dev, dtype=torch.float64) * m.Lx

@@ -11,6 +11,8 @@ poisson_solver.pyx emits ``#include "Eigen/Dense"`` for a cimport it never
 uses; empty stub headers stand in for Eigen.
 
 Usage: python oracle/build_ref.py [reference_root]
+The reference root comes from the argument, else the QDSIM_REFERENCE_ROOT
+environment variable, else the location this recipe was written for.
 """
 import os
 import sys
@@ -30,6 +32,11 @@ MODULES = [
 ]
 
 
+def default_root() -> str:
+    """Reference tree: $QDSIM_REFERENCE_ROOT, else the recipe's default."""
+    return os.environ.get("QDSIM_REFERENCE_ROOT", "/root/reference")
+
+
 def _so(short):
     hits = sorted(OUT.rglob(f"{short}*.so"))
     return hits[0] if hits else None
@@ -39,9 +46,9 @@ def built() -> bool:
     return all(_so(short) is not None for short, _, _ in MODULES)
 
 
-def build(ref_root: str = "/root/reference", quiet: bool = True) -> bool:
+def build(ref_root: str | None = None, quiet: bool = True) -> bool:
     """Compile the modules; returns False if the reference tree is absent."""
-    ref = Path(ref_root)
+    ref = Path(ref_root or default_root())
     if not (ref / "qdsim_cython").is_dir():
         return False
     import numpy
@@ -87,6 +94,6 @@ def import_ref(short: str):
 
 
 if __name__ == "__main__":
-    ok = build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", quiet=False)
+    ok = build(sys.argv[1] if len(sys.argv) > 1 else None, quiet=False)
     print("reference modules built:" if ok else "reference not found", OUT)
     sys.exit(0 if ok else 1)

@@ -93,6 +93,19 @@ def boundary_nodes(nodes, Lx, Ly):
     return (np.abs(x) < 1e-12) | (np.abs(x - Lx) < 1e-12) | (np.abs(y) < 1e-12) | (np.abs(y - Ly) < 1e-12)
 
 
+def replace_boundary_rows(A, fixed):
+    """The reference's Dirichlet treatment of CythonSchrodingerSolver
+    (qdsim_cython/solvers/schrodinger_solver.pyx:253-283): every boundary row
+    of H and of M becomes the identity row (row zeroed, diagonal 1)."""
+    L = A.tolil()
+    for i in np.where(fixed)[0]:
+        L[i, :] = 0
+        L[i, i] = 1
+    out = L.tocsr()
+    out.sort_indices()
+    return out
+
+
 def eig_free_sm(H, M, fixed, k):
     """The k eigenvalues of smallest magnitude (the reference calls
     eigsh(..., which='SM'), schrodinger_solver.pyx:447-453) of the physical

@@ -68,8 +68,9 @@ class _Mesh:
         return self._m.elems.tolist()
 
 
-def main(ref_root="/root/reference"):
-    FEI = _load_reference(Path(ref_root))
+def main(ref_root=None):
+    from oracle.build_ref import default_root
+    FEI = _load_reference(Path(ref_root or default_root()))
     m = structured_mesh(1, NX, NY, LX, LY)
     it = FEI(_Mesh(m), use_cpp=False)
     rng = np.random.default_rng(SEED)

@@ -8,7 +8,12 @@ Cases (SI units, as the reference uses them):
   fixed     FixedOpenSystemSolver(11, 7, 100e-9, 60e-9, m*, V)
             ._assemble_matrices_robust() CSR of H and M, and solve(4)
   cython    CythonSchrodingerSolver on SimpleMesh(9, 6, 8e-6, 5e-6) (micrometre
-            cells, so its 1e-15 m^2 area test keeps every element): solve(4)
+            cells, so its 1e-15 m^2 area test keeps every element): solve(4),
+            and the CSR of the H and M that solve() hands to eigsh (the
+            assembled pencil after the boundary-row replacement; the class
+            keeps them private, so they are captured at that call by giving
+            the module a scipy.sparse.linalg stand-in whose eigsh records its
+            arguments and then runs scipy's)
   poisson   CythonPoissonSolver on SimpleMesh(9, 6, 8e-6, 5e-6): stiffness and
             mass CSR, solve(0.0, 0.5) potential and electric field
 """
@@ -82,7 +87,25 @@ def main():
 
     um = mm.SimpleMesh(9, 6, 8e-6, 5e-6)
     cs = ss.CythonSchrodingerSolver(um, m_func_um, v_func_um)
-    E, _ = cs.solve(4)
+    captured = {}
+    real_spla = ss.spla
+
+    class _RecordingLinalg:
+        def __getattr__(self, name):
+            return getattr(real_spla, name)
+
+        def eigsh(self, A, *args, **kw):
+            captured.setdefault("H", A.copy())
+            captured.setdefault("M", kw["M"].copy())
+            return real_spla.eigsh(A, *args, **kw)
+
+    ss.spla = _RecordingLinalg()
+    try:
+        E, _ = cs.solve(4)
+    finally:
+        ss.spla = real_spla
+    csr_parts("cython_H", captured["H"], out)
+    csr_parts("cython_M", captured["M"], out)
     out["cython_E"] = np.sort(np.real(E))
     out["cython_nnz"] = cs.get_matrix_info()["hamiltonian_nnz"]
 

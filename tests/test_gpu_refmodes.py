@@ -66,6 +66,26 @@ def test_ref_cython_mode_matches_oracle(cuda):
     assert _rel(prob.to_scipy(out["M"]), Mr) < 1e-12
 
 
+def test_ref_cython_mode_matches_compiled_reference(cuda):
+    """GPU assembly in the Cython solver's element formulas, with the
+    reference's boundary-row replacement applied on the host, equals the H and
+    M the compiled CythonSchrodingerSolver passes to eigsh (fixture captured
+    from the compiled module) at 1e-12."""
+    from qdsim_b200 import _native as N, fem as F, mesh as Mh
+    m = Mh.StructuredMesh(1, 8, 5, 8e-6, 5e-6)
+    c, V = _elem_inputs(m, v_um)
+    prob = F.FEMProblem(m, dirichlet=False, device=cuda)
+    out = prob.assemble(c, V, mode=N.QD_ASM_REF_CYTHON)
+    fixed = RC.boundary_nodes(m.nodes, 8e-6, 5e-6)
+    H = RC.replace_boundary_rows(prob.to_scipy(out["H"]), fixed)
+    M = RC.replace_boundary_rows(prob.to_scipy(out["M"]), fixed)
+    n = m.num_nodes
+    Hr, Mr = _csr("cython_H", n), _csr("cython_M", n)
+    assert np.array_equal(H.indices, Hr.indices) and np.array_equal(M.indices, Mr.indices)
+    assert _rel(H, Hr) < 1e-12
+    assert _rel(M, Mr) < 1e-12
+
+
 def test_poisson_stiffness_matches_compiled_reference(cuda):
     from qdsim_b200 import mesh as Mh, poisson as P
     m = Mh.StructuredMesh(1, 8, 5, 8e-6, 5e-6)
