@@ -343,21 +343,29 @@ int qd_fe_interpolate(int order, int32_t nx, int32_t ny, double Lx, double Ly, i
                       double *d_grad_y, int32_t *d_element, int outside_zero, void *stream);
 
 /* ---------------------------------------------------------------------------
- * Adjoint (Hellmann-Feynman) gradients of L = sum_s w_s E_s with respect to
- * nodal V and the per-element kinetic coefficient c.  With M-normalised
- * eigenvectors, dE_s/dV_l = psi_s^T (dH/dV_l) psi_s and
- * dE_s/dc_e = psi_s^T K_e psi_s / c_e (M depends on neither).  No reference
- * counterpart: the reference has no derivatives; the checker is central finite
- * differences of the FP64 eigenvalues.
- *   d_psi        double[n_dofs * n_states] row-major (psi[dof*n_states + s])
- *   d_w          double[n_states] weights
+ * Adjoint (Hellmann-Feynman) gradients of L = Re sum_s w_s E_s with respect
+ * to nodal V and the per-element kinetic coefficient c.  M depends on neither,
+ * so with normalised eigenvectors dE_s/dp = x_s^T (dH/dp) x_s:
+ *   - Hermitian pencil (is_complex = 0): real x_s with x^T M x = 1;
+ *   - complex-symmetric open-system pencil H + i Himag (is_complex = 1):
+ *     complex x_s with the bilinear normalisation x^T M x = 1 (no
+ *     conjugation; the left eigenvector of a complex-symmetric pencil is x
+ *     itself), complex weights w_s = dL/dRe E_s - i dL/dIm E_s.
+ * No reference counterpart: the reference has no derivatives (its CAP pencil
+ * is solved densely in backend/src/schrodinger.cpp:699-818, with the
+ * (V + i eta) weak form of backend/src/fem.cpp:970-976); the checker is central
+ * finite differences of the FP64 eigenvalues and the FP64 oracle gradient.
+ *   d_psi        is_complex = 0: double[n_dofs * n_states] (psi[dof*n_states + s]);
+ *                is_complex = 1: interleaved (re, im) pairs, 16-byte aligned
+ *   d_w          double[n_states] (real) or [2 * n_states] (re, im per state)
  *   d_nadjptr/d_nadj  node adjacency from qd_node_adjacency
- *   d_dofmap     int32[num_nodes]
- *   outputs      d_dLdV[num_nodes], d_dLdc[num_elems]
+ *   d_dofmap     int32[num_nodes] (-1 for an eliminated node: psi = 0 there)
+ *   outputs      d_dLdV[num_nodes], d_dLdc[num_elems] (caller-allocated)
+ * One launch; every output is a fixed-order sum (reproducible, no atomics).
  * ------------------------------------------------------------------------- */
-int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states,
+int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states, int is_complex,
                const double *d_nodes, const int32_t *d_elems, const int32_t *d_dofmap,
-               const double *d_c, const double *d_psi, const double *d_w,
+               const double *d_psi, const double *d_w,
                const int32_t *d_nadjptr, const int32_t *d_nadj,
                double *d_dLdV, double *d_dLdc, void *stream);
 
@@ -372,6 +380,23 @@ int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states,
  * ------------------------------------------------------------------------- */
 int qd_prof_enable(int on);
 int qd_prof_read(double *ms, int64_t *launches, int reset);
+
+/* ---------------------------------------------------------------------------
+ * Failure-path diagnostic with no reference counterpart (the reference's GPU
+ * code has no device-side waits; its failure handling is the host-side
+ * RecoveryManager of backend/include/recovery_manager.h:47, which returns
+ * dummy eigenpairs from backend/src/solver.cpp:183-192).  Runs the bounded
+ * mbarrier wait that every bulk-copy pipeline of this library uses on a
+ * barrier that nothing completes, with a limit of limit_ns (capped at 2 s):
+ * the wait expires, the kernel records it in *d_status (bit 0), drains its own
+ * 256-byte bulk copy from d_src when with_copy != 0 (16-byte aligned; bit 1 if
+ * that drain also expired, bit 2 if the copied bytes differ) and returns.
+ * Synchronises `stream`; *h_status receives the status word.  Returns
+ * QD_ERR_TIMEOUT when the wait expired (the expected outcome), the status
+ * production entry points return after such an expiry.
+ * ------------------------------------------------------------------------- */
+int qd_bounded_wait_selftest(int64_t limit_ns, const void *d_src, int with_copy,
+                             int32_t *d_status, int32_t *h_status, void *stream);
 
 #ifdef __cplusplus
 }

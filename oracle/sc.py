@@ -116,9 +116,12 @@ def mix(old, upd, hist_u, hist_r, beta, anderson):
     return old + beta * (upd - old)
 
 
-def run(junction, k, iterations, V_p=None, damping=0.3, anderson_start=5, history=3, phi0=None):
+def run(junction, k, iterations, V_p=None, damping=0.3, anderson_start=5, history=3, phi0=None,
+        on_iter=None):
     """The mixed fixed-point iteration for every bias point of ``junction``;
-    returns phi [N, nb], errors [iterations, nb], E [nb, k] of the last map."""
+    returns phi [N, nb], errors [iterations, nb], E [nb, k] of the last map.
+    ``on_iter(it, phi, E)`` (optional) sees each iteration's mixed potential
+    and the levels of its map."""
     j = junction
     mesh = j.mesh
     nb = len(j.biases)
@@ -153,4 +156,6 @@ def run(junction, k, iterations, V_p=None, damping=0.3, anderson_start=5, histor
             prev[b] = err[b]
         phi = new
         errors.append(err)
+        if on_iter is not None:
+            on_iter(it, phi, E)
     return phi, np.array(errors), E

@@ -108,3 +108,25 @@ def test_cap_solver_tends_to_hermitian_levels(cuda, w_scale):
     else:
         assert (-res.E.imag).max() <= W.max() and (-res.E.imag).min() >= -1e-3 * W.max()
         assert (np.abs(got - near) / np.abs(near)).max() <= 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cap_nearest20_at_config_size(cuda, precision):
+    """The open-system configuration at its stated size (P2 400x200 cells on
+    200x100 nm, 318,801 DOFs, CAP -i 50 meV (d/10 nm)^2 in a 10 nm layer):
+    the 20 eigenvalues nearest -0.05 eV against the oracle's shift-invert
+    eigs on the same pencil (tests/golden/c2_nearest20.npz, made by
+    tests/golden/make_c2_golden.py), 1e-9 relative, certified complete, with
+    x^T M x = 1 and small residuals."""
+    import os
+    from qdsim_b200 import cap as CP
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                "c2_nearest20.npz"))["E"]
+    d = _c2(400, 200)
+    res = CP.CAPSolver(d.mesh, d.c, d.V, d.W, device=cuda).solve(
+        k=20, sigma=-0.05, nev=40, b=48, precision=precision, tol=1e-9)
+    assert res.info["complete"], res.info
+    err = np.array([np.min(np.abs(res.E - g)) / abs(g) for g in gold])
+    assert err.max() <= 1e-9, (err.max(), res.info)
+    assert len({int(np.argmin(np.abs(res.E - g))) for g in gold}) == 20
+    assert res.residual.max() < 1e-8, res.residual.max()

@@ -50,3 +50,52 @@ def test_sc_implicit_bias_derivative(cuda):
         fd.append((Es[0] - Es[1]) / (2 * d))
     fd = np.array(fd)
     assert np.allclose(dE, fd, rtol=2e-3, atol=1e-6), (dE, fd)
+
+
+def _c5_pair():
+    import os
+    from qdsim_b200 import workloads as W
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c5_sc.npz"))
+    j = W.c5_junction(64)
+    return dataclasses.replace(j, biases=j.biases[z["bias_idx"]]), z
+
+
+def test_sc_loop_matches_restatement_at_config_size(cuda):
+    """The junction at its stated size (P1 300x100 cells, 10 states, 40
+    iterations: damping, then Anderson with the line search) for the lowest
+    and the highest of the 64 seeded bias points, FP64 eigensolves and PCG,
+    against the FP64 restatement's run (tests/golden/c5_sc.npz, made by
+    tests/golden/make_c5_golden.py): the error of every iteration, the final
+    potential and the levels of the last map.  The eigensolves run far past
+    the eigenvalue target (tol 1e-20 on the quadratic estimate) so that the
+    densities, which depend on the eigenvectors to first order, follow the
+    restatement's to ~1e-9 over all 40 iterations."""
+    from qdsim_b200.sc import BatchedSC
+    j, z = _c5_pair()
+    sc = BatchedSC(j, k=10, device=cuda, precision="fp64", tol=1e-20, pcg_tol=1e-14)
+    phi, err = sc.solve(iterations=40)
+    err = err.cpu().numpy()
+    assert np.allclose(err, z["errors"], rtol=1e-3, atol=0), np.abs(err / z["errors"] - 1).max()
+    st = int(z["stride"])
+    phi = phi.cpu().numpy()[::st]
+    assert np.abs(phi - z["phi"]).max() <= 1e-7 * np.abs(z["phi"]).max()
+    assert np.allclose(sc.E.cpu().numpy(), z["E"], rtol=1e-10, atol=0)
+
+
+def test_sc_loop_mixed_precision_at_config_size(cuda):
+    """The same two bias points with the configuration's own solver settings
+    (mixed-precision eigensolves to 1e-9, PCG to 1e-12): the potential after
+    40 iterations within 1e-3 of the FP64 restatement's (normwise), the
+    levels within 1e-4, and the first eight iterations' errors within 1 %
+    (later errors fall below the eigenvector error the 1e-9 eigenvalue target
+    leaves, so they are not compared)."""
+    from qdsim_b200.sc import BatchedSC
+    j, z = _c5_pair()
+    sc = BatchedSC(j, k=10, device=cuda)
+    phi, err = sc.solve(iterations=40)
+    err = err.cpu().numpy()
+    assert np.allclose(err[:8], z["errors"][:8], rtol=1e-2, atol=0)
+    st = int(z["stride"])
+    phi = phi.cpu().numpy()[::st]
+    assert np.linalg.norm(phi - z["phi"]) <= 1e-3 * np.linalg.norm(z["phi"])
+    assert np.allclose(sc.E.cpu().numpy(), z["E"], rtol=1e-4, atol=0)
