@@ -693,9 +693,8 @@ def main():
         cfg["block"] = args.block
     args.block = int(cfg["block"])
     db.set_shift(cfg["shift_ev"])
-    solve_kw = dict(b=args.block, precision=args.precision, tol=args.tol,
-                    max_iter=args.max_iter, tol32=cfg["tol32"],
-                    stag_window=cfg["stag_window"])
+    solve_kw = dict(AT.solve_kwargs(cfg, args.tol, args.precision, args.max_iter),
+                    b=args.block)
 
     def step():
         db.assemble()

@@ -167,9 +167,8 @@ typedef struct {
  * The initial block is drawn from `seed` (deterministic).  Returns
  * QD_ERR_NOT_CONVERGED if any dot hits max_iter (results still written).
  * ------------------------------------------------------------------------- */
-int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_total, int b,
-                             int prec_mode, const qd_dst_prec *h_prec, size_t *bytes);
-/* Solver options (pass NULL for the defaults):
+/* Solver options (pass NULL for the defaults; the same options to the
+ * workspace query and the solve):
  *   tol32        estimate at which a dot leaves the FP32 phase (<= 0: max(100 tol, 1e-7))
  *   stag_window  FP32 iterations without halving the estimate before a dot
  *                switches to FP64 anyway (<= 0: 12)
@@ -180,14 +179,23 @@ int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_t
  *                self-consistent iteration's eigenvectors); NULL: random
  *   eig_scale    energy below which eigenvalue errors are measured absolutely:
  *                the estimate divides by max(|t|, eig_scale) instead of |t|
- *                (levels near zero energy); <= 0: purely relative */
+ *                (levels near zero energy); <= 0: purely relative
+ *   chunk_rows   rows per chunk, the CTA unit of every row-parallel kernel
+ *                (SpMM, Gram, orthogonalisation, update) and of the per-chunk
+ *                partial sums; a multiple of 64 in [256, 8192], else 1024 */
 typedef struct {
   double tol32;
   int32_t stag_window;
   int32_t graphs;
   const double *x0;
   double eig_scale;
+  int32_t chunk_rows;
+  int32_t reserved;
 } qd_lobpcg_opts;
+
+int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_total, int b,
+                             int prec_mode, const qd_dst_prec *h_prec,
+                             const qd_lobpcg_opts *opts, size_t *bytes);
 
 int qd_lobpcg_solve(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_row_off,
                     const int32_t *d_rowptr, const int32_t *d_col,
@@ -261,7 +269,10 @@ int qd_sc_mix(int32_t nb, int64_t n_nodes, int anderson, int nhist, const double
  *                the free rows, x_D = the initial X with its free entries
  *                zeroed (the Dirichlet values alone): a warm start X lowers
  *                the work, not the target; h_relres reports the same ratio
- *   h_iters/h_relres  host outputs: iterations used, final max relative residual
+ *   h_iters/h_relres  host outputs: iterations launched (the host checks
+ *                convergence every 16 iterations, so this is the CG iteration
+ *                count rounded up to a multiple of 16, or max_iter), final max
+ *                relative residual
  * ------------------------------------------------------------------------- */
 int qd_pcg_workspace_size(int32_t n, int nrhs, size_t *bytes);
 int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_col,
@@ -283,7 +294,12 @@ int qd_pcg_solve(int32_t n, int nrhs, const int32_t *d_rowptr, const int32_t *d_
  *     larger problems return QD_ERR_LIMIT without launching anything.
  *   - The first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress, with that device current); make that first call
- *     before any stream capture.
+ *     before any stream capture.  Under CUDA's default lazy module loading
+ *     that lookup is also what loads this code's module on the device, and
+ *     so what reserves the 16 MiB there: a caller inside a runtime that owns
+ *     all device memory should make the first call during its own set-up,
+ *     while memory is still free.  The address is cached per device for the
+ *     life of the process; cudaDeviceReset between calls is not supported.
  *   - All calls share the one array and it keeps the previous call's
  *     contents; each call zeroes its block counter (a memset on the stream)
  *     and rewrites every other scratch word before reading it, so nothing
@@ -361,13 +377,15 @@ int qd_fe_interpolate(int order, int32_t nx, int32_t ny, double Lx, double Ly, i
  *   d_nadjptr/d_nadj  node adjacency from qd_node_adjacency
  *   d_dofmap     int32[num_nodes] (-1 for an eliminated node: psi = 0 there)
  *   outputs      d_dLdV[num_nodes], d_dLdc[num_elems] (caller-allocated)
- * One launch; every output is a fixed-order sum (reproducible, no atomics).
+ *   d_work       scratch, double[num_elems * k] (k = 3, 6, 10 nodes per element)
+ * Two launches (element pass, node gather); every output is a fixed-order
+ * sum (reproducible, no atomics).
  * ------------------------------------------------------------------------- */
 int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n_states, int is_complex,
                const double *d_nodes, const int32_t *d_elems, const int32_t *d_dofmap,
                const double *d_psi, const double *d_w,
                const int32_t *d_nadjptr, const int32_t *d_nadj,
-               double *d_dLdV, double *d_dLdc, void *stream);
+               double *d_dLdV, double *d_dLdc, double *d_work, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Per-kernel-kind timing with CUDA events, recorded on the stream of each

@@ -46,7 +46,7 @@ SIGNATURES = {
     "qd_assemble": (_int, [_int, _int, _i64, _i64, _i32, _p, _p, _p, _p, _p,
                            _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_spmm_dual": (_int, [_i32, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p]),
-    "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _i64, _int, _int, _p, _p]),
+    "qd_lobpcg_workspace_size": (_int, [_i32, _i64, _i64, _int, _int, _p, _p, _p]),
     "qd_lobpcg_solve": (_int, [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _int, _int, _int, _dbl,
                                _int, _u64, _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p]),
     "qd_dst_precond_workspace_size": (_int, [_i32, _p, _int, _p, _p]),
@@ -70,7 +70,7 @@ SIGNATURES = {
                              _p, _p]),
     "qd_sc_mix": (_int, [_i32, _i64, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_adjoint": (_int, [_int, _i64, _i64, _int, _int, _p, _p, _p, _p, _p, _p, _p,
-                          _p, _p, _p]),
+                          _p, _p, _p, _p]),
 }
 
 
@@ -84,8 +84,9 @@ assert DST_PREC_DTYPE.itemsize == 40
 # struct qd_lobpcg_opts (include/qdsim_b200.h)
 LOBPCG_OPTS_DTYPE = _np.dtype([("tol32", _np.float64), ("stag_window", _np.int32),
                                ("graphs", _np.int32), ("x0", _np.uint64),
-                               ("eig_scale", _np.float64)], align=True)
-assert LOBPCG_OPTS_DTYPE.itemsize == 32
+                               ("eig_scale", _np.float64), ("chunk_rows", _np.int32),
+                               ("reserved", _np.int32)], align=True)
+assert LOBPCG_OPTS_DTYPE.itemsize == 40
 
 
 class QDError(RuntimeError):

@@ -83,24 +83,27 @@ def cluster_weights(E, w, degenerate_rtol=1e-8, E_next=None):
 
 
 class _Outputs:
-    """Preallocated gradient arrays of one problem (reused between calls)."""
+    """Preallocated gradient arrays and the element-pass scratch of one
+    problem (reused between calls)."""
 
     def __init__(self):
         self.key = None
-        self.dV = self.dc = None
+        self.dV = self.dc = self.work = None
 
     def get(self, m, dev):
         key = (m.num_nodes, m.num_elements, str(dev))
         if self.key != key:
             self.dV = torch.empty(m.num_nodes, dtype=torch.float64, device=dev)
             self.dc = torch.empty(m.num_elements, dtype=torch.float64, device=dev)
+            self.work = torch.empty(m.elems.size, dtype=torch.float64, device=dev)
             self.key = key
-        return self.dV, self.dc
+        return self.dV, self.dc, self.work
 
 
 def energy_gradients(prob: FEMProblem, psi_reduced: torch.Tensor, weights, stream=None,
                      out=None):
-    """dL/dV (nodal) and dL/dc (per element) on the device, one launch.
+    """dL/dV (nodal) and dL/dc (per element) on the device (an element pass
+    and a node gather).
 
     ``psi_reduced``: [n_dofs, ns] real (Hermitian pencil, M-normalised) or
     complex (complex-symmetric pencil, x^T M x = 1); ``weights``: ns real or
@@ -124,16 +127,15 @@ def energy_gradients(prob: FEMProblem, psi_reduced: torch.Tensor, weights, strea
     wt = torch.as_tensor(wv, dtype=torch.float64, device=dev)
     nptr, nadj = prob.node_adjacency()
     m = prob.mesh
-    if out is None:
-        if not hasattr(prob, "_adj_out"):
-            prob._adj_out = _Outputs()
-        dV, dc = prob._adj_out.get(m, dev)
-    else:
+    if not hasattr(prob, "_adj_out"):
+        prob._adj_out = _Outputs()
+    dV, dc, work = prob._adj_out.get(m, dev)
+    if out is not None:
         dV, dc = out
     N.check(N.lib().qd_adjoint(m.order, m.num_nodes, m.num_elements, ns, 1 if cplx else 0,
                                N.ptr(prob.d_nodes), N.ptr(prob.d_elems), N.ptr(prob.d_dofmap),
                                N.ptr(psi), N.ptr(wt), N.ptr(nptr), N.ptr(nadj), N.ptr(dV),
-                               N.ptr(dc), stream_ptr(stream)), "qd_adjoint")
+                               N.ptr(dc), N.ptr(work), stream_ptr(stream)), "qd_adjoint")
     return dV, dc
 
 

@@ -1,11 +1,17 @@
 """Autotuner for the batched eigensolve.
 
-Picks, for one batch of dots, the LOBPCG block size, the DST preconditioner
-shift and the FP32 -> FP64 hand-over of the mixed mode (FP32 target and
-stagnation window) by timing solves of the batch itself on the GPU.  The
-search is coordinate descent over a small candidate set (one parameter at a
-time, the others fixed at the best values found so far); a configuration only
-counts if every dot converges.  Results are cached in a JSON file keyed by the
+Picks, for one batch of dots, the kernels' tile parameters and the solver's
+parameters by timing solves of the batch itself on the GPU:
+ - ``chunk_rows``: rows per CTA of every row-parallel kernel (SpMM, Gram,
+   orthogonalisation, update), which also sets how many per-chunk partial
+   sums the reductions add up;
+ - ``block``: the LOBPCG block width B, the vector-row width every kernel is
+   compiled for (B / 4 threads per row in the SpMMs, the Gram tile grid);
+ - ``shift_ev``: the DST preconditioner's shift;
+ - ``tol32`` / ``stag_window``: the FP32 -> FP64 hand-over of the mixed mode.
+The search is coordinate descent over a small candidate set (one parameter at
+a time, the others fixed at the best values found so far); a configuration
+only counts if every dot converges.  Results are cached in a JSON file keyed by the
 GPU name and a signature of the batch (dot sizes, nonzeros, k, tolerance), so
 a later run of the same batch shape reads the tuned values instead of
 re-tuning.
@@ -25,13 +31,23 @@ from pathlib import Path
 import numpy as np
 
 DEFAULT_CACHE = Path(__file__).resolve().parent / "tuned.json"
-DEFAULTS = {"block": 12, "shift_ev": 0.02, "stag_window": 12, "tol32": 1e-7}
+DEFAULTS = {"block": 12, "shift_ev": 0.02, "stag_window": 12, "tol32": 1e-7,
+            "chunk_rows": 1024}
 SPACE = {
+    "chunk_rows": [512, 1024, 2048, 4096],
     "shift_ev": [0.01, 0.02, 0.04],
     "block": [12, 16],
     "stag_window": [8, 12, 20],
     "tol32": [3e-8, 1e-7, 3e-7],
 }
+ORDER = ("chunk_rows", "shift_ev", "block", "stag_window", "tol32")
+
+
+def solve_kwargs(cfg, tol, precision="mixed", max_iter=4000):
+    """Keyword arguments of ``DeviceBatch.solve`` for a configuration."""
+    return dict(b=int(cfg["block"]), precision=precision, tol=tol, max_iter=max_iter,
+                tol32=cfg["tol32"], stag_window=cfg["stag_window"],
+                chunk_rows=int(cfg.get("chunk_rows", DEFAULTS["chunk_rows"])))
 
 
 def signature(host_batch, k: int, tol: float, gpu_name: str) -> str:
@@ -47,22 +63,22 @@ def _gpu_name(device) -> str:
     return torch.cuda.get_device_name(device)
 
 
-def load(host_batch, k: int, tol: float, device="cuda", cache=DEFAULT_CACHE):
-    """Tuned configuration for this batch shape on this GPU, or None."""
+def load(host_batch, k: int, tol: float, device="cuda", cache=DEFAULT_CACHE, gpu_name=None):
+    """Tuned configuration for this batch shape on this GPU, or None (entries
+    from before a parameter existed get that parameter's default)."""
     try:
         with open(cache) as f:
             entries = json.load(f)
     except (OSError, ValueError):
         return None
-    e = entries.get(signature(host_batch, k, tol, _gpu_name(device)))
-    return dict(e["config"]) if e else None
+    e = entries.get(signature(host_batch, k, tol, gpu_name or _gpu_name(device)))
+    return dict(DEFAULTS, **e["config"]) if e else None
 
 
 def _time_solve(db, k, tol, cfg, repeats):
     import torch
     db.set_shift(cfg["shift_ev"])
-    kw = dict(b=cfg["block"], precision="mixed", tol=tol, max_iter=4000,
-              tol32=cfg["tol32"], stag_window=cfg["stag_window"])
+    kw = solve_kwargs(cfg, tol)
     db.solve(k, **kw)                     # warm (workspace, graphs)
     torch.cuda.synchronize()
     best = None
@@ -79,32 +95,49 @@ def _time_solve(db, k, tol, cfg, repeats):
     return best, converged
 
 
-def tune(host_batch, k: int = 8, tol: float = 1e-9, device="cuda", space=None, repeats=2,
-         cache=DEFAULT_CACHE, verbose=False):
-    """Coordinate-descent search; returns (config, trace) and updates the cache."""
-    from .batch import DeviceBatch
+def search(timer, space=None, start=None, verbose=False):
+    """Coordinate descent: ``timer(cfg) -> (ms, converged)``; returns (best
+    config, best ms, trace).  Parameters are visited in ORDER; a candidate
+    replaces the best only if it converged and is faster."""
     space = space or SPACE
-    db = DeviceBatch(host_batch, device)
-    db.upload(non_blocking=False)
-    db.assemble()
-    best = dict(DEFAULTS)
-    best_ms, ok = _time_solve(db, k, tol, best, repeats)
+    best = dict(start or DEFAULTS)
+    best_ms, ok = timer(best)
     trace = [{"config": dict(best), "ms": best_ms, "converged": ok}]
+    seen = {tuple(sorted(best.items()))}
     if not ok:
         best_ms = float("inf")
-    for name in ("shift_ev", "block", "stag_window", "tol32"):
-        for value in space[name]:
-            if value == best[name]:
-                continue
+    for name in ORDER:
+        for value in space.get(name, []):
             cand = dict(best)
             cand[name] = value
-            ms, ok = _time_solve(db, k, tol, cand, repeats)
+            key = tuple(sorted(cand.items()))
+            if key in seen:           # timed already (e.g. the value best started from)
+                continue
+            seen.add(key)
+            ms, ok = timer(cand)
             trace.append({"config": dict(cand), "ms": ms, "converged": ok})
             if verbose:
                 print(f"  {name}={value}: {ms:.1f} ms{'' if ok else ' (not converged)'}", flush=True)
             if ok and ms < best_ms:
                 best, best_ms = cand, ms
-    entry = {"config": best, "ms": best_ms, "gpu": _gpu_name(device), "k": k, "tol": tol,
+    return best, best_ms, trace
+
+
+def tune(host_batch, k: int = 8, tol: float = 1e-9, device="cuda", space=None, repeats=2,
+         cache=DEFAULT_CACHE, verbose=False, timer=None, gpu_name=None):
+    """Coordinate-descent search; returns (config, trace) and updates the
+    cache.  ``timer`` replaces the GPU timing (tests)."""
+    if timer is None:
+        from .batch import DeviceBatch
+        db = DeviceBatch(host_batch, device)
+        db.upload(non_blocking=False)
+        db.assemble()
+
+        def timer(cfg):
+            return _time_solve(db, k, tol, cfg, repeats)
+    gpu = gpu_name or _gpu_name(device)
+    best, best_ms, trace = search(timer, space, verbose=verbose)
+    entry = {"config": best, "ms": best_ms, "gpu": gpu, "k": k, "tol": tol,
              "n_dots": host_batch.n_dots, "rows": int(host_batch.n), "nnz": int(host_batch.nnz),
              "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()), "trace": trace}
     entries = {}
@@ -113,7 +146,7 @@ def tune(host_batch, k: int = 8, tol: float = 1e-9, device="cuda", space=None, r
             entries = json.load(f)
     except (OSError, ValueError):
         pass
-    entries[signature(host_batch, k, tol, _gpu_name(device))] = entry
+    entries[signature(host_batch, k, tol, gpu)] = entry
     os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
     with open(cache, "w") as f:
         json.dump(entries, f, indent=1)

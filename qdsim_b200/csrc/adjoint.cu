@@ -12,13 +12,14 @@
 // with the assembly kernel's reference tables (T_lij = int phi_l phi_i phi_j
 // on the reference triangle).
 //
-// One launch, persistent blocks.  A group of GS lanes (8 / 16 / 32 for
-// P1 / P2 / P3) takes one unit at a time: an element (its dL/dc) or a node
-// (its dL/dV, summed over the node's incident elements in adjacency order,
-// so the result is reproducible without atomics).  The group stages the
-// element's K x n_states amplitudes in shared memory; each lane owns a few of
-// the K^2 (i, j) pairs, forms U_ij and its contribution, and the group sums
-// by shuffles.  No reference counterpart (the reference has no derivatives);
+// Two launches.  The element pass gives each element to a group of GS lanes
+// (8 / 16 / 32 for P1 / P2 / P3, persistent blocks): the group stages the
+// element's K x n_states amplitudes in shared memory, each lane owns a few of
+// the K^2 (i, j) pairs and forms U_ij and its contributions, and the group
+// sums by shuffles into dL/dc_e and the element's K nodal contributions
+// (caller scratch, num_elems x K).  The node pass sums each node's
+// contributions over its incident elements in adjacency order, so every
+// result is reproducible without atomics, and each element is evaluated once.  No reference counterpart (the reference has no derivatives);
 // checked against central finite differences and the FP64 oracle gradient.
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -102,13 +103,14 @@ __device__ inline double pair_u(int i, int j, int ns, const double *s_re, const 
   return u;
 }
 
+// Pass 1, one element per group: dL/dc_e and the element's contribution to
+// each of its K nodes' dL/dV, gl[e][l] = A_e sum_ij T_lij U_ij.
 template <int K, bool CPLX>
 __global__ void __launch_bounds__(kThreads)
-adjoint_kernel(int64_t nn, int64_t ne, int ns, const double2 *__restrict__ nodes,
-               const int32_t *__restrict__ elems, const int32_t *__restrict__ dofmap,
-               const double *__restrict__ psi, const double *__restrict__ w,
-               const int32_t *__restrict__ nadjptr, const int32_t *__restrict__ nadj,
-               double *__restrict__ dLdV, double *__restrict__ dLdc) {
+adjoint_elem_kernel(int64_t ne, int ns, const double2 *__restrict__ nodes,
+                    const int32_t *__restrict__ elems, const int32_t *__restrict__ dofmap,
+                    const double *__restrict__ psi, const double *__restrict__ w,
+                    double *__restrict__ dLdc, double *__restrict__ gl) {
   constexpr int KK = K * K;
   constexpr int GS = AdjCfg<K>::GS;
   constexpr int NG = kThreads / GS;
@@ -124,54 +126,58 @@ adjoint_kernel(int64_t nn, int64_t ne, int ns, const double2 *__restrict__ nodes
   __syncthreads();
 
   const int grp = threadIdx.x / GS, lane = threadIdx.x % GS;
-  const unsigned mask = GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << ((threadIdx.x & 31) / GS * GS));
+  const unsigned mask =
+      GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << ((threadIdx.x & 31) / GS * GS));
   double *s_re = s_amp[grp];
   double *s_im = s_re + K * ns;
-  const int64_t units = ne + nn;
-  for (int64_t u = int64_t(blockIdx.x) * NG + grp; u < units; u += int64_t(gridDim.x) * NG) {
-    if (u < ne) {
-      // dL/dc_e
-      const int e = int(u);
-      double A, g00, g01, g11;
-      element_geom<K>(e, nodes, elems, A, g00, g01, g11);
-      stage_element<K, GS, CPLX>(e, ns, lane, elems, dofmap, psi, s_re, s_im, mask);
-      double acc = 0.0;
+  for (int64_t u = int64_t(blockIdx.x) * NG + grp; u < ne; u += int64_t(gridDim.x) * NG) {
+    const int e = int(u);
+    double A, g00, g01, g11;
+    element_geom<K>(e, nodes, elems, A, g00, g01, g11);
+    stage_element<K, GS, CPLX>(e, ns, lane, elems, dofmap, psi, s_re, s_im, mask);
+    double acc_c = 0.0, acc[K];
 #pragma unroll
-      for (int q = 0; q < PP; ++q) {
-        const int ij = lane + q * GS;
-        if (ij < KK) {
-          const int i = ij / K, j = ij - i * K;
-          const double kh = g00 * s_S[ij] + g01 * s_S[KK + ij] + g11 * s_S[2 * KK + ij];
-          acc = fma(kh, pair_u<CPLX>(i, j, ns, s_re, s_im, s_w), acc);
-        }
-      }
-      acc = group_sum<GS>(acc, mask);
-      if (lane == 0) dLdc[e] = A * acc;
-      __syncwarp(mask);
-    } else {
-      // dL/dV_g over the node's incident elements, in adjacency order
-      const int64_t g = u - ne;
-      double acc = 0.0;
-      for (int t = nadjptr[g]; t < nadjptr[g + 1]; ++t) {
-        const int packed = nadj[t];
-        const int e = packed >> 4, l = packed & 15;
-        double A, g00, g01, g11;
-        element_geom<K>(e, nodes, elems, A, g00, g01, g11);
-        stage_element<K, GS, CPLX>(e, ns, lane, elems, dofmap, psi, s_re, s_im, mask);
-        double part = 0.0;
+    for (int l = 0; l < K; ++l) acc[l] = 0.0;
 #pragma unroll
-        for (int q = 0; q < PP; ++q) {
-          const int ij = lane + q * GS;
-          if (ij < KK) {
-            const int i = ij / K, j = ij - i * K;
-            part = fma(s_T[l * KK + ij], pair_u<CPLX>(i, j, ns, s_re, s_im, s_w), part);
-          }
-        }
-        acc += A * group_sum<GS>(part, mask);
-        __syncwarp(mask);
+    for (int q = 0; q < PP; ++q) {
+      const int ij = lane + q * GS;
+      if (ij < KK) {
+        const int i = ij / K, j = ij - i * K;
+        const double uij = pair_u<CPLX>(i, j, ns, s_re, s_im, s_w);
+        const double kh = g00 * s_S[ij] + g01 * s_S[KK + ij] + g11 * s_S[2 * KK + ij];
+        acc_c = fma(kh, uij, acc_c);
+#pragma unroll
+        for (int l = 0; l < K; ++l) acc[l] = fma(s_T[l * KK + ij], uij, acc[l]);
       }
-      if (lane == 0) dLdV[g] = acc;
     }
+    acc_c = group_sum<GS>(acc_c, mask);
+#pragma unroll
+    for (int l = 0; l < K; ++l) acc[l] = group_sum<GS>(acc[l], mask);
+    if (lane == 0) dLdc[e] = A * acc_c;
+    if (lane < K) {
+      double v = 0.0;
+#pragma unroll
+      for (int l = 0; l < K; ++l) v = (lane == l) ? acc[l] : v;
+      gl[size_t(e) * K + lane] = A * v;
+    }
+    __syncwarp(mask);
+  }
+}
+
+// Pass 2, one thread per node: dL/dV_g = sum over the node's incident
+// (element, local index) pairs, in adjacency order, of gl[e][l].
+template <int K>
+__global__ void adjoint_node_kernel(int64_t nn, const int32_t *__restrict__ nadjptr,
+                                    const int32_t *__restrict__ nadj,
+                                    const double *__restrict__ gl, double *__restrict__ dLdV) {
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < nn;
+       g += int64_t(gridDim.x) * blockDim.x) {
+    double acc = 0.0;
+    for (int t = nadjptr[g]; t < nadjptr[g + 1]; ++t) {
+      const int packed = nadj[t];
+      acc += gl[size_t(packed >> 4) * K + (packed & 15)];
+    }
+    dLdV[g] = acc;
   }
 }
 
@@ -179,18 +185,20 @@ template <int K>
 int launch_adjoint(int64_t nn, int64_t ne, int ns, bool cplx, const double *nodes,
                    const int32_t *elems, const int32_t *dofmap, const double *psi,
                    const double *w, const int32_t *nadjptr, const int32_t *nadj, double *dLdV,
-                   double *dLdc, cudaStream_t s) {
+                   double *dLdc, double *gl, cudaStream_t s) {
   const double2 *nd = reinterpret_cast<const double2 *>(nodes);
   constexpr int NG = kThreads / AdjCfg<K>::GS;
-  const int64_t units = nn + ne;
-  const int blocks = int(std::min<int64_t>((units + NG - 1) / NG, 148 * 8));
+  const int eblocks = int(std::min<int64_t>((ne + NG - 1) / NG, 148 * 8));
   qd::prof_begin(qd::PK_ADJOINT, s);
   if (cplx)
-    adjoint_kernel<K, true><<<blocks, kThreads, 0, s>>>(nn, ne, ns, nd, elems, dofmap, psi, w,
-                                                        nadjptr, nadj, dLdV, dLdc);
+    adjoint_elem_kernel<K, true><<<eblocks, kThreads, 0, s>>>(ne, ns, nd, elems, dofmap, psi, w,
+                                                             dLdc, gl);
   else
-    adjoint_kernel<K, false><<<blocks, kThreads, 0, s>>>(nn, ne, ns, nd, elems, dofmap, psi, w,
-                                                         nadjptr, nadj, dLdV, dLdc);
+    adjoint_elem_kernel<K, false><<<eblocks, kThreads, 0, s>>>(ne, ns, nd, elems, dofmap, psi,
+                                                              w, dLdc, gl);
+  QD_CHECK_LAUNCH();
+  const int nblocks = int(std::min<int64_t>((nn + 255) / 256, 148 * 16));
+  adjoint_node_kernel<K><<<nblocks, 256, 0, s>>>(nn, nadjptr, nadj, gl, dLdV);
   QD_CHECK_LAUNCH();
   qd::prof_end(qd::PK_ADJOINT, s);
   return QD_OK;
@@ -202,12 +210,12 @@ extern "C" int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n
                           int is_complex, const double *d_nodes, const int32_t *d_elems,
                           const int32_t *d_dofmap, const double *d_psi, const double *d_w,
                           const int32_t *d_nadjptr, const int32_t *d_nadj, double *d_dLdV,
-                          double *d_dLdc, void *stream) {
+                          double *d_dLdc, double *d_work, void *stream) {
   if (order < 1 || order > 3 || num_nodes <= 0 || num_elems <= 0) return QD_ERR_INVALID;
   if (n_states < 1 || n_states > kMaxStates) return QD_ERR_LIMIT;
   if (num_elems >= (int64_t(1) << 27) || num_nodes >= (int64_t(1) << 31)) return QD_ERR_LIMIT;
   if (!d_nodes || !d_elems || !d_dofmap || !d_psi || !d_w || !d_nadjptr || !d_nadj || !d_dLdV ||
-      !d_dLdc)
+      !d_dLdc || !d_work)
     return QD_ERR_INVALID;
   if (is_complex && (reinterpret_cast<uintptr_t>(d_psi) & 15)) return QD_ERR_INVALID;
   int st = ensure_tables();
@@ -215,8 +223,8 @@ extern "C" int qd_adjoint(int order, int64_t num_nodes, int64_t num_elems, int n
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool c = is_complex != 0;
   switch (order) {
-    case 1: return launch_adjoint<3>(num_nodes, num_elems, n_states, c, d_nodes, d_elems, d_dofmap, d_psi, d_w, d_nadjptr, d_nadj, d_dLdV, d_dLdc, s);
-    case 2: return launch_adjoint<6>(num_nodes, num_elems, n_states, c, d_nodes, d_elems, d_dofmap, d_psi, d_w, d_nadjptr, d_nadj, d_dLdV, d_dLdc, s);
-    default: return launch_adjoint<10>(num_nodes, num_elems, n_states, c, d_nodes, d_elems, d_dofmap, d_psi, d_w, d_nadjptr, d_nadj, d_dLdV, d_dLdc, s);
+    case 1: return launch_adjoint<3>(num_nodes, num_elems, n_states, c, d_nodes, d_elems, d_dofmap, d_psi, d_w, d_nadjptr, d_nadj, d_dLdV, d_dLdc, d_work, s);
+    case 2: return launch_adjoint<6>(num_nodes, num_elems, n_states, c, d_nodes, d_elems, d_dofmap, d_psi, d_w, d_nadjptr, d_nadj, d_dLdV, d_dLdc, d_work, s);
+    default: return launch_adjoint<10>(num_nodes, num_elems, n_states, c, d_nodes, d_elems, d_dofmap, d_psi, d_w, d_nadjptr, d_nadj, d_dLdV, d_dLdc, d_work, s);
   }
 }

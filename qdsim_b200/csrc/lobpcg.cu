@@ -46,7 +46,14 @@
 
 namespace {
 
-constexpr int kChunkRows = 1024;
+constexpr int kChunkRows = 1024;      // default rows per chunk (qd_lobpcg_opts.chunk_rows)
+
+// Rows per chunk (the CTA unit of every row-parallel kernel): the option's
+// value when it is a multiple of 64 in [256, 8192], else the default.
+int chunk_rows_of(const qd_lobpcg_opts *opts) {
+  const int c = opts ? opts->chunk_rows : 0;
+  return (c >= 256 && c <= 8192 && c % 64 == 0) ? c : kChunkRows;
+}
 constexpr int kMaxB = 16;
 constexpr int kMaxM = 3 * kMaxB;
 constexpr int kStagWindow = 12;     // FP32 iterations without halving the estimate
@@ -1352,6 +1359,31 @@ __global__ void count_active_kernel(const DotState *st, int n, int *out) {
   if (threadIdx.x == 0) *out = s;
 }
 
+// Device-side control of the solver's WHILE graph (the loop over iteration
+// blocks): counts the active dots and keeps the loop running while some dot
+// is active, no bounded wait has expired and fewer than `cap` blocks have run.
+// The block counter makes the loop end after at most `cap` bodies whatever
+// the dots' state.  first != 0: the check before the first body (resets the
+// counter); otherwise the check at the end of a body (counts that block).
+__global__ void loop_control_kernel(const DotState *st, int n, int *count, int cap,
+                                    const int *wait_err, cudaGraphConditionalHandle cond,
+                                    int first) {
+  __shared__ int s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  int c = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c += st[i].active;
+  atomicAdd(&s, c);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int blocks = first ? 0 : count[1] + 1;
+    count[0] = s;
+    count[1] = blocks;
+    const bool go = s > 0 && blocks < cap && *wait_err == 0;
+    cudaGraphSetConditional(cond, go ? 1u : 0u);
+  }
+}
+
 // FP32 -> FP64 hand-over of the dots that left the FP32 phase this iteration:
 // X64 = X32 on their rows, the other FP64 blocks cleared (P restarts empty).
 template <int B>
@@ -1478,11 +1510,11 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   return QD_OK;
 }
 
-int count_chunks(int n_dots, const int32_t *row_off) {
+int count_chunks(int n_dots, const int32_t *row_off, int chunk_rows) {
   int64_t c = 0;
   for (int d = 0; d < n_dots; ++d) {
     const int n = row_off[d + 1] - row_off[d];
-    c += (n + kChunkRows - 1) / kChunkRows;
+    c += (n + chunk_rows - 1) / chunk_rows;
   }
   return int(c);
 }
@@ -1637,61 +1669,117 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
     }
     return QD_OK;
   };
-  // Iterations run in blocks of kGraphBlock; after each block one host
-  // read of the number of active dots decides whether to stop.  The first
-  // block is enqueued directly (it also sets every kernel's attributes); the
-  // following blocks replay a CUDA graph of one block, captured once on a
-  // private stream and launched into the caller's stream.  Kernel arguments
-  // are the same in every iteration (per-dot progress lives on the device),
-  // so one graph serves all blocks.  With per-kernel timing enabled, or
-  // graphs switched off in the options, every block is enqueued directly.
+  // Iterations run in blocks of kGraphBlock.  The first block is enqueued
+  // directly (it also sets every kernel's attributes).  The rest of the solve
+  // is one CUDA graph: a WHILE conditional node whose body is one block of
+  // iterations followed by loop_control_kernel, which counts the active dots
+  // on the device and sets the loop condition; a check before the loop decides
+  // whether the body runs at all.  So the whole solve runs with no host
+  // round trip until it has converged (or hit max_iter, or a bounded wait
+  // expired).  The graph is captured on a private stream and launched into the
+  // caller's stream; kernel arguments are the same in every iteration
+  // (per-dot progress lives on the device).  Where conditional graph nodes are
+  // unavailable, with per-kernel timing enabled, or with graphs switched off
+  // in the options, blocks are enqueued directly and the host reads the
+  // active-dot count after each one.
   constexpr int kGraphBlock = 8;
   const bool graphs = use_graphs && !qd::prof_enabled();
+  const int total_blocks = (prm.max_iter + kGraphBlock + kGraphBlock - 1) / kGraphBlock;
   struct GraphGuard {
     cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~GraphGuard() {
       if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
       if (cap) cudaStreamDestroy(cap);
     }
   } gg;
-  uint64_t graph_launches = 0;
-  int host_count = n_dots;
   iters_run = 0;
-  for (int blk = 0; iters_run < prm.max_iter + kGraphBlock; ++blk) {
-    if (blk == 0 || !graphs) {
+  for (int i = 0; i < kGraphBlock; ++i) {
+    const int st = iteration(s);
+    if (st != QD_OK) return st;
+  }
+  iters_run = kGraphBlock;
+  if (total_blocks <= 1) return QD_OK;
+  bool device_loop = false;
+  if (graphs) {
+    // WHILE graph: [check] -> WHILE(cond) { kGraphBlock iterations; control }
+    cudaGraphConditionalHandle cond;
+    cudaGraphNode_t pre = nullptr, loop = nullptr;
+    size_t nnodes = 1;
+    uint64_t body_launches = 0;
+    bool ok = cudaStreamCreateWithFlags(&gg.cap, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaGraphCreate(&gg.graph, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&cond, gg.graph, 0, cudaGraphCondAssignDefault) ==
+                  cudaSuccess;
+    if (ok) {
+      QD_CUDA_TRY(cudaStreamBeginCaptureToGraph(gg.cap, gg.graph, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal));
+      loop_control_kernel<<<1, 256, 0, gg.cap>>>(L.st, n_dots, L.count, total_blocks - 1,
+                                                 L.wait_err, cond, 1);
+      const cudaError_t le = cudaGetLastError();
+      cudaGraph_t g = gg.graph;
+      QD_CUDA_TRY(cudaStreamEndCapture(gg.cap, &g));
+      QD_CUDA_TRY(le);
+      QD_LAUNCHED();
+      ok = cudaGraphGetNodes(gg.graph, &pre, &nnodes) == cudaSuccess && nnodes == 1;
+    }
+    if (ok) {
+      cudaGraphNodeParams p = {};
+      p.type = cudaGraphNodeTypeConditional;
+      p.conditional.handle = cond;
+      p.conditional.type = cudaGraphCondTypeWhile;
+      p.conditional.size = 1;
+      ok = cudaGraphAddNode(&loop, gg.graph, &pre, 1, &p) == cudaSuccess;
+      if (ok) {
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        QD_CUDA_TRY(cudaStreamBeginCaptureToGraph(gg.cap, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+        const uint64_t l0 = qd::g_launches.load();
+        int st = QD_OK;
+        for (int i = 0; i < kGraphBlock && st == QD_OK; ++i) st = iteration(gg.cap);
+        if (st == QD_OK) {
+          loop_control_kernel<<<1, 256, 0, gg.cap>>>(L.st, n_dots, L.count, total_blocks - 1,
+                                                     L.wait_err, cond, 0);
+          if (cudaGetLastError() != cudaSuccess) st = QD_ERR_CUDA;
+          QD_LAUNCHED();
+        }
+        body_launches = qd::g_launches.load() - l0;
+        const cudaError_t ce = cudaStreamEndCapture(gg.cap, &body);
+        if (st != QD_OK) return st;
+        QD_CUDA_TRY(ce);
+        QD_CUDA_TRY(cudaGraphInstantiate(&gg.exec, gg.graph, 0));
+        QD_CUDA_TRY(cudaGraphLaunch(gg.exec, s));
+        int blocks = 0;
+        QD_CUDA_TRY(cudaMemcpyAsync(&blocks, L.count + 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                    s));
+        QD_CUDA_TRY(cudaStreamSynchronize(s));
+        // the body's launches were counted once while it was captured
+        if (blocks > 1)
+          qd::g_launches.fetch_add(body_launches * uint64_t(blocks - 1),
+                                   std::memory_order_relaxed);
+        if (blocks == 0) qd::g_launches.fetch_sub(body_launches, std::memory_order_relaxed);
+        iters_run += kGraphBlock * blocks;
+        device_loop = true;
+      }
+    }
+    if (!ok) cudaGetLastError();    // clear the error of an unsupported conditional node
+  }
+  if (!device_loop) {
+    int host_count = n_dots;
+    for (int blk = 1; blk < total_blocks; ++blk) {
+      count_active_kernel<<<1, 256, 0, s>>>(L.st, n_dots, L.count);
+      QD_CHECK_LAUNCH();
+      QD_CUDA_TRY(cudaMemcpyAsync(&host_count, L.count, sizeof(int), cudaMemcpyDeviceToHost, s));
+      QD_CUDA_TRY(cudaStreamSynchronize(s));
+      if (host_count == 0) break;
       for (int i = 0; i < kGraphBlock; ++i) {
         const int st = iteration(s);
         if (st != QD_OK) return st;
       }
-    } else {
-      if (!gg.exec) {
-        QD_CUDA_TRY(cudaStreamCreateWithFlags(&gg.cap, cudaStreamNonBlocking));
-        const uint64_t l0 = qd::g_launches.load();
-        cudaGraph_t graph = nullptr;
-        QD_CUDA_TRY(cudaStreamBeginCapture(gg.cap, cudaStreamCaptureModeThreadLocal));
-        int st = QD_OK;
-        for (int i = 0; i < kGraphBlock && st == QD_OK; ++i) st = iteration(gg.cap);
-        const cudaError_t ce = cudaStreamEndCapture(gg.cap, &graph);
-        if (st != QD_OK || ce != cudaSuccess) {
-          if (graph) cudaGraphDestroy(graph);
-          return st != QD_OK ? st : QD_ERR_CUDA;
-        }
-        graph_launches = qd::g_launches.load() - l0;   // counted once, for this replay
-        const cudaError_t ie = cudaGraphInstantiate(&gg.exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ie != cudaSuccess) return QD_ERR_CUDA;
-      } else {
-        qd::g_launches.fetch_add(graph_launches, std::memory_order_relaxed);
-      }
-      QD_CUDA_TRY(cudaGraphLaunch(gg.exec, s));
+      iters_run += kGraphBlock;
     }
-    iters_run += kGraphBlock;
-    count_active_kernel<<<1, 256, 0, s>>>(L.st, n_dots, L.count);
-    QD_CHECK_LAUNCH();
-    QD_CUDA_TRY(cudaMemcpyAsync(&host_count, L.count, sizeof(int), cudaMemcpyDeviceToHost, s));
-    QD_CUDA_TRY(cudaStreamSynchronize(s));
-    if (host_count == 0) break;
   }
   return QD_OK;
 }
@@ -1704,7 +1792,8 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
             double *d_res_out, int32_t *d_iters_out, int32_t *h_info, int32_t *h_counts,
             void *d_work, size_t work_bytes, const qd_lobpcg_opts *opts, cudaStream_t s) {
   const int64_t n_rows = h_row_off[n_dots];
-  const int nchunks = count_chunks(n_dots, h_row_off);
+  const int chunk_rows = chunk_rows_of(opts);
+  const int nchunks = count_chunks(n_dots, h_row_off, chunk_rows);
   int64_t ntx = 0, nty = 0;
   if (h_prec) {
     if (!d_mats) return QD_ERR_INVALID;
@@ -1778,8 +1867,8 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     x.run[x.phase] = 1;
     x.best = 1e300;
     x.chunk0 = int(chunks.size());
-    for (int r = h_row_off[d]; r < h_row_off[d + 1]; r += kChunkRows)
-      chunks.push_back(Chunk{d, r, std::min(r + kChunkRows, h_row_off[d + 1]), 0});
+    for (int r = h_row_off[d]; r < h_row_off[d + 1]; r += chunk_rows)
+      chunks.push_back(Chunk{d, r, std::min(r + chunk_rows, h_row_off[d + 1]), 0});
     x.chunk1 = int(chunks.size());
     if (x.chunk1 == x.chunk0) {
       x.active = 0;
@@ -1868,12 +1957,13 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
 
 extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total,
                                         int64_t nnz_total, int b, int prec_mode,
-                                        const qd_dst_prec *h_prec, size_t *bytes) {
+                                        const qd_dst_prec *h_prec, const qd_lobpcg_opts *opts,
+                                        size_t *bytes) {
   if (!bytes || n_dots <= 0 || n_rows_total <= 0 || nnz_total <= 0 || b < 4 || b > kMaxB ||
       b % 4)
     return QD_ERR_INVALID;
   // upper bound on the chunk count: every dot contributes at most one partial chunk
-  const int nchunks = int(n_rows_total / kChunkRows) + n_dots;
+  const int nchunks = int(n_rows_total / chunk_rows_of(opts)) + n_dots;
   int64_t ntx = 0, nty = 0;
   if (h_prec) qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);

@@ -49,10 +49,12 @@ def pack_block_diagonal(mats):
     return np.asarray(row_off, dtype=np.int32), rowptr, col, H, M
 
 
-def workspace_bytes(n_dots: int, n_rows: int, nnz: int, b: int, prec: int, h_prec=None) -> int:
+def workspace_bytes(n_dots: int, n_rows: int, nnz: int, b: int, prec: int, h_prec=None,
+                    opts=None) -> int:
     out = C.c_size_t()
     N.check(N.lib().qd_lobpcg_workspace_size(n_dots, n_rows, nnz, b, prec, N.ptr(h_prec),
-                                             C.byref(out)), "qd_lobpcg_workspace_size")
+                                             N.ptr(opts), C.byref(out)),
+            "qd_lobpcg_workspace_size")
     return int(out.value)
 
 
@@ -138,14 +140,17 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
                   max_iter=2000, seed=1234, workspace: Workspace | None = None, stream=None,
                   allow_not_converged=True, precond: DSTPreconditioner | None = None,
                   tol32: float | None = None, stag_window: int | None = None,
-                  graphs: bool = True, x0=None, eig_scale: float = 0.0):
+                  graphs: bool = True, x0=None, eig_scale: float = 0.0,
+                  chunk_rows: int | None = None):
     """Solve a packed block-diagonal batch; returns (E, X_all, res, iters, info, status).
 
     ``tol32`` / ``stag_window`` tune the FP32 -> FP64 hand-over of the mixed
     mode (``None``: library defaults); ``graphs=False`` enqueues every kernel
     instead of replaying CUDA graphs; ``x0`` (device float64 [n_rows, k])
     warm-starts the first k block vectors; ``eig_scale`` (eV) measures
-    eigenvalue errors relative to max(|E|, eig_scale) (levels near zero)."""
+    eigenvalue errors relative to max(|E|, eig_scale) (levels near zero);
+    ``chunk_rows`` sets the rows per CTA of the row-parallel kernels (a
+    multiple of 64 in [256, 8192]; ``None``: 1024)."""
     n_dots = len(row_off) - 1
     n_rows = int(row_off[-1])
     if b is None:
@@ -155,7 +160,15 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
     dev = H.device
     h_prec = precond.desc if precond is not None else None
     d_mats = precond.d_mats if precond is not None else None
-    nbytes = workspace_bytes(n_dots, n_rows, col.numel(), b, prec, h_prec)
+    opts = np.zeros(1, dtype=N.LOBPCG_OPTS_DTYPE)
+    if x0 is not None:
+        x0 = x0.to(dev, torch.float64).contiguous()
+        if x0.numel() != n_rows * k:
+            raise ValueError("x0 must hold n_rows x k values")
+    opts[0] = (float(tol32) if tol32 else 0.0, int(stag_window) if stag_window else 0,
+               1 if graphs else 0, int(x0.data_ptr()) if x0 is not None else 0,
+               float(eig_scale), int(chunk_rows) if chunk_rows else 0, 0)
+    nbytes = workspace_bytes(n_dots, n_rows, col.numel(), b, prec, h_prec, opts)
     ws = (workspace or Workspace(dev)).get(nbytes)
     X = torch.empty(n_rows * k, dtype=torch.float64, device=dev)
     E = torch.empty(n_dots * k, dtype=torch.float64, device=dev)
@@ -164,14 +177,6 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
     info = np.zeros(4, dtype=np.int32)
     counts = np.zeros((n_dots, 6), dtype=np.int32)
     ro = np.ascontiguousarray(row_off, dtype=np.int32)
-    opts = np.zeros(1, dtype=N.LOBPCG_OPTS_DTYPE)
-    if x0 is not None:
-        x0 = x0.to(dev, torch.float64).contiguous()
-        if x0.numel() != n_rows * k:
-            raise ValueError("x0 must hold n_rows x k values")
-    opts[0] = (float(tol32) if tol32 else 0.0, int(stag_window) if stag_window else 0,
-               1 if graphs else 0, int(x0.data_ptr()) if x0 is not None else 0,
-               float(eig_scale))
     st = N.lib().qd_lobpcg_solve(
         n_dots, N.ptr(ro), None, N.ptr(rowptr), N.ptr(col), N.ptr(H), N.ptr(M), N.ptr(h_prec),
         N.ptr(d_mats), k, b, prec,

@@ -52,7 +52,18 @@ class FieldInterpolator:
 
         Returns a dict of device tensors: ``value`` ((P,) or (F, P)), and with
         ``gradient`` ``grad_x`` / ``grad_y`` of the same shape, with
-        ``element`` ``element`` ((P,) int32, -1 outside the mesh)."""
+        ``element`` ``element`` ((P,) int32, -1 outside the mesh).
+
+        With an explicit ``stream`` the input copies, the output allocations and
+        the launch all happen on that stream, so the kernel never reads inputs
+        still being copied on another stream and the caching allocator ties the
+        outputs to the stream that writes them."""
+        if stream is not None:
+            with torch.cuda.stream(stream):
+                return self._evaluate(x, y, field, gradient, element, stream)
+        return self._evaluate(x, y, field, gradient, element, None)
+
+    def _evaluate(self, x, y, field, gradient, element, stream):
         m = self.mesh
         xs, ys = _points(x, self.device), _points(y, self.device)
         if xs.numel() != ys.numel():

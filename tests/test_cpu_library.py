@@ -40,13 +40,13 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.qd_assemble(4, 0, 10, 10, 5, *([None] * 16)) == N.QD_ERR_INVALID
     assert L.qd_assemble(2, N.QD_ASM_REF_FIXED, 10, 10, 5, *([None] * 16)) == N.QD_ERR_INVALID
     out = C.c_size_t()
-    assert L.qd_lobpcg_workspace_size(1, 100, 900, 3, 0, None, C.byref(out)) == N.QD_ERR_INVALID
-    assert L.qd_lobpcg_workspace_size(1, 100, 0, 12, 0, None, C.byref(out)) == N.QD_ERR_INVALID
-    assert L.qd_lobpcg_workspace_size(1, 100, 900, 12, 0, None, C.byref(out)) == N.QD_OK
+    assert L.qd_lobpcg_workspace_size(1, 100, 900, 3, 0, None, None, C.byref(out)) == N.QD_ERR_INVALID
+    assert L.qd_lobpcg_workspace_size(1, 100, 0, 12, 0, None, None, C.byref(out)) == N.QD_ERR_INVALID
+    assert L.qd_lobpcg_workspace_size(1, 100, 900, 12, 0, None, None, C.byref(out)) == N.QD_OK
     assert out.value > 9 * 100 * 12 * 8
     fp64 = out.value
     # mixed precision adds the FP32 vector blocks and FP32 (H, M) pairs
-    assert L.qd_lobpcg_workspace_size(1, 100, 900, 12, 1, None, C.byref(out)) == N.QD_OK
+    assert L.qd_lobpcg_workspace_size(1, 100, 900, 12, 1, None, None, C.byref(out)) == N.QD_OK
     assert out.value >= fp64 + 9 * 100 * 12 * 4 + 900 * 8
     assert L.qd_pcg_workspace_size(100, 300, C.byref(out)) == N.QD_ERR_INVALID
     ro = np.array([0, 5], np.int32)

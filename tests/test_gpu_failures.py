@@ -52,9 +52,9 @@ def test_nan_mass_matrix_is_a_breakdown(cuda):
     from qdsim_b200 import _native as N
     hb, db = _dot_batch(cuda)
     db.M[::7] = float("nan")
-    E, X, R, it, info, st = db.solve(8, b=12, precision="fp64", tol=1e-9, max_iter=50)
-    assert st == N.QD_ERR_BREAKDOWN
-    assert info["converged_dots"] == 0
+    with pytest.raises(N.QDError) as exc:
+        db.solve(8, b=12, precision="fp64", tol=1e-9, max_iter=50)
+    assert exc.value.status == N.QD_ERR_BREAKDOWN
     torch.cuda.synchronize()          # the context is still usable
 
 
@@ -63,8 +63,9 @@ def test_indefinite_pencil_is_a_breakdown(cuda, precision):
     from qdsim_b200 import _native as N
     hb, db = _dot_batch(cuda)
     db.M.neg_()                        # negative definite "mass matrix"
-    E, X, R, it, info, st = db.solve(8, b=12, precision=precision, tol=1e-9, max_iter=50)
-    assert st == N.QD_ERR_BREAKDOWN
+    with pytest.raises(N.QDError) as exc:
+        db.solve(8, b=12, precision=precision, tol=1e-9, max_iter=50)
+    assert exc.value.status == N.QD_ERR_BREAKDOWN
     # a healthy solve on the same device afterwards
     db.assemble()
     E, X, R, it, info, st = db.solve(8, b=12, precision=precision, tol=1e-9, max_iter=500)
