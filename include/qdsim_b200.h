@@ -41,7 +41,9 @@ enum {
 enum {
   QD_ASM_FEM = 0,             /* fem.cpp weak form, nodal V/W interpolated        */
   QD_ASM_REF_CYTHON = 1,      /* schrodinger_solver.pyx:201-251 element formulas  */
-  QD_ASM_REF_FIXED = 2        /* fixed_open_system_solver.pyx:197-271 formulas    */
+  QD_ASM_REF_FIXED = 2,       /* fixed_open_system_solver.pyx:197-271 formulas    */
+  QD_ASM_REF_CPP = 3          /* schrodinger.cpp:92-230: P1 stiffness, V and M by
+                                 the centroid rule (every entry V A/9, A/9)       */
 };
 
 /* eigensolver precision modes */

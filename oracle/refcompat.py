@@ -13,6 +13,12 @@ All quantities in SI, as the reference uses them.
   (qdsim_cython/solvers/schrodinger_solver.pyx:120-251): P1 stiffness with
   gradients, V A/3 on the diagonal, added a second time at local nodes 1 and 2
   (:224-236); area < 1e-15 m^2 skipped (:151).
+* ``cpp_assembly`` -- SchrodingerSolver::assemble_matrices_cpu
+  (backend/src/schrodinger.cpp:92-230): P1 stiffness with gradients, the
+  potential and the mass by the one-point centroid rule (every entry of the
+  element matrices V A/9 and A/9).  That mass matrix is singular (each
+  element adds a rank-one term), which is why the reference's dense solve
+  (:699-724) falls back to adding reg I to it.
 * Boundary handling: the reference replaces boundary rows by identity rows
   (:253-283; fixed solver: nodes 0 and N-1 only, :273-291).  The physical
   eigenpairs of that pencil are those of the pencil restricted to the free
@@ -86,6 +92,20 @@ def cython_assembly(nodes, elems, m_func, V_func):
         Me[:, i, i] = 2.0 * A / 12.0
     n = nodes.shape[0]
     return _csr(elems[keep], He[keep], n), _csr(elems[keep], Me[keep], n)
+
+
+def cpp_assembly(nodes, elems, m_func, V_func):
+    P0, P1, P2, det, A = _tri(nodes, elems)
+    m, V = element_centroid_values(nodes, elems, m_func, V_func)
+    inv = 1.0 / det
+    g = np.stack([np.stack([(P1[:, 1] - P2[:, 1]) * inv, (P2[:, 0] - P1[:, 0]) * inv], 1),
+                  np.stack([(P2[:, 1] - P0[:, 1]) * inv, (P0[:, 0] - P2[:, 0]) * inv], 1),
+                  np.stack([(P0[:, 1] - P1[:, 1]) * inv, (P1[:, 0] - P0[:, 0]) * inv], 1)], 1)
+    kin = HBAR * HBAR / (2.0 * m) * A
+    He = kin[:, None, None] * np.einsum('eid,ejd->eij', g, g) + (V * A / 9.0)[:, None, None]
+    Me = np.broadcast_to((A / 9.0)[:, None, None], He.shape).copy()
+    n = nodes.shape[0]
+    return _csr(elems, He, n), _csr(elems, Me, n)
 
 
 def boundary_nodes(nodes, Lx, Ly):

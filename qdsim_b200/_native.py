@@ -23,6 +23,7 @@ QD_ERR_TIMEOUT = -8
 QD_ASM_FEM = 0
 QD_ASM_REF_CYTHON = 1
 QD_ASM_REF_FIXED = 2
+QD_ASM_REF_CPP = 3
 
 QD_PREC_FP64 = 0
 QD_PREC_MIXED = 1

@@ -22,6 +22,9 @@
 //               nodes 1 and 2 (:224-236); consistent mass.
 //   REF_FIXED:  fixed_open_system_solver.pyx:225-255 -- c A/3 on the diagonal and
 //               c A/6 off it (no gradients), V A/3 on the diagonal; consistent mass.
+//   REF_CPP:    SchrodingerSolver::assemble_matrices_cpu (backend/src/schrodinger.cpp:
+//               92-230) -- correct P1 stiffness; the potential and the mass by the
+//               one-point centroid rule, every entry V A/9 and A/9.
 #include <cuda_runtime.h>
 #include "common.h"
 #include "devtables.cuh"
@@ -185,12 +188,15 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
           } else if (mode == QD_ASM_REF_CYTHON) {
             hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]);
             if (a == b) hk += (a == 0 ? 1.0 : 2.0) * (st.V[t][0] * At / 3.0);
-          } else {
+          } else if (mode == QD_ASM_REF_FIXED) {
             hk = (st.cA[t] / 3.0) * (a == b ? 1.0 : 0.5);
             if (a == b) hk += st.V[t][0] * At / 3.0;
+          } else {
+            hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]) +
+                 st.V[t][0] * At / 9.0;
           }
           h += hk;
-          mm += At * Mr[ab];
+          mm += mode == QD_ASM_REF_CPP ? At / 9.0 : At * Mr[ab];
         }
         H[rp + s] = h;
         M[rp + s] = mm;
@@ -235,7 +241,8 @@ extern "C" int qd_assemble(int order, int mode, int64_t num_nodes, int64_t num_e
                            const uint8_t *d_contrib, const uint8_t *d_slotcnt, double *d_H,
                            double *d_M, double *d_Himag, int32_t *d_status, void *stream) {
   if (order < 1 || order > 3) return QD_ERR_INVALID;
-  if (mode != QD_ASM_FEM && mode != QD_ASM_REF_CYTHON && mode != QD_ASM_REF_FIXED)
+  if (mode != QD_ASM_FEM && mode != QD_ASM_REF_CYTHON && mode != QD_ASM_REF_FIXED &&
+      mode != QD_ASM_REF_CPP)
     return QD_ERR_INVALID;
   if (mode != QD_ASM_FEM && order != 1) return QD_ERR_INVALID;
   if (num_nodes <= 0 || num_elems <= 0 || n_dofs < 0) return QD_ERR_INVALID;

@@ -71,7 +71,8 @@ constexpr double kCholPivot32 = 1e-5;    // smallest Cholesky pivot of the scale
 #endif
 
 struct Chunk {
-  int dot, begin, end, pad;
+  int dot, begin, end;
+  int jacobi;       // the dot has no lattice: diagonal (Jacobi) preconditioning
 };
 
 struct DotState {
@@ -1359,6 +1360,39 @@ __global__ void count_active_kernel(const DotState *st, int n, int *out) {
   if (threadIdx.x == 0) *out = s;
 }
 
+// Diagonal (Jacobi) preconditioner of the dots without a lattice (refined
+// meshes, natural boundaries): per row d_r = max(|H_rr|, sum_{j != r} |H_rj|),
+// the stiffness scale of the row (stiffness rows sum to about zero, so the
+// off-diagonal sum tracks the diagonal even where the potential cancels it),
+// and W_r <- W_r / d_r.
+__global__ void jacobi_diag_kernel(const Chunk *chunks, const int32_t *__restrict__ rowptr,
+                                   const int32_t *__restrict__ col,
+                                   const double *__restrict__ H, double *__restrict__ dinv) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!ch.jacobi) return;
+  for (int r = ch.begin + threadIdx.x; r < ch.end; r += blockDim.x) {
+    double dg = 0.0, off = 0.0;
+    for (int p = rowptr[r]; p < rowptr[r + 1]; ++p) {
+      const double h = fabs(H[p]);
+      if (col[p] == r) dg = h;
+      else off += h;
+    }
+    const double d = fmax(dg, off);
+    dinv[r] = d > 0.0 ? 1.0 / d : 1.0;
+  }
+}
+
+template <typename TV, int B>
+__global__ void jacobi_apply_kernel(const Chunk *chunks, const DotState *st, int ph,
+                                    const double *__restrict__ dinv, TV *__restrict__ W) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!ch.jacobi || !st[ch.dot].run[ph]) return;
+  for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
+    const size_t o = size_t(ch.begin) * B + idx;
+    W[o] = TV(double(W[o]) * dinv[ch.begin + idx / B]);
+  }
+}
+
 // Device-side control of the solver's WHILE graph (the loop over iteration
 // blocks): counts the active dots and keeps the loop running while some dot
 // is active, no bounded wait has expired and fewer than `cap` blocks have run.
@@ -1456,6 +1490,8 @@ struct Layout {
   int rows_x, rows_y;    // largest TMEM row block of the x / y passes
   const uint16_t *mats;
   int *wait_err;         // set by a kernel whose bounded wait ran out
+  double *dinv;          // Jacobi preconditioner of the dots without a lattice
+  int njac;              // chunks of such dots
   float2 *hm32;          // FP32 (H, M) pairs per nonzero (mixed precision only)
   int32_t *col32;        // copy of the column indices with bulk-copy slack (mixed only)
   float *rs32;           // row sums of the FP32 H values, summed in FP64 (mixed only)
@@ -1469,7 +1505,7 @@ size_t rr_smem_bytes(int B) {
 }
 
 int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nchunks,
-          int64_t ntx, int64_t nty, bool mixed, Layout &L) {
+          int64_t ntx, int64_t nty, bool mixed, bool jacobi, Layout &L) {
   const int m = 3 * B;
   L.chunks = ar.take<Chunk>(nchunks);
   L.row_off = ar.take<int32_t>(n_dots + 1);
@@ -1491,6 +1527,8 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   L.rs32 = mixed ? ar.take<float>(size_t(n_rows)) : nullptr;
   L.hm_exp = ar.take<int>(2);
   L.hm_sh = L.hm_sm = 1.0;
+  L.dinv = jacobi ? ar.take<double>(size_t(n_rows)) : nullptr;
+  L.njac = 0;
   L.nchunks = nchunks;
   L.ntx = ntx;
   L.nty = nty;
@@ -1508,6 +1546,14 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
     L.tiles_x = L.tiles_y = nullptr;
   }
   return QD_OK;
+}
+
+// Some dot has no lattice (no descriptor, or nx <= 0): Jacobi preconditioning.
+bool needs_jacobi(int n_dots, const qd_dst_prec *h_prec) {
+  if (!h_prec) return true;
+  for (int d = 0; d < n_dots; ++d)
+    if (h_prec[d].nx <= 0) return true;
+  return false;
 }
 
 int count_chunks(int n_dots, const int32_t *row_off, int chunk_rows) {
@@ -1571,6 +1617,12 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
                                       L.wait_err, s);
     qd::prof_end(qd::PK_PRECOND, s);
     if (e != cudaSuccess) return QD_ERR_CUDA;
+  }
+  if (L.njac > 0) {
+    qd::prof_begin(qd::PK_PRECOND, s);
+    jacobi_apply_kernel<TV, B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, PH, L.dinv, b.W);
+    qd::prof_end(qd::PK_PRECOND, s);
+    QD_CHECK_LAUNCH();
   }
   qd::prof_begin(qd::PK_ORTHO, s);
   {
@@ -1812,16 +1864,17 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   QD_CUDA_TRY(cudaStreamSynchronize(s));
   if (nnz <= 0) return QD_ERR_INVALID;
   const bool mixed_mode = prec_mode == QD_PREC_MIXED;
+  const bool jacobi = needs_jacobi(n_dots, h_prec);
   {
     qd::Arena need(nullptr, 0);
     Layout tmp;
-    carve(need, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, tmp);
+    carve(need, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, jacobi, tmp);
     if (need.used > work_bytes) return QD_ERR_WORKSPACE;
   }
   if (reinterpret_cast<uintptr_t>(d_work) % 256 != 0) return QD_ERR_WORKSPACE;
   qd::Arena ar(d_work, work_bytes);
   Layout L;
-  carve(ar, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, L);
+  carve(ar, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, jacobi, L);
   if (mixed_mode) {
     const int init[2] = {INT_MIN, INT_MIN};
     int e2[2];
@@ -1867,8 +1920,11 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     x.run[x.phase] = 1;
     x.best = 1e300;
     x.chunk0 = int(chunks.size());
-    for (int r = h_row_off[d]; r < h_row_off[d + 1]; r += chunk_rows)
-      chunks.push_back(Chunk{d, r, std::min(r + chunk_rows, h_row_off[d + 1]), 0});
+    const int jac = (!h_prec || h_prec[d].nx <= 0) ? 1 : 0;
+    for (int r = h_row_off[d]; r < h_row_off[d + 1]; r += chunk_rows) {
+      chunks.push_back(Chunk{d, r, std::min(r + chunk_rows, h_row_off[d + 1]), jac});
+      L.njac += jac;
+    }
     x.chunk1 = int(chunks.size());
     if (x.chunk1 == x.chunk0) {
       x.active = 0;
@@ -1878,6 +1934,10 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   }
   QD_CUDA_TRY(cudaMemcpyAsync(L.chunks, chunks.data(), chunks.size() * sizeof(Chunk),
                               cudaMemcpyHostToDevice, s));
+  if (L.njac > 0) {
+    jacobi_diag_kernel<<<int(chunks.size()), 256, 0, s>>>(L.chunks, d_rowptr, d_col, d_H, L.dinv);
+    QD_CHECK_LAUNCH();
+  }
   QD_CUDA_TRY(cudaMemcpyAsync(L.st, st.data(), st.size() * sizeof(DotState),
                               cudaMemcpyHostToDevice, s));
   QD_CUDA_TRY(cudaMemcpyAsync(L.row_off, h_row_off, sizeof(int32_t) * (n_dots + 1),
@@ -1969,7 +2029,7 @@ extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total,
   qd::Arena ar(nullptr, 0);
   Layout L;
   carve(ar, n_dots, n_rows_total, nnz_total, b, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED,
-        L);
+        needs_jacobi(n_dots, h_prec), L);
   *bytes = ar.used;
   return QD_OK;
 }

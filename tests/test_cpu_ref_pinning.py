@@ -108,3 +108,19 @@ def test_poisson_matrices_and_potential_match_reference():
     assert _rel(phi, G["poisson_phi"]) < 1e-10
     ex, ey = OP.electric_field(phi, 9, 6, 1e-6, 1e-6)
     assert _rel(ex, G["poisson_Ex"]) < 1e-9 and _rel(ey, G["poisson_Ey"]) < 1e-8
+
+
+def test_cpp_solver_mass_matrix_is_singular():
+    """The C++ SchrodingerSolver's centroid-rule mass matrix (every element
+    entry A/9, backend/src/schrodinger.cpp:171-211) is singular: each element
+    adds a rank-one term.  So the eigenpairs its dense solve returns depend
+    on the regularisation it adds when the Cholesky factorisation fails
+    (reg I with reg >= 1e-10 m^2 against entries ~1e-18 m^2, :706-724), not on
+    the pencil; only its assembly is reproduced (QD_ASM_REF_CPP)."""
+    om = O.structured_mesh(1, 20, 12, 60e-9, 40e-9)
+    H, M = RC.cpp_assembly(om.nodes, om.elems, m_nm, v_nm)
+    w = np.linalg.eigvalsh(M.toarray())
+    assert (np.abs(w) <= 1e-12 * w.max()).sum() >= 1
+    # H keeps the exact P1 stiffness: its kinetic part annihilates constants
+    Hk, _ = RC.cpp_assembly(om.nodes, om.elems, m_nm, lambda x, y: 0.0)
+    assert np.abs(Hk @ np.ones(om.num_nodes)).max() <= 1e-12 * abs(Hk).max()

@@ -94,3 +94,21 @@ def test_poisson_stiffness_matches_compiled_reference(cuda):
     n = m.num_nodes
     assert _rel(prob.fem.to_scipy(prob.K) * OP.EPS0, _csr("poisson_K", n)) < 1e-12
     assert _rel(prob.fem.to_scipy(prob.M), _csr("poisson_M", n)) < 1e-12
+
+
+def test_ref_cpp_mode_matches_oracle(cuda):
+    """The C++ SchrodingerSolver's element formulas (QD_ASM_REF_CPP: P1
+    stiffness, potential and mass by the centroid rule) on the GPU equal the
+    oracle's restatement at 1e-12."""
+    from qdsim_b200 import _native as N, fem as F, mesh as Mh
+    m = Mh.StructuredMesh(1, 20, 12, 60e-9, 40e-9)
+    c, V = _elem_inputs(m, v_nm)
+    prob = F.FEMProblem(m, dirichlet=False, device=cuda)
+    out = prob.assemble(c, V, mode=N.QD_ASM_REF_CPP)
+    mstar = HBAR * HBAR / (2 * c)
+    cen = m.centroids()
+    lut = {tuple(p): (ms, v) for p, ms, v in zip(map(tuple, cen), mstar, V)}
+    Hr, Mr = RC.cpp_assembly(m.nodes, m.elems, lambda x, y: lut[(x, y)][0],
+                             lambda x, y: lut[(x, y)][1])
+    assert _rel(prob.to_scipy(out["H"]), Hr) < 1e-12
+    assert _rel(prob.to_scipy(out["M"]), Mr) < 1e-12
