@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--max-iter", type=int, default=4000)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / plain-FP64 / CPU legs")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="enqueue every kernel directly instead of the solver's CUDA graph "
+                         "(for profilers)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -694,7 +697,7 @@ def main():
     args.block = int(cfg["block"])
     db.set_shift(cfg["shift_ev"])
     solve_kw = dict(AT.solve_kwargs(cfg, args.tol, args.precision, args.max_iter),
-                    b=args.block)
+                    b=args.block, graphs=not args.no_graphs)
 
     def step():
         db.assemble()

@@ -3,6 +3,8 @@
     python kernels_bench.py cap_spmm [--prec fp64|fp32] [--b 48] [--launches 10]
     python kernels_bench.py pcg [--iters 32]
     python kernels_bench.py interp [--points 16777216] [--gradient] [--sorted]
+    python kernels_bench.py adjoint [--launches 10]
+    python kernels_bench.py sc [--iters 6]
 
 ``cap_spmm``: ``qd_cap_spmm`` on the open-system pencil of P2 400x200 cells on
 200x100 nm (318,801 DOFs, 3.65M nonzeros) for a block of b complex columns;
@@ -15,6 +17,11 @@ and elements), in random order or sorted by cell (``--sorted``, the order of
 a resampling onto another mesh's nodes); prints ms per launch and GB/s of
 algorithmic bytes (16 B of coordinates in, 8 B per value out, 20 B more with
 gradients and elements, the field read once).
+``adjoint``: ``qd_adjoint`` (element pass and node gather) on the P3 150x75-cell
+dot with the four lowest eigenvectors from the GPU solve; prints ms per call.
+``sc``: the batched self-consistent loop of the p-n junction (P1 300x100
+cells, 64 bias points, 10 states) for a few iterations; prints ms per
+iteration (densities, mixing, the batched eigensolve and PCG inside).
 The launch sequence is fixed, so a profiler can select launches by index.
 """
 from __future__ import annotations
@@ -113,9 +120,45 @@ def interp(points: int, gradient: bool, ordered: bool, launches: int, dev):
             "GBps": alg / (ms * 1e-3) / 1e9, "Gpoints_per_s": points / (ms * 1e-3) / 1e9}
 
 
+def adjoint(launches: int, dev):
+    from qdsim_b200 import adjoint as AD, batch as Bt, fem as F, workloads as W
+    d = W.c3_dot(0)
+    hb = Bt.HostBatch([d])
+    db = Bt.DeviceBatch(hb, dev)
+    db.upload(non_blocking=False)
+    db.assemble()
+    X = db.solve(4, b=8, precision="fp64", tol=1e-12, max_iter=400)[1]
+    prob = F.FEMProblem(d.mesh, device=dev)
+    w = np.array([0.0, 2.0, 1.0, 1.0])
+    AD.energy_gradients(prob, X, w)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        AD.energy_gradients(prob, X, w)
+    e1.record()
+    torch.cuda.synchronize()
+    return {"kernel": "adjoint_elem_kernel + adjoint_node_kernel", "nodes": int(d.mesh.num_nodes),
+            "elements": int(d.mesh.num_elements), "ms_per_call": e0.elapsed_time(e1) / launches}
+
+
+def sc(iters: int, dev):
+    from qdsim_b200 import workloads as W
+    from qdsim_b200.sc import BatchedSC
+    s = BatchedSC(W.c5_junction(64), k=10, device=dev)
+    s.solve(iterations=2)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s.solve(iterations=iters)
+    e1.record()
+    torch.cuda.synchronize()
+    return {"case": "p-n junction, 64 bias points", "ms_per_iteration": e0.elapsed_time(e1) / iters}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["cap_spmm", "pcg", "interp"])
+    ap.add_argument("case", choices=["cap_spmm", "pcg", "interp", "adjoint", "sc"])
     ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--b", type=int, default=48)
     ap.add_argument("--launches", type=int, default=10)
@@ -131,6 +174,10 @@ def main(argv=None):
         r = cap_spmm(a.prec, a.b, a.launches, dev)
     elif a.case == "pcg":
         r = pcg(a.iters, dev)
+    elif a.case == "adjoint":
+        r = adjoint(a.launches, dev)
+    elif a.case == "sc":
+        r = sc(a.iters, dev)
     else:
         r = interp(a.points, a.gradient, a.sorted, a.launches, dev)
     print(json.dumps(r))

@@ -359,7 +359,11 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
   bool ok = true;
   for (int i = 0; i < nsub; ++i) {
     const int sst = i % kCsrStages;
-    const int r = ch.begin + i * kCsrSub + sub;
+    // the sub-tile's rows in two halves of one parity each (even offsets,
+    // then odd): on the row-major lattice of a P2 mesh, rows two apart have
+    // the same stencil, so the k-th neighbours gathered by one warp lie close
+    const int ofs = sub < kCsrSub / 2 ? 2 * sub : 2 * (sub - kCsrSub / 2) + 1;
+    const int r = ch.begin + i * kCsrSub + ofs;
     const bool live = r < ch.end;
     int p0 = 0, p1 = 0;
     if (live) {
