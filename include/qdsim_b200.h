@@ -360,6 +360,29 @@ int qd_fe_interpolate(int order, int32_t nx, int32_t ny, double Lx, double Ly, i
                       const double *d_x, const double *d_y, double *d_value, double *d_grad_x,
                       double *d_grad_y, int32_t *d_element, int outside_zero, void *stream);
 
+/* Field evaluation on an unstructured (refined) order-p triangular mesh over
+ * [0, Lx] x [0, Ly], with the same outputs, outside-point rules and element
+ * choice as qd_fe_interpolate (the reference scans every element,
+ * backend/src/fe_interpolator.cpp:54-431; its refined meshes come from
+ * FEMSolver::adapt_mesh, backend/src/fem.cpp:486-542).  Points are located
+ * through a bucket grid of grid_nx x grid_ny cells: d_cell_ptr
+ * int32[grid_nx * grid_ny + 1] and d_cell_elems list, per cell and in
+ * ascending element order, the elements whose vertex bounding box, padded by
+ * more than the -1e-10 acceptance band, meets the cell.  The nearest-node
+ * search of outside points covers the cells within max(cell width, cell
+ * height) of the point's projection onto the rectangle, which holds the
+ * nearest node when every corner of every cell is a node (a mesh refined from
+ * the grid_nx x grid_ny structured mesh).  d_nadjptr / d_nadj: node adjacency
+ * from qd_node_adjacency (needed only with gradients).  d_nodes double2. */
+int qd_fe_interpolate_tri(int order, int64_t num_nodes, int64_t num_elems,
+                          const double *d_nodes, const int32_t *d_elems, int32_t grid_nx,
+                          int32_t grid_ny, double Lx, double Ly, const int32_t *d_cell_ptr,
+                          const int32_t *d_cell_elems, const int32_t *d_nadjptr,
+                          const int32_t *d_nadj, int nfield, int64_t field_stride,
+                          const double *d_field, int64_t npts, const double *d_x,
+                          const double *d_y, double *d_value, double *d_grad_x, double *d_grad_y,
+                          int32_t *d_element, int outside_zero, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Adjoint (Hellmann-Feynman) gradients of L = Re sum_s w_s E_s with respect
  * to nodal V and the per-element kinetic coefficient c.  M depends on neither,

@@ -64,6 +64,9 @@ SIGNATURES = {
     "qd_fe_interpolate": (_int, [_int, _i32, _i32, _dbl, _dbl, _int, _i64, _p, _i64, _p, _p,
                                  _p, _p, _p, _p, _int, _p]),
     "qd_bounded_wait_selftest": (_int, [_i64, _p, _int, _p, _p, _p]),
+    "qd_fe_interpolate_tri": (_int, [_int, _i64, _i64, _p, _p, _i32, _i32, _dbl, _dbl, _p, _p,
+                                     _p, _p, _int, _i64, _p, _i64, _p, _p, _p, _p, _p, _p, _int,
+                                     _p]),
     "qd_prof_enable": (_int, [_int]),
     "qd_prof_read": (_int, [_p, _p, _int]),
     "qd_sc_potential": (_int, [_i32, _i64, _p, _p, _p, _p]),

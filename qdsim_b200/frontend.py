@@ -168,8 +168,10 @@ class FEMSolver:
         conforming red-green closure (``qdsim_b200.adapt``).  With a
         ``cache_dir`` the refined mesh is stored as mesh_<norm>.npz (<norm> the
         eigenvector's 2-norm, six decimals) and reused when that file exists.
-        The refined mesh is unstructured: the interpolator is not available on
-        it, and the eigensolve runs without the DST preconditioner."""
+        The refined mesh is unstructured: the interpolator locates points
+        through a bucket grid over the original cells (qd_fe_interpolate_tri),
+        and the eigensolve takes the Jacobi preconditioner instead of the DST
+        one, which needs the lattice."""
         psi = np.real(np.asarray(eigenvector)).astype(np.float64).reshape(-1)
         si, nm = self.mesh._si, self.mesh._nm
         cache = (os.path.join(cache_dir, f"mesh_{np.linalg.norm(psi):.6f}.npz")

@@ -167,9 +167,9 @@ def test_frontend_adapt_mesh_host_logic(tmp_path, monkeypatch):
     fem2.adapt_mesh(psi, thr, str(tmp_path))
     np.testing.assert_array_equal(mesh2.get_elements(), mesh.get_elements())
     np.testing.assert_allclose(mesh2.get_nodes(), mesh.get_nodes(), rtol=0, atol=0)
-    # the interpolator needs the lattice
-    with pytest.raises(NotImplementedError):
-        fem.get_interpolator()
+    # the interpolator works on the refined mesh through its bucket grid
+    fi = fem.get_interpolator()
+    assert fi._fi._tri is not None and fi._fi._tri["cell_ptr"].numel() == 10 * 6 + 1
 
 
 def test_adaptive_step_improves_levels_with_fewer_elements():

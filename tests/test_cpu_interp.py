@@ -288,6 +288,42 @@ def test_field_interpolator_rejects_bad_arguments_without_gpu():
         fi.evaluate([0.5], [0.5], np.zeros(m.num_nodes - 1))           # wrong field length
     with pytest.raises(ValueError):
         fi.evaluate([0.5], [0.5], np.zeros((2, 3, m.num_nodes)))       # not (N,) or (F, N)
-    tm = refine(m, np.ones(m.num_elements, bool))
-    with pytest.raises(NotImplementedError):
-        FieldInterpolator(tm, device="cpu")                            # needs the lattice
+    with pytest.raises(TypeError):
+        FieldInterpolator(object(), device="cpu")                      # not a mesh
+
+
+def test_element_buckets_hold_every_candidate():
+    """The bucket grid of a refined mesh: every element is listed in each
+    cell its (padded) bounding box meets, lists ascend, and for seeded
+    points the oracle's containing element is in the bucket of the point's
+    cell (so the kernel's first passing element is the scan's)."""
+    from oracle.adapt import element_gradients
+    from oracle.fem import Mesh
+    from oracle.interp import Interpolator
+    from qdsim_b200.adapt import refine, refinement_flags
+    from qdsim_b200.interp import element_buckets
+    from qdsim_b200.mesh import StructuredMesh
+    m = StructuredMesh(2, 10, 6, 30.0, 18.0)
+    for _ in range(2):
+        psi = np.exp(-((m.nodes[:, 0] - 12.0) ** 2 + (m.nodes[:, 1] - 10.0) ** 2) / 18.0)
+        g = element_gradients(m.nodes, m.elems, psi)
+        m = refine(m, refinement_flags(m, psi, float(np.quantile(np.hypot(*g.T), 0.75))))
+    ptr, cel = element_buckets(m.nodes, m.elems, m.nx, m.ny, m.Lx, m.Ly)
+    assert ptr[0] == 0 and ptr[-1] == cel.size
+    for c in range(m.nx * m.ny):
+        lst = cel[ptr[c]:ptr[c + 1]]
+        assert np.all(np.diff(lst) > 0)
+    hx, hy = m.Lx / m.nx, m.Ly / m.ny
+    for e in range(m.num_elements):
+        v = m.nodes[m.elems[e, :3]]
+        for i in range(int(v[:, 0].min() // hx), min(int(v[:, 0].max() // hx), m.nx - 1) + 1):
+            for j in range(int(v[:, 1].min() // hy), min(int(v[:, 1].max() // hy), m.ny - 1) + 1):
+                c = j * m.nx + i
+                assert e in cel[ptr[c]:ptr[c + 1]]
+    om = Mesh(m.order, m.nx, m.ny, m.Lx, m.Ly, m.nodes, m.elems, m.boundary)
+    it = Interpolator(om)
+    rng = np.random.default_rng(2)
+    for x, y in zip(rng.uniform(0, m.Lx, 200), rng.uniform(0, m.Ly, 200)):
+        e = it.find_element(x, y)
+        c = min(int(y // hy), m.ny - 1) * m.nx + min(int(x // hx), m.nx - 1)
+        assert e in cel[ptr[c]:ptr[c + 1]]

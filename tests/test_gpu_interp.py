@@ -170,3 +170,56 @@ def test_frontend_interpolator_and_interpolated_potential(cuda):
     b.assemble_matrices()
     d = (a.get_H() - b.get_H()).tocoo()
     assert np.abs(d.data).max(initial=0.0) <= 1e-12 * np.abs(a.get_H().data).max()
+
+
+def _refined_pair(order, nx, ny, Lx, Ly, steps=2):
+    """A structured mesh refined twice where a seeded Gaussian varies fastest
+    (the quarter of elements with the largest gradient, red-green closure),
+    and the oracle mesh with the same nodes and elements."""
+    from oracle.adapt import element_gradients
+    from oracle.fem import Mesh
+    from qdsim_b200.adapt import refine, refinement_flags
+    from qdsim_b200.mesh import StructuredMesh
+    m = StructuredMesh(order, nx, ny, Lx, Ly)
+    for _ in range(steps):
+        x, y = m.nodes[:, 0], m.nodes[:, 1]
+        psi = np.exp(-((x - 0.4 * Lx) ** 2 + (y - 0.55 * Ly) ** 2) / (0.02 * Lx * Lx))
+        g = element_gradients(m.nodes, m.elems, psi)
+        m = refine(m, refinement_flags(m, psi, float(np.quantile(np.hypot(g[:, 0], g[:, 1]),
+                                                                 0.75))))
+    om = Mesh(m.order, m.nx, m.ny, m.Lx, m.Ly, m.nodes, m.elems, m.boundary)
+    return m, om
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("outside", ["nearest", "zero"])
+def test_refined_mesh_points_match_oracle_scan(cuda, order, outside):
+    """qd_fe_interpolate_tri on a mesh refined twice: containing elements
+    identical to the oracle's scan over all elements (points on refined edges
+    and vertices, hanging-free green bisections, the boundary band, outside
+    and non-finite points), values 1e-12, gradients 1e-10."""
+    from qdsim_b200.interp import FieldInterpolator
+    m, om = _refined_pair(order, 10, 6, 30.0, 18.0)
+    assert m.num_elements > 2 * 10 * 6
+    rng = np.random.default_rng(order)
+    sm, om0 = _mesh_pair(order, 10, 6, 30.0, 18.0)
+    x, y = _probe_points(om0, rng)
+    # plus the refined mesh's own nodes and edge midpoints of its elements
+    k = rng.choice(m.num_nodes, 80)
+    e = rng.choice(m.num_elements, 60)
+    v = m.nodes[m.elems[e, :3]]
+    x = np.concatenate([x, m.nodes[k, 0], 0.5 * (v[:, 0, 0] + v[:, 1, 0])])
+    y = np.concatenate([y, m.nodes[k, 1], 0.5 * (v[:, 0, 1] + v[:, 1, 1])])
+    fields = rng.standard_normal((2, m.num_nodes))
+    fi = FieldInterpolator(m, device=cuda, outside=outside)
+    r = fi.evaluate(x, y, fields, gradient=True, element=True)
+    ov, ogx, ogy, oe = Interpolator(om).evaluate_many(x, y, fields, gradient=True,
+                                                     zero_outside=outside == "zero")
+    el = r["element"].cpu().numpy()
+    np.testing.assert_array_equal(el, oe)
+    assert (el >= 0).sum() > 300 and (el < 0).sum() > 20
+    np.testing.assert_allclose(r["value"].cpu().numpy(), ov, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(r["grad_x"].cpu().numpy(), ogx, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(r["grad_y"].cpu().numpy(), ogy, rtol=0, atol=1e-10)
+    v = fi.evaluate(x, y, fields)["value"].cpu().numpy()
+    np.testing.assert_allclose(v, ov, rtol=0, atol=1e-12)
