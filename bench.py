@@ -596,35 +596,43 @@ def cap_measurement(dev):
     return out
 
 
-def algorithmic_bytes(hb, counts, k_block):
+def algorithmic_bytes(hb, counts, k_block, mixed=True):
     """Algorithmic bytes per kernel kind, from the per-dot launch counts.
 
-    Per dot and launch (n rows, z nonzeros, block B, s bytes per vector
-    element: 4 in the FP32 phase, 8 in the FP64 phase; v bytes of matrix values
-    per nonzero: 8 for the FP32 phase's (H, M) pairs, 16 for FP64 H and M):
-      spmm   products of [X P] (+ residual W) and of W, per iteration:
-             2 (z (4 + v) + 4 n) + 3 n B s gathered + 7 n B s written
-             (counts[:, 0] counts both SpMM launches of an iteration)
-      gram   9 n B s read
-      dst    4 transform passes: (2 s + 12) bytes per element of W (n B)
-      ortho  3 n B s (C_W, C_P) + 7 n B s read + 4 n B s written
-      update 3 n B s read + 2 n B s written
+    Per dot and launch (n rows, z nonzeros, block B; counts[:, 0] and
+    counts[:, 3] count both SpMM launches of an iteration):
+      FP32 phase (vectors 4 bytes, matrix values an 8-byte FP32 (H, M) pair):
+        spmm   2 (z (4 + 8) + 4 n) + 3 n B 4 gathered + 7 n B 4 written
+        gram   9 n B 4 read;  dst (2 4 + 12) n B;  ortho 14 n B 4;  update 5 n B 4
+      FP64 phase of the plain form (vectors 8, values 16): the same with 8 / 16
+      finishing phase of the mixed form (X, HX, MX FP64; W, P and their
+      products FP32; X's products from the FP64 values, W's from the pairs):
+        spmm   z (4 + 16) + z (4 + 8) + 8 n + n B (8 + 4 + 2 8 + 3 4 + 4 + 2 4)
+        gram   n B (3 8 + 6 4);  dst (2 4 + 12) n B
+        ortho  n B (8 + 2 4) + n B (3 8 + 4 4 + 4 4);  update n B (8 + 2 4 + 8 + 4)
     """
     z = np.asarray(hb.nnz_per_dot, dtype=np.float64)
     n = np.asarray(hb.rows_per_dot, dtype=np.float64)
     B = k_block
     out = {}
-    for ph, s, v in ((0, 4.0, 8.0), (1, 8.0, 16.0)):
-        spmm_iter = 2 * (z * (4 + v) + 4 * n) + 3 * n * B * s + 7 * n * B * s
-        per = {
-            "spmm": (counts[:, ph * 3 + 0] / 2.0) * spmm_iter,
-            "gram": counts[:, ph * 3 + 1] * 9 * n * B * s,
-            "dst_precond": counts[:, ph * 3 + 1] * n * B * (2 * s + 12),
-            "ortho": counts[:, ph * 3 + 1] * 14 * n * B * s,
-            "update": counts[:, ph * 3 + 2] * 5 * n * B * s,
-        }
+
+    def add(per):
         for name, arr in per.items():
             out[name] = out.get(name, 0.0) + float(np.sum(arr))
+
+    for ph in (0, 1):
+        it = counts[:, ph * 3 + 0] / 2.0
+        gr = counts[:, ph * 3 + 1]
+        up = counts[:, ph * 3 + 2]
+        if ph == 1 and mixed:
+            add({"spmm": it * (32 * z + 8 * n + 52 * n * B),
+                 "gram": gr * 48 * n * B, "dst_precond": gr * 20 * n * B,
+                 "ortho": gr * 72 * n * B, "update": up * 28 * n * B})
+            continue
+        s, v = (4.0, 8.0) if ph == 0 else (8.0, 16.0)
+        add({"spmm": it * (2 * (z * (4 + v) + 4 * n) + 3 * n * B * s + 7 * n * B * s),
+             "gram": gr * 9 * n * B * s, "dst_precond": gr * n * B * (2 * s + 12),
+             "ortho": gr * 14 * n * B * s, "update": up * 5 * n * B * s})
     return out
 
 
@@ -776,7 +784,7 @@ def main():
             accuracy = {"error": repr(e)}
 
     # ---- roofline of the dominant kernel ------------------------------------
-    bytes_kind = algorithmic_bytes(hb, counts, args.block)
+    bytes_kind = algorithmic_bytes(hb, counts, args.block, args.precision == "mixed")
     # assembly: nodes (x, y), connectivity, per-element c, nodal V in; H, M out
     a = hb.arrays
     n_nodes, n_el = a["nodes"].shape[0], a["c"].shape[0]

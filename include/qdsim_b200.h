@@ -49,7 +49,9 @@ enum {
 /* eigensolver precision modes */
 enum {
   QD_PREC_FP64 = 0,           /* FP64 vectors throughout (the plain form)         */
-  QD_PREC_MIXED = 1           /* per dot: FP32 vector phase, then FP64 finishing  */
+  QD_PREC_MIXED = 1           /* per dot: FP32 vector phase, then a finishing phase
+                                 with X, HX, MX in FP64 and W, P and their
+                                 products in FP32                                 */
 };
 
 const char *qd_version(void);

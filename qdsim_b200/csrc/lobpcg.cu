@@ -28,9 +28,12 @@
 // when the basis is nearly dependent and the coefficients are large.
 //
 // Precision: QD_PREC_FP64 stores vectors in FP64.  QD_PREC_MIXED runs the
-// same iteration with FP32 vector storage and FP32 update arithmetic (matrix
-// values, SpMM accumulation and Gram sums stay FP64) until the FP32 residual
-// criterion or stagnation, then converts X to FP64 and finishes in FP64.
+// iteration with FP32 vectors, FP32 (H, M) values and FP32 SpMM accumulation
+// (Gram sums, Cholesky/SVQB and Rayleigh-Ritz in FP64) until the FP32 target
+// or stagnation, then finishes with X, HX, MX in FP64 -- one FP64 product of
+// X per iteration gives the residual and the Rayleigh-Ritz blocks of X, and X
+// is updated in FP64 -- while the search directions W, P and their products
+// stay FP32 (W's products by the FP32 SpMM).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <climits>
@@ -178,24 +181,30 @@ spmm_chunk_kernel(const Chunk *chunks, const DotState *st, const int32_t *__rest
 // Explicit products of the current X and P (no drift from implicit updates):
 // HX, MX, HP, MP, the residual W = HX - MX Theta and per-chunk column norms
 // sum r^2 and sum (Mx)^2.  2G threads per row: g < G own X columns, the rest P.
-template <typename TV, int B, typename MAT>
-__global__ void __launch_bounds__(128 * (B / 4), sizeof(TV) == 4 ? 3 : 2)
+// TX is the storage of X and its products, TP that of the search directions
+// P, HP, MP and of W: (double, double) in the plain FP64 form; (double, float)
+// in the mixed form's finishing phase, where X and its products (the residual
+// and the Rayleigh-Ritz blocks of X) stay FP64 and the search directions FP32.
+// Accumulation is FP64 throughout.
+template <typename TX, typename TP, int B, typename MAT>
+__global__ void __launch_bounds__(128 * (B / 4), sizeof(TX) == 4 ? 3 : 2)
 spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
                const int32_t *__restrict__ col, const MAT A, const double *__restrict__ theta,
-               const TV *__restrict__ X, const TV *__restrict__ P, TV *__restrict__ HX,
-               TV *__restrict__ MX, TV *__restrict__ HP, TV *__restrict__ MP,
-               TV *__restrict__ W, double *__restrict__ norms) {
+               const TX *__restrict__ X, const TP *__restrict__ P, TX *__restrict__ HX,
+               TX *__restrict__ MX, TP *__restrict__ HP, TP *__restrict__ MP,
+               TP *__restrict__ W, double *__restrict__ norms) {
   constexpr int G = B / 4;
   constexpr int G2 = 2 * G;
   constexpr int RPP = 64;   // rows per pass (blockDim = 64 * G2)
+  constexpr int PH = sizeof(TX) == 8 ? 1 : 0;
   __shared__ double s_th[B];
   __shared__ double s_red[RPP * G2 * 8];
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
-  if (!sd.run[sizeof(TV) == 8]) return;
+  if (!sd.run[PH]) return;
   const bool with_p = sd.has_p != 0;
   if (threadIdx.x == 0 && blockIdx.x == sd.chunk0)
-    const_cast<DotState *>(st)[ch.dot].launches[sizeof(TV) == 8][0]++;
+    const_cast<DotState *>(st)[ch.dot].launches[PH][0]++;
   if (threadIdx.x < B) s_th[threadIdx.x] = theta[size_t(ch.dot) * B + threadIdx.x];
   __syncthreads();
   const int sub = threadIdx.x / G2, gg = threadIdx.x % G2;
@@ -211,12 +220,11 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   for (int r = ch.begin + sub; r < ch.end; r += RPP) {
     if (!isx && !with_p) {
       double z[4] = {0, 0, 0, 0};
-      qd::V4<TV>::store(HP + size_t(r) * B + 4 * g, z);
-      qd::V4<TV>::store(MP + size_t(r) * B + 4 * g, z);
+      qd::V4<TP>::store(HP + size_t(r) * B + 4 * g, z);
+      qd::V4<TP>::store(MP + size_t(r) * B + 4 * g, z);
       continue;
     }
     double h[4] = {0, 0, 0, 0}, m[4] = {0, 0, 0, 0};
-    const TV *src = isx ? X : P;
     const int p0 = __ldg(rowptr + r), p1 = __ldg(rowptr + r + 1);
 #pragma unroll 4
     for (int p = p0; p < p1; ++p) {
@@ -224,7 +232,8 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
       double hv, mv;
       A.get(p, hv, mv);
       double x[4];
-      qd::V4<TV>::load(src + size_t(j) * B + 4 * g, x);
+      if (isx) qd::V4<TX>::load(X + size_t(j) * B + 4 * g, x);
+      else qd::V4<TP>::load(P + size_t(j) * B + 4 * g, x);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         h[c] = fma(hv, x[c], h[c]);
@@ -237,17 +246,17 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         // residual from the stored (rounded) products, as the iteration sees them
-        const double hq = double(TV(h[c])), mq = double(TV(m[c]));
+        const double hq = double(TX(h[c])), mq = double(TX(m[c]));
         res[c] = hq - s_th[4 * g + c] * mq;
         my_red[(2 * c) * NTX] += res[c] * res[c];
         my_red[(2 * c + 1) * NTX] += mq * mq;
       }
-      qd::V4<TV>::store(HX + o, h);
-      qd::V4<TV>::store(MX + o, m);
-      qd::V4<TV>::store(W + o, res);
+      qd::V4<TX>::store(HX + o, h);
+      qd::V4<TX>::store(MX + o, m);
+      qd::V4<TP>::store(W + o, res);
     } else {
-      qd::V4<TV>::store(HP + o, h);
-      qd::V4<TV>::store(MP + o, m);
+      qd::V4<TP>::store(HP + o, h);
+      qd::V4<TP>::store(MP + o, m);
     }
   }
   // per-chunk column norms (fixed-order reduction over the CTA's rows)
@@ -297,7 +306,7 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
               const double *__restrict__ theta, const float *__restrict__ X,
               const float *__restrict__ P, float *__restrict__ HX, float *__restrict__ MX,
               float *__restrict__ HP, float *__restrict__ MP, float *__restrict__ W,
-              double *__restrict__ norms, int *wait_err) {
+              double *__restrict__ norms, int *wait_err, int ph) {
   constexpr int G = B / 4;
   constexpr int G2 = XP ? 2 * G : G;
   constexpr int NT = kCsrSub * G2;
@@ -312,13 +321,15 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
   __shared__ double s_th[B];
   __shared__ double s_red[XP ? NT * 8 : 1];
 
+  // ph: the phase whose dots this launch serves (the products of X and P only
+  // in the FP32 phase; W's products also in the mixed form's finishing phase)
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
-  if (!sd.run[0]) return;
+  if (!sd.run[ph]) return;
   const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
   if (tid == 0 && blockIdx.x == sd.chunk0)
-    const_cast<DotState *>(st)[ch.dot].launches[0][0]++;
+    const_cast<DotState *>(st)[ch.dot].launches[ph][0]++;
   if (XP && tid < B) s_th[tid] = theta[size_t(ch.dot) * B + tid];
   const int sub = tid / G2, gg = tid % G2;
   const bool isx = gg < G;
@@ -1331,6 +1342,375 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
   pipe.finish(ok, wait_err);
 }
 
+// ---------------------------------------------------------------------------
+// The mixed form's finishing phase: X, HX, MX in FP64 (the residual, the
+// Rayleigh-Ritz blocks of X and the update of X carry the 1e-9 target), the
+// search directions W, P and their products HW, HP, MW, MP in FP32 (the
+// blocks whose rounding enters the Ritz values only through their small
+// coefficients).  The kernels below are the mixed-type forms of the FP32/FP64
+// ones above; all arithmetic on FP64 data is FP64.
+// ---------------------------------------------------------------------------
+
+// Per chunk: partial = [MX^T W, MX^T P] (B x B each) with FP64 MX and FP32 W, P.
+template <int B> using OgMxPipe = qd::MixedPipe<double, 1, float, 2, B, 32, 4>;
+
+template <int B>
+__global__ void __launch_bounds__(256)
+ortho_gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *MX, const float *W,
+                     const float *P, double *partial, int *wait_err) {
+  using PP = OgMxPipe<B>;
+  using C = OgCfg<B>;
+  constexpr int NQ = C::NQ, NT = C::NT, RG = C::RG, NOUT = 2 * B * B;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  double *red = reinterpret_cast<double *>(dsm + PP::BYTES);
+  const Chunk ch = chunks[blockIdx.x];
+  if (!st[ch.dot].run[1]) return;
+  const int tid = threadIdx.x;
+  const bool worker = tid < NT * RG;
+  const int task = tid % NT, rg = tid / NT;
+  const int which = task / (NQ * NQ), bi = (task % (NQ * NQ)) / NQ, bj = task % NQ;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  const void *src[3] = {MX, W, P};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (ok && worker) {
+      const int nr = pipe.rows(i);
+      const double *tm = pipe.tx(i, 0) + 4 * bi;
+      const float *tr = pipe.tw(i, which) + 4 * bj;
+      for (int row = rg; row < nr; row += RG) {
+        double x[4];
+        float y[4];
+        lds4(tm + row * B, x);
+        lds4(tr + row * B, y);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], double(y[b]), acc[a][b]);
+      }
+    }
+    pipe.release(i, ok);
+  }
+  if (!pipe.finish(ok, wait_err)) return;
+  if (worker) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) red[(size_t(rg) * NT + task) * 16 + a * 4 + b] = acc[a][b];
+  }
+  __syncthreads();
+  double *out = partial + size_t(blockIdx.x) * NOUT;
+  for (int e = tid; e < NOUT; e += blockDim.x) {
+    const int w = e / (B * B), ij = e % (B * B), i = ij / B, j = ij % B;
+    const int tk = w * NQ * NQ + (i / 4) * NQ + (j / 4), ab = (i % 4) * 4 + (j % 4);
+    double v = 0.0;
+    for (int g = 0; g < RG; ++g) v += red[(size_t(g) * NT + tk) * 16 + ab];
+    out[e] = v;
+  }
+}
+
+// W <- W - X C_W; with P: P <- P - X C_P, HP <- HP - HX C_P, MP <- MP - MX C_P,
+// FP64 arithmetic on the exact FP32 inputs, each result rounded once to FP32
+// (relative to itself: the cancellation happens before the rounding).
+template <int B> using OaMxPipe = qd::MixedPipe<double, 3, float, 4, B, 16, 4>;
+
+template <int B>
+__global__ void __launch_bounds__(256)
+ortho_apply_mx_kernel(const Chunk *chunks, const DotState *st, const double *csum,
+                      const double *X, const double *HX, const double *MX, float *W, float *P,
+                      float *HP, float *MP, int *wait_err) {
+  using PP = OaMxPipe<B>;
+  constexpr int NOUT = 2 * B * B;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  double *sC = reinterpret_cast<double *>(dsm + PP::BYTES);
+  const Chunk ch = chunks[blockIdx.x];
+  const DotState &sd = st[ch.dot];
+  if (!sd.run[1]) return;
+  const bool with_p = sd.has_p != 0;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < NOUT; e += blockDim.x) sC[e] = csum[size_t(ch.dot) * NOUT + e];
+  const void *src[7] = {X, HX, MX, W, P, HP, MP};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);   // its barrier also publishes sC
+  const int nthr = (int(blockDim.x) / B) * B;
+  const int j = tid % B;
+  const bool owner = tid < nthr;
+  double cw[B], cp[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    cw[q] = sC[q * B + j];
+    cp[q] = sC[B * B + q * B + j];
+  }
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (ok && owner) {
+      const int nr = pipe.rows(i), r0 = pipe.row0(i);
+      const double *tx = pipe.tx(i, 0), *thx = pipe.tx(i, 1), *tmx = pipe.tx(i, 2);
+      const float *tw = pipe.tw(i, 0), *tp = pipe.tw(i, 1), *thp = pipe.tw(i, 2),
+                  *tmp = pipe.tw(i, 3);
+      for (int e = tid; e < nr * B; e += nthr) {
+        const int row = e / B;
+        const size_t o = size_t(r0) * B + e;
+        double dw = 0.0;
+#pragma unroll
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          double t[4];
+          lds4(tx + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) dw = fma(t[u], cw[q4 + u], dw);
+        }
+        W[o] = float(double(tw[e]) - dw);
+        if (with_p) {
+          double dp = 0.0, dhp = 0.0, dmp = 0.0;
+#pragma unroll
+          for (int q4 = 0; q4 < B; q4 += 4) {
+            double t0[4], t1[4], t2[4];
+            lds4(tx + row * B + q4, t0);
+            lds4(thx + row * B + q4, t1);
+            lds4(tmx + row * B + q4, t2);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const double c = cp[q4 + u];
+              dp = fma(t0[u], c, dp);
+              dhp = fma(t1[u], c, dhp);
+              dmp = fma(t2[u], c, dmp);
+            }
+          }
+          P[o] = float(double(tp[e]) - dp);
+          HP[o] = float(double(thp[e]) - dhp);
+          MP[o] = float(double(tmp[e]) - dmp);
+        }
+      }
+    }
+    pipe.release(i, ok);
+  }
+  pipe.finish(ok, wait_err);
+}
+
+// Gram partials of the finishing phase, per chunk A_c = S^T HS, B_c = S^T MS
+// for S = [X W P].  The rows of the X block are formed from the FP64
+// products, (S^T HS)_{x, s} = (H x)^T s (H and M symmetric): HX^T X, HX^T W,
+// HX^T P (and MX^T ...), in FP64; the W and P rows from FP32 data, summed in
+// FP32 within a sub-tile and in FP64 across sub-tiles.  Same task layout and
+// output as gram_kernel<double, B>.
+template <int B> using GramMxPipe = qd::MixedPipe<double, 3, float, 6, B, 32, 3>;
+
+template <int B>
+__global__ void __launch_bounds__(GramCfg<double, B>::THREADS, 2)
+gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *X, const float *W,
+               const float *P, const double *HX, const float *HW, const float *HP,
+               const double *MX, const float *MW, const float *MP, double *partial,
+               int *wait_err) {
+  using C = GramCfg<double, B>;
+  using PP = GramMxPipe<B>;
+  constexpr int m = C::m, NB = C::NB, NT = C::NT, NT2 = C::NT2, RG = C::RG;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  const Chunk ch = chunks[blockIdx.x];
+  if (!st[ch.dot].run[1]) return;
+  const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[1][1]++;
+  const bool worker = tid < NT2 * RG;
+  const int task2 = tid % NT2, rg = tid / NT2;
+  const int which = task2 / NT, task = task2 % NT;   // which: 0 S^T HS, 1 S^T MS
+  int bi = 0, rem = task;
+  while (rem >= NB - bi) {
+    rem -= NB - bi;
+    ++bi;
+  }
+  const int bj = bi + rem;
+  const int bs = (4 * bi) / B, br = (4 * bj) / B, cs = (4 * bi) % B, cr = (4 * bj) % B;
+  // 0: (HX or MX)^T X, 1: (HX or MX)^T (W or P), 2: (W or P)^T (HW, HP, MW or MP)
+  const int kind = bs == 0 ? (br == 0 ? 0 : 1) : 2;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  // pipe blocks: FP64 X, HX, MX; FP32 W, P, HW, HP, MW, MP
+  const void *src[9] = {X, HX, MX, W, P, HW, HP, MW, MP};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (worker && ok) {
+      const int nr = pipe.rows(i);
+      if (kind == 2) {
+        const float *sa_p = pipe.tw(i, bs - 1) + cs;
+        const float *rb_p = pipe.tw(i, 2 + 2 * which + (br - 1)) + cr;
+        float t[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) t[a][b] = 0.f;
+        for (int row = rg; row < nr; row += RG) {
+          float sa[4], rb[4];
+          lds4(sa_p + row * B, sa);
+          lds4(rb_p + row * B, rb);
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) t[a][b] = fmaf(sa[a], rb[b], t[a][b]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] += double(t[a][b]);
+      } else {
+        const double *sa_p = pipe.tx(i, 1 + which) + cs;
+        for (int row = rg; row < nr; row += RG) {
+          double sa[4], rb[4];
+          lds4(sa_p + row * B, sa);
+          if (kind == 0) {
+            lds4(pipe.tx(i, 0) + cr + row * B, rb);
+          } else {
+            float rf[4];
+            lds4(pipe.tw(i, br - 1) + cr + row * B, rf);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) rb[b] = double(rf[b]);
+          }
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(sa[a], rb[b], acc[a][b]);
+        }
+      }
+    }
+    pipe.release(i, ok);
+  }
+  if (!pipe.finish(ok, wait_err)) return;
+  double *out = partial + size_t(blockIdx.x) * 2 * m * m;
+  if (RG > 1) {
+    double *red = reinterpret_cast<double *>(dsm);   // NT2 * 16 doubles < one stage
+    for (int g = 1; g < RG; ++g) {
+      if (worker && rg == g) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) red[task2 * 16 + a * 4 + b] = acc[a][b];
+      }
+      __syncthreads();
+      if (worker && rg == 0) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] += red[task2 * 16 + a * 4 + b];
+      }
+      __syncthreads();
+    }
+  }
+  if (worker && rg == 0) {
+    double *o = out + size_t(which) * m * m;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int i = 4 * bi + a, j = 4 * bj + b;
+        o[i * m + j] = acc[a][b];
+        if (bi != bj) o[j * m + i] = acc[a][b];
+      }
+  }
+}
+
+// X <- S Y in FP64 (X FP64, W and P FP32 exact in FP64); P <- [W P] Y_wp
+// rounded to FP32.
+template <int B> using UpdMxPipe = qd::MixedPipe<double, 1, float, 2, B, 32, 4>;
+
+template <int B>
+__global__ void __launch_bounds__(256)
+update_mx_kernel(const Chunk *chunks, const DotState *st, const double *coef, double *X,
+                 const float *W, float *P, int *wait_err) {
+  constexpr int m = 3 * B;
+  using PP = UpdMxPipe<B>;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  double *sY = reinterpret_cast<double *>(dsm + PP::BYTES);
+  const Chunk ch = chunks[blockIdx.x];
+  if (!st[ch.dot].run[1]) return;
+  const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == st[ch.dot].chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[1][2]++;
+  const double *Yg = coef + size_t(ch.dot) * m * B;
+  for (int i = tid; i < m * B; i += blockDim.x) sY[i] = Yg[i];
+  const void *src[3] = {X, W, P};
+  PP pipe;
+  pipe.init(dsm, src, ch.begin, ch.end);   // its barrier also publishes sY
+  const int nthr = (int(blockDim.x) / B) * B;
+  const int j = tid % B;
+  const bool owner = tid < nthr;
+  double cy[3 * B];
+#pragma unroll
+  for (int q = 0; q < 3 * B; ++q) cy[q] = sY[q * B + j];
+  bool ok = true;
+  for (int i = 0; i < pipe.nsub; ++i) {
+    ok = pipe.wait(i) && ok;
+    if (ok && owner) {
+      const int nr = pipe.rows(i), r0 = pipe.row0(i);
+      const double *tx = pipe.tx(i, 0);
+      const float *tw = pipe.tw(i, 0), *tp = pipe.tw(i, 1);
+      for (int e = tid; e < nr * B; e += nthr) {
+        const int row = e / B;
+        double x = 0.0, p = 0.0;
+#pragma unroll
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          double t[4];
+          lds4(tx + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) x = fma(t[u], cy[q4 + u], x);
+        }
+#pragma unroll
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          float t[4];
+          lds4(tw + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const double v = double(t[u]) * cy[B + q4 + u];
+            x += v;
+            p += v;
+          }
+        }
+#pragma unroll
+        for (int q4 = 0; q4 < B; q4 += 4) {
+          float t[4];
+          lds4(tp + row * B + q4, t);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const double v = double(t[u]) * cy[2 * B + q4 + u];
+            x += v;
+            p += v;
+          }
+        }
+        const size_t o = size_t(r0) * B + e;
+        X[o] = x;
+        P[o] = float(p);
+      }
+    }
+    pipe.release(i, ok);
+  }
+  pipe.finish(ok, wait_err);
+}
+
+// FP32 -> finishing-phase hand-over in the mixed form: X64 = X32 on the rows
+// of the dots that left the FP32 phase this iteration (P, W and the products
+// stay in their FP32 blocks; the first finishing iteration recomputes them).
+template <int B>
+__global__ void transition_x_kernel(const Chunk *chunks, const DotState *st, const float *X32,
+                                    double *X) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!st[ch.dot].switching) return;
+  for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
+    const size_t o = size_t(ch.begin) * B + idx;
+    X[o] = double(X32[o]);
+  }
+}
+
 // out[d][v] = sum over the chunks of dot d of partial[c * nvals + v], in chunk
 // order (deterministic).  One thread per (dot, value): the latency of the
 // chunk loop is hidden by the number of threads instead of being paid
@@ -1422,22 +1802,6 @@ __global__ void loop_control_kernel(const DotState *st, int n, int *count, int c
   }
 }
 
-// FP32 -> FP64 hand-over of the dots that left the FP32 phase this iteration:
-// X64 = X32 on their rows, the other FP64 blocks cleared (P restarts empty).
-template <int B>
-__global__ void transition_rows_kernel(const Chunk *chunks, const DotState *st, const float *X32,
-                                       const float *P32, double *X, double *W, double *P,
-                                       double *HW, double *MW, double *HP, double *MP) {
-  const Chunk ch = chunks[blockIdx.x];
-  if (!st[ch.dot].switching) return;
-  for (int idx = threadIdx.x; idx < (ch.end - ch.begin) * B; idx += blockDim.x) {
-    const size_t o = size_t(ch.begin) * B + idx;
-    X[o] = double(X32[o]);
-    P[o] = double(P32[o]);   // the search direction carries over (its products are explicit)
-    W[o] = HW[o] = MW[o] = HP[o] = MP[o] = 0.0;
-  }
-}
-
 __global__ void transition_state_kernel(DotState *st, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1523,7 +1887,10 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   L.norms = ar.take<double>(size_t(nchunks) * 2 * B);
   L.count = ar.take<int>(4);
   L.wait_err = ar.take<int>(1);
-  for (int i = 0; i < 9; ++i) L.slot[i] = ar.take<double>(size_t(n_rows) * B);
+  // FP64 blocks: all nine in the plain form; X, HX, MX (slots 0, 3, 6) in the
+  // mixed form, whose finishing phase keeps the search directions in FP32
+  for (int i = 0; i < 9; ++i)
+    L.slot[i] = (!mixed || i % 3 == 0) ? ar.take<double>(size_t(n_rows) * B) : nullptr;
   for (int i = 0; i < 9; ++i) L.slot32[i] = mixed ? ar.take<float>(size_t(n_rows) * B) : nullptr;
   // +slack: the FP32 SpMM rounds its bulk copies out to 16-byte boundaries
   L.hm32 = mixed ? ar.take<float2>(size_t(nnz) + 2) : nullptr;
@@ -1605,11 +1972,11 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
     if (smem_attr<spmm32_kernel<B, true>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
     spmm32_kernel<B, true><<<L.nchunks, 128 * G, CsrStage::BYTES, s>>>(
         L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.X, b.P,
-        b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err);
+        b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err, 0);
   } else {
-    spmm_xp_kernel<TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A,
-                                                        L.theta, b.X, b.P, b.HX, b.MX, b.HP,
-                                                        b.MP, b.W, L.norms);
+    spmm_xp_kernel<TV, TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A,
+                                                            L.theta, b.X, b.P, b.HX, b.MX,
+                                                            b.HP, b.MP, b.W, L.norms);
   }
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
@@ -1652,7 +2019,7 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
     if (smem_attr<spmm32_kernel<B, false>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
     spmm32_kernel<B, false><<<L.nchunks, 64 * G, CsrStage::BYTES, s>>>(
         L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W,
-        nullptr, b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err);
+        nullptr, b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, 0);
   } else {
     spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, b.W,
                                                           b.HW, b.MW);
@@ -1685,6 +2052,89 @@ int update_step(const Layout &L, const Bufs<TV> &b, cudaStream_t s) {
   return QD_OK;
 }
 
+// Everything of one iteration up to the Rayleigh-Ritz step for the dots in
+// the mixed form's finishing phase: X, HX, MX in FP64, W, P and their
+// products in FP32 (b32), W's products by the FP32 SpMM.
+template <int B>
+int phase_sequence_mx(const Layout &L, const Bufs<float> &b, const Bufs<double> &x64,
+                      int n_dots, const int32_t *rowptr, const int32_t *col, const double *H,
+                      const double *M, cudaStream_t s) {
+  constexpr int G = B / 4;
+  using GC = GramCfg<double, B>;
+  qd::prof_begin(qd::PK_SPMM, s);
+  spmm_xp_kernel<double, float, B><<<L.nchunks, 128 * G, 0, s>>>(
+      L.chunks, L.st, rowptr, col, qd::MatF64{H, M}, L.theta, x64.X, b.P, x64.HX, x64.MX, b.HP,
+      b.MP, b.W, L.norms);
+  qd::prof_end(qd::PK_SPMM, s);
+  QD_CHECK_LAUNCH();
+  if (L.ntx > 0) {
+    qd::prof_begin(qd::PK_PRECOND, s);
+    cudaError_t e = qd::dst_apply<float>(L.tiles_x, L.ntx, L.rows_x, L.tiles_y, L.nty, L.rows_y,
+                                         &L.st[0].run[1], int(sizeof(DotState) / sizeof(int)),
+                                         L.desc, L.row_off, L.mats, B, b.W, b.W, L.tmp1, L.tmp2,
+                                         L.wait_err, s);
+    qd::prof_end(qd::PK_PRECOND, s);
+    if (e != cudaSuccess) return QD_ERR_CUDA;
+  }
+  if (L.njac > 0) {
+    qd::prof_begin(qd::PK_PRECOND, s);
+    jacobi_apply_kernel<float, B><<<L.nchunks, 256, 0, s>>>(L.chunks, L.st, 1, L.dinv, b.W);
+    qd::prof_end(qd::PK_PRECOND, s);
+    QD_CHECK_LAUNCH();
+  }
+  qd::prof_begin(qd::PK_ORTHO, s);
+  {
+    constexpr size_t bytes = OgMxPipe<B>::BYTES + OgCfg<B>::RED_BYTES;
+    if (smem_attr<ortho_gram_mx_kernel<B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+    ortho_gram_mx_kernel<B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, x64.MX, b.W, b.P,
+                                                          L.partial, L.wait_err);
+  }
+  QD_CHECK_LAUNCH();
+  dot_reduce_kernel<<<dim3((2 * B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, 1, L.partial,
+                                                                         2 * B * B, L.dotsum);
+  QD_CHECK_LAUNCH();
+  {
+    constexpr size_t bytes = OaMxPipe<B>::BYTES + 2 * B * B * sizeof(double);
+    if (smem_attr<ortho_apply_mx_kernel<B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+    ortho_apply_mx_kernel<B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, L.dotsum, x64.X,
+                                                           x64.HX, x64.MX, b.W, b.P, b.HP,
+                                                           b.MP, L.wait_err);
+  }
+  qd::prof_end(qd::PK_ORTHO, s);
+  QD_CHECK_LAUNCH();
+  qd::prof_begin(qd::PK_SPMM, s);
+  if (smem_attr<spmm32_kernel<B, false>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
+  spmm32_kernel<B, false><<<L.nchunks, 64 * G, CsrStage::BYTES, s>>>(
+      L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W, nullptr,
+      b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, 1);
+  qd::prof_end(qd::PK_SPMM, s);
+  QD_CHECK_LAUNCH();
+  qd::prof_begin(qd::PK_GRAM, s);
+  if (smem_attr<gram_mx_kernel<B>>(GramMxPipe<B>::BYTES) != cudaSuccess) return QD_ERR_CUDA;
+  gram_mx_kernel<B><<<L.nchunks, GC::THREADS, GramMxPipe<B>::BYTES, s>>>(
+      L.chunks, L.st, x64.X, b.W, b.P, x64.HX, b.HW, b.HP, x64.MX, b.MW, b.MP, L.partial,
+      L.wait_err);
+  QD_CHECK_LAUNCH();
+  dot_reduce_kernel<<<dim3((2 * 9 * B * B + 255) / 256, n_dots), 256, 0, s>>>(
+      L.st, 1, L.partial, 2 * 9 * B * B, L.gramsum);
+  qd::prof_end(qd::PK_GRAM, s);
+  QD_CHECK_LAUNCH();
+  return QD_OK;
+}
+
+template <int B>
+int update_step_mx(const Layout &L, const Bufs<float> &b, const Bufs<double> &x64,
+                   cudaStream_t s) {
+  qd::prof_begin(qd::PK_UPDATE, s);
+  constexpr size_t bytes = UpdMxPipe<B>::BYTES + 3 * B * B * sizeof(double);
+  if (smem_attr<update_mx_kernel<B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+  update_mx_kernel<B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, L.coef, x64.X, b.W, b.P,
+                                                    L.wait_err);
+  qd::prof_end(qd::PK_UPDATE, s);
+  QD_CHECK_LAUNCH();
+  return QD_OK;
+}
+
 // The iteration loop.  In mixed precision every dot starts in the FP32 phase
 // and switches to the FP64 phase on its own (FP32 target reached, stagnation
 // or iteration cap); both phases advance in every host iteration, so a dot's
@@ -1698,13 +2148,20 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
   QD_CUDA_TRY(cudaFuncSetAttribute(rr_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(rr_smem)));
   // One LOBPCG iteration for every dot (both phases), enqueued on stream q.
+  // The mixed form runs the FP32 phase's sequence for its FP32-phase dots and
+  // the finishing sequence (FP64 X, FP32 search directions) for the others;
+  // the plain form runs the FP64 sequence.
   auto iteration = [&](cudaStream_t q) -> int {
     int st;
     if (mixed) {
       Bufs<float> b32(L.slot32);
       if ((st = phase_sequence<float, B>(L, b32, n_dots, rowptr, col, H, M, q)) != QD_OK) return st;
+      if ((st = phase_sequence_mx<B>(L, b32, b64, n_dots, rowptr, col, H, M, q)) != QD_OK)
+        return st;
+    } else {
+      if ((st = phase_sequence<double, B>(L, b64, n_dots, rowptr, col, H, M, q)) != QD_OK)
+        return st;
     }
-    if ((st = phase_sequence<double, B>(L, b64, n_dots, rowptr, col, H, M, q)) != QD_OK) return st;
     qd::prof_begin(qd::PK_RR, q);
     rr_kernel<B><<<n_dots, 256, rr_smem, q>>>(L.st, L.gramsum, L.norms, L.theta, L.coef,
                                               L.relres, prm);
@@ -1713,15 +2170,13 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
     if (mixed) {
       Bufs<float> b32(L.slot32);
       if ((st = update_step<float, B>(L, b32, q)) != QD_OK) return st;
-    }
-    if ((st = update_step<double, B>(L, b64, q)) != QD_OK) return st;
-    if (mixed) {
-      transition_rows_kernel<B><<<L.nchunks, 256, 0, q>>>(L.chunks, L.st, L.slot32[0],
-                                                          L.slot32[2], b64.X, b64.W, b64.P,
-                                                          b64.HW, b64.MW, b64.HP, b64.MP);
+      if ((st = update_step_mx<B>(L, b32, b64, q)) != QD_OK) return st;
+      transition_x_kernel<B><<<L.nchunks, 256, 0, q>>>(L.chunks, L.st, L.slot32[0], b64.X);
       QD_CHECK_LAUNCH();
       transition_state_kernel<<<(n_dots + 127) / 128, 128, 0, q>>>(L.st, n_dots);
       QD_CHECK_LAUNCH();
+    } else {
+      if ((st = update_step<double, B>(L, b64, q)) != QD_OK) return st;
     }
     return QD_OK;
   };

@@ -90,3 +90,88 @@ struct BlockPipe {
 };
 
 }  // namespace qd
+
+namespace qd {
+
+// The same protocol for a sub-tile of NX blocks of TX followed by NW blocks of
+// TW (e.g. the FP64 blocks X, HX, MX beside the FP32 search directions):
+// tx(i, a) / tw(i, a) return block a of each kind in sub-tile i.  Each block
+// of a stage is one row longer than its data (bank skew, as above); every
+// block offset is a multiple of 16 bytes because B % 4 == 0.
+template <typename TX, int NX, typename TW, int NW, int B, int SUB, int STAGES>
+struct MixedPipe {
+  static constexpr size_t BX = size_t(SUB + 1) * B * sizeof(TX);
+  static constexpr size_t BW = size_t(SUB + 1) * B * sizeof(TW);
+  static constexpr size_t STAGE = NX * BX + NW * BW;
+  static constexpr size_t BAR_OFF = size_t(STAGES) * STAGE;
+  static constexpr size_t BYTES = BAR_OFF + 8 * STAGES;
+  static_assert(B % 4 == 0, "rows of B elements must be 16-byte multiples");
+
+  unsigned char *stage;
+  uint64_t *full;
+  const void *const *src;   // NX + NW block base pointers (global, row-major n x B)
+  int begin, end, nsub;
+
+  __device__ static size_t off(int a) {
+    return a < NX ? size_t(a) * BX : NX * BX + size_t(a - NX) * BW;
+  }
+  __device__ static size_t esz(int a) { return a < NX ? sizeof(TX) : sizeof(TW); }
+
+  __device__ void init(unsigned char *dsm, const void *const *src_, int begin_, int end_) {
+    stage = dsm;
+    full = reinterpret_cast<uint64_t *>(dsm + BAR_OFF);
+    src = src_;
+    begin = begin_;
+    end = end_;
+    nsub = (end - begin + SUB - 1) / SUB;
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < STAGES; ++s) tc::mbar_init(&full[s], 1);
+      tc::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < STAGES && i < nsub; ++i) issue(i);
+  }
+  __device__ int rows(int i) const { return min(SUB, end - (begin + i * SUB)); }
+  __device__ int row0(int i) const { return begin + i * SUB; }
+  __device__ const TX *tx(int i, int a) const {
+    return reinterpret_cast<const TX *>(stage + size_t(i % STAGES) * STAGE + off(a));
+  }
+  __device__ const TW *tw(int i, int a) const {
+    return reinterpret_cast<const TW *>(stage + size_t(i % STAGES) * STAGE + off(NX + a));
+  }
+
+  __device__ void issue(int i) {   // thread 0
+    const int s = i % STAGES;
+    const uint32_t nr = uint32_t(rows(i));
+    uint32_t total = 0;
+#pragma unroll
+    for (int a = 0; a < NX + NW; ++a) total += nr * B * uint32_t(esz(a));
+    tc::mbar_arrive_expect_tx(&full[s], total);
+#pragma unroll
+    for (int a = 0; a < NX + NW; ++a) {
+      const size_t e = esz(a);
+      tc::bulk_g2s(stage + size_t(s) * STAGE + off(a),
+                   static_cast<const unsigned char *>(src[a]) + size_t(row0(i)) * B * e,
+                   nr * B * uint32_t(e), &full[s]);
+    }
+  }
+  __device__ bool wait(int i) {
+    return tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, kPipeWaitNs);
+  }
+  __device__ void release(int i, bool ok) {
+    __syncthreads();
+    if (threadIdx.x == 0 && ok && i + STAGES < nsub) issue(i + STAGES);
+  }
+  __device__ bool finish(bool ok, int *err) {
+    if (!__syncthreads_or(!ok)) return true;
+    if (threadIdx.x == 0) {
+      atomicOr(err, 1);
+      for (int i = nsub - STAGES > 0 ? nsub - STAGES : 0; i < nsub; ++i)
+        tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, kPipeWaitNs);
+    }
+    return false;
+  }
+};
+
+}  // namespace qd

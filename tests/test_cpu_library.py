@@ -45,9 +45,10 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.qd_lobpcg_workspace_size(1, 100, 900, 12, 0, None, None, C.byref(out)) == N.QD_OK
     assert out.value > 9 * 100 * 12 * 8
     fp64 = out.value
-    # mixed precision adds the FP32 vector blocks and FP32 (H, M) pairs
+    # mixed precision: nine FP32 vector blocks, three FP64 ones (X, HX, MX) and
+    # the FP32 (H, M) pairs instead of nine FP64 blocks
     assert L.qd_lobpcg_workspace_size(1, 100, 900, 12, 1, None, None, C.byref(out)) == N.QD_OK
-    assert out.value >= fp64 + 9 * 100 * 12 * 4 + 900 * 8
+    assert out.value >= fp64 - 6 * 100 * 12 * 8 + 9 * 100 * 12 * 4 + 900 * 8
     assert L.qd_pcg_workspace_size(100, 300, C.byref(out)) == N.QD_ERR_INVALID
     ro = np.array([0, 5], np.int32)
     info = np.zeros(4, np.int32)
