@@ -65,6 +65,7 @@ constexpr double kSafety = 1.0;
 constexpr double kRelCap = 1e-2;
 constexpr double kJacobiRel64 = 2e-15;   // relative Jacobi threshold, FP64 phase
 constexpr double kJacobiRel32 = 1e-10;   // FP32 phase
+constexpr double kJacobiRelMx = 1e-12;   // the mixed form's finishing phase
 constexpr double kCholPivot32 = 1e-5;    // smallest Cholesky pivot of the scaled Gram (FP32 phase)
 #ifndef QD_SVQB_TAU64
 #define QD_SVQB_TAU64 1e-12
@@ -647,6 +648,7 @@ struct RRParams {
   int max_iter;    // total iteration cap per dot
   int stag_window; // FP32 iterations without halving the estimate before the switch
   double eig_scale; // floor of |theta| in the relative error estimate (0: none)
+  int mixed;        // the mixed form: its finishing phase has FP32 W and P blocks
 };
 
 // Cyclic Jacobi eigensolver for a symmetric n x n matrix A (leading dimension
@@ -910,7 +912,9 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
 
   // Jacobi threshold: the FP32 phase's Gram matrices carry ~1e-7 relative
   // errors, so resolving the small eigenproblems beyond 1e-10 buys nothing
-  const double jrel = s.phase == 0 ? kJacobiRel32 : kJacobiRel64;
+  // (and the mixed form's finishing phase carries FP32 W and P blocks: below
+  // 1e-12 their rounding is all a rotation would resolve)
+  const double jrel = s.phase == 0 ? kJacobiRel32 : (prm.mixed ? kJacobiRelMx : kJacobiRel64);
 
   // 2. Gram matrices of the dot (summed over its chunks by dot_reduce_kernel)
   const double *gsum = partial + size_t(d) * 2 * m * m;
@@ -1519,16 +1523,39 @@ gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *X, const f
     const_cast<DotState *>(st)[ch.dot].launches[1][1]++;
   const bool worker = tid < NT2 * RG;
   const int task2 = tid % NT2, rg = tid / NT2;
-  const int which = task2 / NT, task = task2 % NT;   // which: 0 S^T HS, 1 S^T MS
-  int bi = 0, rem = task;
-  while (rem >= NB - bi) {
-    rem -= NB - bi;
-    ++bi;
+  // tasks ordered by kind, so that the lanes of a warp share one code path:
+  //   2: (W or P)^T (HW, HP, MW or MP)   bi, bj in [GB, NB)
+  //   1: (HX or MX)^T (W or P)           bi in [0, GB), bj in [GB, NB)
+  //   0: (HX or MX)^T X                  bi, bj in [0, GB)
+  // each kind for S^T HS (which 0), then for S^T MS
+  constexpr int GB = B / 4, T2 = (2 * GB) * (2 * GB + 1) / 2, T1 = GB * 2 * GB,
+                T0 = GB * (GB + 1) / 2;
+  static_assert(T2 + T1 + T0 == NT, "task split");
+  int which, kind, bi, bj;
+  {
+    int t = task2, k, size, base;
+    if (t < 2 * T2) {
+      kind = 2; which = t / T2; k = t % T2; size = 2 * GB; base = GB;
+    } else if ((t -= 2 * T2) < 2 * T1) {
+      kind = 1; which = t / T1; k = t % T1; size = 0; base = 0;
+    } else {
+      t -= 2 * T1;
+      kind = 0; which = t / T0; k = t % T0; size = GB; base = 0;
+    }
+    if (kind == 1) {
+      bi = k / (2 * GB);
+      bj = GB + k % (2 * GB);
+    } else {   // upper triangle of a size x size square starting at base
+      int r = 0;
+      while (k >= size - r) {
+        k -= size - r;
+        ++r;
+      }
+      bi = base + r;
+      bj = base + r + k;
+    }
   }
-  const int bj = bi + rem;
   const int bs = (4 * bi) / B, br = (4 * bj) / B, cs = (4 * bi) % B, cr = (4 * bj) % B;
-  // 0: (HX or MX)^T X, 1: (HX or MX)^T (W or P), 2: (W or P)^T (HW, HP, MW or MP)
-  const int kind = bs == 0 ? (br == 0 ? 0 : 1) : 2;
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -2414,6 +2441,7 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   prm.tol32 = std::max(100.0 * tol, kTol32Floor);
   prm.stag_window = kStagWindow;
   prm.eig_scale = 0.0;
+  prm.mixed = prec_mode == QD_PREC_MIXED ? 1 : 0;
   bool graphs = true;
   const double *x0 = opts ? opts->x0 : nullptr;
   if (opts) {
