@@ -67,6 +67,10 @@ constexpr double kJacobiRel64 = 2e-15;   // relative Jacobi threshold, FP64 phas
 constexpr double kJacobiRel32 = 1e-10;   // FP32 phase
 constexpr double kJacobiRelMx = 1e-12;   // the mixed form's finishing phase
 constexpr double kCholPivot32 = 1e-5;    // smallest Cholesky pivot of the scaled Gram (FP32 phase)
+// ... in the mixed form's finishing phase: a basis of condition number below
+// ~1e4 orthonormalised by Cholesky keeps its orthogonality to ~1e-12, well
+// inside the 1e-9 eigenvalue target; worse bases go to SVQB
+constexpr double kCholPivotMx = 1e-4;
 #ifndef QD_SVQB_TAU64
 #define QD_SVQB_TAU64 1e-12
 #endif
@@ -941,11 +945,13 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   //    Q (m x r) in sT.  FP32 phase: Cholesky B' = L L^T (outer-product form,
   //    one barrier per column) and Q = L^-T, as long as every pivot stays above
   //    kCholPivot32 (the scaled Gram has a unit diagonal, so a pivot is the
-  //    squared distance of a basis vector from the span of the previous ones).
-  //    Otherwise, and always in the FP64 phase: SVQB (Jacobi on B', drop
+  //    squared distance of a basis vector from the span of the previous ones);
+  //    likewise in the mixed form's finishing phase above kCholPivotMx.
+  //    Otherwise, and always in the plain FP64 form: SVQB (Jacobi on B', drop
   //    directions with S < tau max S, Q = U_keep S_keep^-1/2).
   bool chol = false;
-  if (s.phase == 0) {
+  if (s.phase == 0 || prm.mixed) {
+    const double pivot_floor = s.phase == 0 ? kCholPivot32 : kCholPivotMx;
     const int mu = has_p ? m : 2 * B;
     bool usable = true;
     for (int i = 0; i < mu; ++i) usable = usable && sD[i] > 0.0;
@@ -955,7 +961,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
       bool ok = true;
       for (int k = 0; k < mu; ++k) {
         const double piv = sZ[k * m + k];   // final since the previous barrier
-        if (!(piv > kCholPivot32)) {        // every thread reads the same value
+        if (!(piv > pivot_floor)) {         // every thread reads the same value
           ok = false;
           break;
         }
