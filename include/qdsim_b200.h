@@ -335,6 +335,72 @@ int qd_cap_spmm(int32_t n, int b, int vec_fp32, const int32_t *d_rowptr, const i
                 void *d_AX, void *d_MX, int ldy, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Open-system eigensolve: the k eigenvalues nearest sigma of the complex-
+ * symmetric pencil (H + i Himag, M), from block LOBPCG over the nev
+ * eigenvalues of smallest real part, entirely on the device.  Replaces the
+ * dense complex solve of backend/src/schrodinger.cpp:699-818 (regularised
+ * Cholesky of M + Eigen ComplexEigenSolver).
+ *   pencil       CSR of n rows (Dirichlet rows removed), FP64 H, Himag
+ *                (NULL: Hermitian pencil) and M; FP32 copies for the mixed
+ *                form (QD_PREC_MIXED: FP32 vectors and products until the
+ *                residuals reach tol32 or stop improving for 8 iterations,
+ *                then FP64 vectors warm-started from them; QD_PREC_FP64:
+ *                FP64 throughout)
+ *   h_prec       DST preconditioner descriptor of the pencil's lattice
+ *                (qd_dst_prec, one dot; NULL: none), d_prec_mats its
+ *                matrices (qd_dst_matrix_fill layout)
+ *   b            block size, even, 2..48 (>= nev; the projected problem is
+ *                3b x 3b), nev <= b levels must converge, k <= nev returned
+ *   tol          relative residual ||A x - theta M x|| / (||M x|| max(|theta|,
+ *                eig_scale)) every one of the nev lowest Ritz pairs reaches
+ *   seed         start block (uniform complex entries in [-1, 1)^2), or
+ *                d_X0 (complex128 [n][b], FP64 form only)
+ * Rayleigh-Ritz: Hermitian M-orthonormal basis of [X P W] (Cholesky of the
+ * diagonally scaled Gram matrix, SVQB when its pivots fall below 1e-6), the
+ * projected non-Hermitian matrix reduced to Schur form by a Jacobi-like
+ * method on a 4-CTA cluster (qd_complex_schur), Ritz vectors by back-
+ * substitution, the b of smallest real part kept.
+ * Outputs: h_E [2k] (re, im) eigenvalues nearest sigma first (the bilinear
+ * Rayleigh quotients x^T A x / x^T M x), d_Xout complex128 [n][k] with
+ * x^T M x = 1, h_res [k] relative residuals ||A x - E M x|| / (|E| ||M x||),
+ * h_info (complete = 1 when no unconverged Ritz value can lie nearer sigma
+ * than the k-th returned eigenvalue).  Returns QD_ERR_NOT_CONVERGED (outputs
+ * written) when max_iter ends the FP64 phase first.
+ * ------------------------------------------------------------------------- */
+typedef struct qd_cap_info {
+  int32_t iters_fp32, iters_fp64;   /* iterations of each phase */
+  int32_t converged, selected;      /* converged among nev; returned (<= k) */
+  int32_t complete;                 /* certified nearest sigma */
+  int32_t schur_sweeps_max;         /* largest sweep count of a Schur solve */
+  int32_t schur_unconverged;        /* Schur solves stopped by the sweep cap */
+  int32_t pad;
+  double fp32_residual;             /* largest residual at the FP32 hand-over */
+  double kth_distance;              /* |E_k - sigma| of the k-th returned */
+  double unconverged_bound;         /* min Re(theta) - sigma over unconverged */
+  double max_residual;              /* largest h_res */
+} qd_cap_info;
+int qd_cap_lobpcg_workspace_size(int32_t n, int b, int precision, const qd_dst_prec *h_prec,
+                                 size_t *bytes);
+int qd_cap_lobpcg_solve(int32_t n, const int32_t *d_rowptr, const int32_t *d_col,
+                        const double *d_H, const double *d_Himag, const double *d_M,
+                        const float *d_H32, const float *d_Himag32, const float *d_M32,
+                        const qd_dst_prec *h_prec, const void *d_prec_mats, int b, int nev, int k,
+                        double sigma, double tol, double tol32, int max_iter, int precision,
+                        double eig_scale, uint64_t seed, const void *d_X0, double *h_E,
+                        void *d_Xout, double *h_res, qd_cap_info *h_info, void *d_work,
+                        size_t work_bytes, void *stream);
+
+/* Schur form C = Z T Z^H of one n x n complex matrix (n <= 144; complex128,
+ * row-major, leading dimensions ldc and ldt): T upper triangular, Z unitary,
+ * by cyclic 2 x 2 unitary rotations in parallel round-robin order (Stewart's
+ * Jacobi-like method for non-Hermitian matrices) on a 4-CTA cluster; a
+ * Hermitian C gives its eigendecomposition.  Stops after a sweep in which no
+ * element below the diagonal exceeded 1e-14 ||C||_F (QD_ERR_NOT_CONVERGED
+ * after max_sweeps sweeps, outputs written).  h_sweeps: sweeps run. */
+int qd_complex_schur(int n, const void *d_C, int ldc, void *d_T, void *d_Z, int ldt, int max_sweeps,
+                     int *h_sweeps, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Finite-element field evaluation at arbitrary points on the structured
  * order-p mesh of [0, Lx] x [0, Ly] with nx x ny cells (lattice node order,
  * element 2 (cj nx + ci) + t).  Replaces FEInterpolator::interpolate,

@@ -75,6 +75,11 @@ SIGNATURES = {
     "qd_sc_mix": (_int, [_i32, _i64, _int, _int, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "qd_adjoint": (_int, [_int, _i64, _i64, _int, _int, _p, _p, _p, _p, _p, _p, _p,
                           _p, _p, _p, _p]),
+    "qd_cap_lobpcg_workspace_size": (_int, [_i32, _int, _int, _p, _p]),
+    "qd_cap_lobpcg_solve": (_int, [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _int, _int, _int,
+                                   _dbl, _dbl, _dbl, _int, _int, _dbl, _u64, _p, _p, _p, _p, _p,
+                                   _p, _sz, _p]),
+    "qd_complex_schur": (_int, [_int, _p, _int, _p, _p, _int, _int, _p, _p]),
 }
 
 
@@ -91,6 +96,16 @@ LOBPCG_OPTS_DTYPE = _np.dtype([("tol32", _np.float64), ("stag_window", _np.int32
                                ("eig_scale", _np.float64), ("chunk_rows", _np.int32),
                                ("reserved", _np.int32)], align=True)
 assert LOBPCG_OPTS_DTYPE.itemsize == 40
+
+# struct qd_cap_info (include/qdsim_b200.h)
+CAP_INFO_DTYPE = _np.dtype([("iters_fp32", _np.int32), ("iters_fp64", _np.int32),
+                            ("converged", _np.int32), ("selected", _np.int32),
+                            ("complete", _np.int32), ("schur_sweeps_max", _np.int32),
+                            ("schur_unconverged", _np.int32), ("pad", _np.int32),
+                            ("fp32_residual", _np.float64), ("kth_distance", _np.float64),
+                            ("unconverged_bound", _np.float64), ("max_residual", _np.float64)],
+                           align=True)
+assert CAP_INFO_DTYPE.itemsize == 64
 
 
 class QDError(RuntimeError):

@@ -10,17 +10,20 @@ appends a constant imaginary part to real eigenvalues
 shift-invert eigs on the same assembled pencil.
 
 Method: block LOBPCG on the complex pencil for the ``nev`` eigenvalues of
-smallest real part, then the ``k`` of them nearest the shift ``sigma``.
+smallest real part, then the ``k`` of them nearest the shift ``sigma``, in
+``qd_cap_lobpcg_solve`` (qdsim_b200/csrc/cap_lobpcg.cu), every step on the
+device:
  - Products AX, MX from ``qd_cap_spmm`` (one CSR pass for H, Himag, M).
  - Preconditioner: the tensor-core DST preconditioner of the real kinetic
    operator, applied to the real and imaginary parts as separate columns.
  - Rayleigh-Ritz with a Hermitian M-orthonormal basis of [X P W] (Cholesky of
-   the diagonally scaled Gram matrix while it is well conditioned, else SVQB)
-   and the projected non-Hermitian eigenproblem solved in FP64 on the host
-   (3b x 3b, LAPACK); the b Ritz pairs of smallest real part are kept.
+   the diagonally scaled Gram matrix while it is well conditioned, else SVQB);
+   the projected non-Hermitian 3b x 3b eigenproblem goes to Schur form by a
+   Jacobi-like method on a 4-CTA cluster; the b Ritz pairs of smallest real
+   part are kept.
  - Mixed form: FP32 vectors and products until the relative residuals reach
    ``tol32`` (or stop improving), then FP64 vectors warm-started from them.
-   Plain form: FP64 throughout.
+   Plain form: FP64 throughout.  Gram sums and the projected problem are FP64.
  - Final eigenvalues are the bilinear Rayleigh quotients x^T A x / x^T M x
    (stationary for complex-symmetric pencils), eigenvectors are normalised
    x^T M x = 1 as the oracle does.
@@ -30,13 +33,11 @@ smallest real part, then the ``k`` of them nearest the shift ``sigma``.
 """
 from __future__ import annotations
 
-import math
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
 import torch
-from scipy.linalg import solve_triangular
-from threadpoolctl import threadpool_limits
 
 from . import _native as N
 from .eigen import DSTPreconditioner
@@ -72,6 +73,14 @@ class CAPProblem:
         spec = DSTPreconditioner.spec_for(mesh, c_elem, V, shift_ev)
         self.prec = DSTPreconditioner([spec], self.device) if spec is not None else None
         self._pws = None
+        self._work = None
+
+    def workspace(self, nbytes):
+        """Solver workspace of at least nbytes (kept between solves)."""
+        if self._work is None or self._work.numel() < nbytes:
+            self._work = None
+            self._work = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        return self._work
 
     # -- kernels ---------------------------------------------------------------
     def spmm(self, X, AX, MX):
@@ -119,184 +128,55 @@ class CAPProblem:
         return out
 
 
-def _orthonormaliser(GM, drop):
-    """B with B^H GM B = I: Cholesky of the diagonally scaled Gram matrix when
-    its smallest pivot shows the basis is well conditioned (condition number
-    below ~1e6), else SVQB, which also drops dependent directions."""
-    d = np.sqrt(np.maximum(GM.diagonal().real, 0.0))
-    if np.all(d > 0.0):
-        Gs = GM / d[:, None] / d[None, :]
-        try:
-            L = np.linalg.cholesky(0.5 * (Gs + Gs.conj().T))
-        except np.linalg.LinAlgError:
-            L = None
-        if L is not None and np.min(np.abs(L.diagonal())) ** 2 > 1e-6:
-            Linv = solve_triangular(L, np.eye(L.shape[0]), lower=True)
-            return Linv.conj().T / d[:, None]
-    return _svqb(GM, drop)
-
-
-def _svqb(GM, drop):
-    """Hermitian M-orthonormalising transform of a basis from its Gram
-    matrix: B with B^H GM B = I on the numerically independent directions."""
-    d = np.sqrt(np.maximum(GM.diagonal().real, 0.0))
-    ok = d > 0.0
-    dinv = np.where(ok, 1.0 / np.where(ok, d, 1.0), 0.0)
-    Gs = GM * dinv[:, None] * dinv[None, :]
-    Gs = 0.5 * (Gs + Gs.conj().T)
-    lam, U = np.linalg.eigh(Gs)
-    keep = lam > drop * max(lam[-1], 1e-300)
-    return (dinv[:, None] * U[:, keep]) / np.sqrt(lam[keep])[None, :]
-
-
-class _Block:
-    """Basis buffers S = [X P W], AS, MS (complex, [n, 3b]) of one precision."""
-
-    def __init__(self, n, b, dtype, device):
-        z = lambda: torch.zeros(n, 3 * b, dtype=dtype, device=device)  # noqa: E731
-        self.S, self.AS, self.MS = z(), z(), z()
-
-
-def lobpcg_cap(prob: CAPProblem, b: int, nev: int, tol: float, max_iter: int,
-               dtype=torch.complex128, X0=None, seed: int = 1234, eig_scale: float = 0.01,
-               stall: int = 0, on_iter=None):
-    """Block LOBPCG on (A, M) for the nev eigenvalues of smallest real part.
-
-    Returns (theta [b] complex numpy sorted by real part, X [n, b], AX, MX,
-    residuals [b], iterations).  With ``stall`` > 0 the iteration also stops
-    when the largest of the first nev residuals has not decreased for that
-    many iterations (the FP32 phase's hand-over)."""
-    n, dev = prob.n, prob.device
-    drop = 1e-6 if dtype == torch.complex64 else 1e-14
-    cur, nxt = _Block(n, b, dtype, dev), _Block(n, b, dtype, dev)
-    if X0 is None:
-        g = torch.Generator(device="cpu").manual_seed(seed)
-        X0 = torch.view_as_complex(torch.randn(n, b, 2, generator=g, dtype=torch.float64))
-    cur.S[:, :b] = X0.to(dev, dtype)
-    X, AX, MX = cur.S[:, :b], cur.AS[:, :b], cur.MS[:, :b]
-    prob.spmm(X, AX, MX)
-    # initial Rayleigh-Ritz on span(X)
-    Y, theta = _rr(cur, b, b, 0, drop)
-    _combine(cur, nxt, Y, b, b, 0, with_p=False)
-    cur, nxt = nxt, cur
-    prob.spmm(cur.S[:, :b], cur.AS[:, :b], cur.MS[:, :b])
-    npc = 0
-    best, since = math.inf, 0
-    res = np.full(b, np.inf)
-    it = 0
-    for it in range(1, max_iter + 1):
-        X, AX, MX = cur.S[:, :b], cur.AS[:, :b], cur.MS[:, :b]
-        th = torch.from_numpy(theta).to(dev, dtype)
-        R = AX - MX * th[None, :]
-        rn = torch.linalg.vector_norm(R, dim=0).double().cpu().numpy()
-        mn = torch.linalg.vector_norm(MX, dim=0).double().cpu().numpy()
-        res = rn / (np.maximum(mn, 1e-300) * np.maximum(np.abs(theta), eig_scale))
-        if on_iter is not None:
-            on_iter(it, theta, res)
-        worst = float(res[:nev].max())
-        if worst <= tol:
-            break
-        if stall:
-            if worst < 0.9 * best:
-                best, since = worst, 0
-            else:
-                since += 1
-                if since >= stall:
-                    break
-        act = np.nonzero(res > tol)[0]
-        act = act if act.size >= 2 else np.arange(b - 2, b)
-        m = int(act.size)
-        Wc = prob.precondition(R[:, torch.from_numpy(act).to(dev)])
-        w0 = b + npc
-        cur.S[:, w0:w0 + m] = Wc
-        prob.spmm(cur.S[:, w0:w0 + m], cur.AS[:, w0:w0 + m], cur.MS[:, w0:w0 + m])
-        Y, theta = _rr(cur, b, b + npc + m, npc, drop)
-        _combine(cur, nxt, Y, b, b + npc + m, npc, with_p=True)
-        cur, nxt = nxt, cur
-        npc = b
-        # explicit products of the new X (P's products are combined)
-        prob.spmm(cur.S[:, :b], cur.AS[:, :b], cur.MS[:, :b])
-    X, AX, MX = cur.S[:, :b], cur.AS[:, :b], cur.MS[:, :b]
-    return theta, X.clone(), AX.clone(), MX.clone(), res, it
-
-
-def _rr(blk: _Block, b, used, npc, drop):
-    """Ritz pairs of (A, M) on span S[:, :used]: (Y [used, b] device, theta)."""
-    S = blk.S[:, :used]
-    GM = (S.mH @ blk.MS[:, :used]).to(torch.complex128).cpu().numpy()
-    GA = (S.mH @ blk.AS[:, :used]).to(torch.complex128).cpu().numpy()
-    # the projected problem is at most 3b x 3b: one BLAS thread (a threaded
-    # BLAS on matrices this small only contends with the host's other work)
-    with threadpool_limits(limits=1, user_api="blas"):
-        return _rr_small(GM, GA, b, drop, blk.S)
-
-
-def _rr_small(GM, GA, b, drop, like):
-    Bm = _orthonormaliser(0.5 * (GM + GM.conj().T), drop)
-    C = Bm.conj().T @ GA @ Bm
-    w, V = np.linalg.eig(C)
-    order = np.argsort(w.real, kind="stable")[:b]
-    Y = Bm @ V[:, order]
-    # Hermitian M-normalise the Ritz vectors (x^H M x = 1)
-    nrm = np.sqrt(np.maximum(np.sum(Y.conj() * (GM @ Y), axis=0).real, 1e-300))
-    Y = Y / nrm[None, :]
-    return torch.from_numpy(Y).to(like.device, like.dtype), w[order]
-
-
-def _combine(cur: _Block, nxt: _Block, Y, b, used, npc, with_p):
-    """nxt.X = cur.S Y; nxt.P = cur.S[:, b:] Y[b:] (and the same for AS, MS)."""
-    for src, dst in ((cur.S, nxt.S), (cur.AS, nxt.AS), (cur.MS, nxt.MS)):
-        dst[:, :b].copy_(src[:, :used] @ Y)
-        if with_p:
-            dst[:, b:2 * b].copy_(src[:, b:used] @ Y[b:])
-
-
-def solve_nearest(prob, k: int = 20, sigma: float = -0.05, nev: int = 40, b: int = 48,
-                  precision: str = "mixed", tol: float = 1e-9, tol32: float = 1e-4,
-                  max_iter: int = 2000, seed: int = 1234, eig_scale: float = 0.01) -> CAPResult:
-    """The k eigenvalues nearest sigma from the nev lowest (by real part) of a
-    problem exposing ``n``, ``device``, ``spmm`` and ``precondition``."""
-    info = {"block": b, "nev": nev, "precision": precision}
-    X0 = None
-    it32 = 0
-    if precision == "mixed":
-        _, X, _, _, res32, it32 = lobpcg_cap(prob, b, nev, tol32, max_iter, dtype=torch.complex64,
-                                             seed=seed, eig_scale=eig_scale, stall=8)
-        X0 = X.to(torch.complex128)
-        info["fp32_residual"] = float(res32[:nev].max())
-    elif precision != "fp64":
+def solve_nearest(prob: CAPProblem, k: int = 20, sigma: float = -0.05, nev: int = 40,
+                  b: int = 48, precision: str = "mixed", tol: float = 1e-9, tol32: float = 1e-4,
+                  max_iter: int = 2000, seed: int = 1234, eig_scale: float = 0.01,
+                  X0: torch.Tensor | None = None) -> CAPResult:
+    """The k eigenvalues nearest sigma from the nev lowest (by real part),
+    by ``qd_cap_lobpcg_solve`` on the device (block b, even, <= 48)."""
+    if precision not in ("mixed", "fp64"):
         raise ValueError("precision must be 'mixed' or 'fp64'")
-    th, X, AX, MX, res, it64 = lobpcg_cap(prob, b, nev, tol, max_iter, dtype=torch.complex128,
-                                          X0=X0, seed=seed, eig_scale=eig_scale)
-    info.update(iters_fp32=int(it32), iters_fp64=int(it64), iterations=int(it32 + it64))
-    E, Xn, rres, sel = nearest_from_block(th, X, AX, MX, res, k, sigma, nev, tol)
-    info.update(sel)
-    return CAPResult(E, Xn, rres, info)
-
-
-def nearest_from_block(theta, X, AX, MX, res, k, sigma, nev, tol):
-    """Bilinear Rayleigh quotients of the converged block columns, x^T M x = 1
-    normalisation, the k nearest sigma and the completeness check."""
-    xtax = (X * AX).sum(dim=0)
-    xtmx = (X * MX).sum(dim=0)
-    E = (xtax / xtmx).cpu().numpy()
-    s = torch.sqrt(xtmx)
-    Xn, AXn, MXn = X / s[None, :], AX / s[None, :], MX / s[None, :]
-    Et = torch.from_numpy(E).to(X.device)
-    R = AXn - MXn * Et[None, :]
-    rres = (torch.linalg.vector_norm(R, dim=0) /
-            (torch.linalg.vector_norm(MXn, dim=0) * torch.abs(Et))).cpu().numpy()
-    conv = np.asarray(res) <= tol
-    conv[nev:] = False
-    idx_c = np.nonzero(conv)[0]
-    pick = idx_c[np.argsort(np.abs(E[idx_c] - sigma), kind="stable")[:k]]
-    dk = float(np.abs(E[pick] - sigma).max()) if pick.size else math.inf
-    unconv = np.nonzero(~conv)[0]
-    bound = float(np.asarray(theta)[unconv].real.min() - sigma) if unconv.size else math.inf
-    sel = dict(converged=int(conv.sum()), complete=bool(pick.size == k and dk < bound),
-               kth_distance=dk, unconverged_bound=bound,
-               max_residual=float(rres[pick].max()) if pick.size else math.inf)
-    return E[pick], Xn[:, torch.from_numpy(pick).to(X.device)], rres[pick], sel
+    if X0 is not None and precision != "fp64":
+        raise ValueError("a start block is taken by the FP64 form only")
+    L = N.lib()
+    pm = N.QD_PREC_MIXED if precision == "mixed" else N.QD_PREC_FP64
+    desc = prob.prec.desc if prob.prec is not None else None
+    nb = C.c_size_t()
+    N.check(L.qd_cap_lobpcg_workspace_size(prob.n, b, pm, N.ptr(desc), C.byref(nb)),
+            "qd_cap_lobpcg_workspace_size")
+    work = prob.workspace(nb.value)
+    E = np.zeros(2 * k)
+    res = np.zeros(k)
+    info = np.zeros(1, dtype=N.CAP_INFO_DTYPE)
+    Xout = torch.empty(prob.n, k, dtype=torch.complex128, device=prob.device)
+    x0 = None
+    if X0 is not None:
+        x0 = X0.to(prob.device, torch.complex128).contiguous()
+        if tuple(x0.shape) != (prob.n, b):
+            raise ValueError("X0 must be [n, b]")
+    st = L.qd_cap_lobpcg_solve(
+        prob.n, N.ptr(prob.fem.d_rowptr), N.ptr(prob.fem.d_col), N.ptr(prob.H), N.ptr(prob.G),
+        N.ptr(prob.M), N.ptr(prob.H32), N.ptr(prob.G32), N.ptr(prob.M32), N.ptr(desc),
+        N.ptr(prob.prec.d_mats) if prob.prec is not None else None, b, nev, k, sigma, tol, tol32,
+        max_iter, pm, eig_scale, seed, N.ptr(x0), N.ptr(E), N.ptr(Xout), N.ptr(res),
+        N.ptr(info), N.ptr(work), work.numel(), stream_ptr())
+    N.check(st, "qd_cap_lobpcg_solve", allow=(N.QD_ERR_NOT_CONVERGED,))
+    f = info[0]
+    sel = int(f["selected"])
+    out = {"block": b, "nev": nev, "precision": precision,
+           "iters_fp32": int(f["iters_fp32"]), "iters_fp64": int(f["iters_fp64"]),
+           "iterations": int(f["iters_fp32"] + f["iters_fp64"]),
+           "converged": int(f["converged"]), "complete": bool(f["complete"]),
+           "kth_distance": float(f["kth_distance"]),
+           "unconverged_bound": float(f["unconverged_bound"]),
+           "max_residual": float(f["max_residual"]),
+           "schur_sweeps_max": int(f["schur_sweeps_max"]),
+           "schur_unconverged": int(f["schur_unconverged"]),
+           "status": N.status_string(st)}
+    if precision == "mixed":
+        out["fp32_residual"] = float(f["fp32_residual"])
+    Ec = E[0::2] + 1j * E[1::2]
+    return CAPResult(Ec[:sel].copy(), Xout[:, :sel], res[:sel].copy(), out)
 
 
 class CAPSolver:

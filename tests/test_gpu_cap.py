@@ -130,3 +130,47 @@ def test_cap_nearest20_at_config_size(cuda, precision):
     assert err.max() <= 1e-9, (err.max(), res.info)
     assert len({int(np.argmin(np.abs(res.E - g))) for g in gold}) == 20
     assert res.residual.max() < 1e-8, res.residual.max()
+
+
+@pytest.mark.parametrize("n", [7, 48, 143, 144])
+def test_complex_schur_kernel_matches_restatement(cuda, n):
+    """qd_complex_schur (4-CTA cluster, matrix rows in distributed shared
+    memory) against its restatement and LAPACK on a Hermitian matrix with a
+    non-Hermitian perturbation: unitary Z, upper triangular T, C = Z T Z^H,
+    the eigenvalues, and the sweep count of the same rotation sequence."""
+    import ctypes as C
+    import torch
+    from qdsim_b200 import _native as N
+    from qdsim_b200.fem import stream_ptr
+    from oracle.cap_lobpcg import schur_jacobi
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    B = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    Cm = 0.5 * (A + A.conj().T) + np.diag(np.linspace(0, 5, n)) + 0.02 * B
+    ld = n + 3
+    Cd = torch.zeros(n, ld, dtype=torch.complex128, device=cuda)
+    Cd[:, :n] = torch.from_numpy(Cm)
+    Td = torch.zeros(n, ld, dtype=torch.complex128, device=cuda)
+    Zd = torch.zeros_like(Td)
+    sw = C.c_int()
+    N.check(N.lib().qd_complex_schur(n, N.ptr(Cd), ld, N.ptr(Td), N.ptr(Zd), ld, 60, C.byref(sw),
+                                     stream_ptr()), "qd_complex_schur")
+    T, Z = Td[:, :n].cpu().numpy(), Zd[:, :n].cpu().numpy()
+    nc = np.linalg.norm(Cm)
+    assert np.abs(Z.conj().T @ Z - np.eye(n)).max() < 1e-12
+    assert np.abs(np.tril(T, -1)).max() <= 1e-13 * nc
+    assert np.linalg.norm(Z @ T @ Z.conj().T - Cm) <= 1e-12 * nc
+    w = np.linalg.eigvals(Cm)
+    assert max(np.min(np.abs(w - x)) for x in np.diag(T)) <= 1e-10 * np.abs(w).max()
+    _, _, sw_ref, conv = schur_jacobi(Cm)
+    assert conv and abs(sw.value - sw_ref) <= 1, (sw.value, sw_ref)
+
+
+def test_cap_solver_rejects_bad_blocks(cuda):
+    from qdsim_b200 import _native as N, cap as CP
+    d = _c2(20, 10)
+    solver = CP.CAPSolver(d.mesh, d.c, d.V, d.W, device=cuda)
+    for b in (7, 50):
+        with pytest.raises(N.QDError) as e:
+            solver.solve(k=4, sigma=-0.05, nev=6, b=b)
+        assert e.value.status == N.QD_ERR_INVALID
