@@ -551,7 +551,8 @@ def cap_measurement(dev):
         secs = time.perf_counter() - t0
         r = {"seconds": secs, "iterations": res.info["iterations"],
              "iters_fp32": res.info["iters_fp32"], "iters_fp64": res.info["iters_fp64"],
-             "complete": res.info["complete"], "max_residual": res.info["max_residual"]}
+             "complete": res.info["complete"], "max_residual": res.info["max_residual"],
+             "schur_sweeps_max": res.info["schur_sweeps_max"]}
         if gold is not None:
             err = np.array([np.min(np.abs(res.E - g)) / abs(g) for g in gold])
             good = int((err <= 1e-9).sum()) if res.info["complete"] else 0

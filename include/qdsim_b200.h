@@ -358,7 +358,7 @@ int qd_cap_spmm(int32_t n, int b, int vec_fp32, const int32_t *d_rowptr, const i
  * Rayleigh-Ritz: Hermitian M-orthonormal basis of [X P W] (Cholesky of the
  * diagonally scaled Gram matrix, SVQB when its pivots fall below 1e-6), the
  * projected non-Hermitian matrix reduced to Schur form by a Jacobi-like
- * method on a 4-CTA cluster (qd_complex_schur), Ritz vectors by back-
+ * method on an 8-CTA cluster (qd_complex_schur), Ritz vectors by back-
  * substitution, the b of smallest real part kept.
  * Outputs: h_E [2k] (re, im) eigenvalues nearest sigma first (the bilinear
  * Rayleigh quotients x^T A x / x^T M x), d_Xout complex128 [n][k] with
@@ -393,7 +393,7 @@ int qd_cap_lobpcg_solve(int32_t n, const int32_t *d_rowptr, const int32_t *d_col
 /* Schur form C = Z T Z^H of one n x n complex matrix (n <= 144; complex128,
  * row-major, leading dimensions ldc and ldt): T upper triangular, Z unitary,
  * by cyclic 2 x 2 unitary rotations in parallel round-robin order (Stewart's
- * Jacobi-like method for non-Hermitian matrices) on a 4-CTA cluster; a
+ * Jacobi-like method for non-Hermitian matrices) on an 8-CTA cluster; a
  * Hermitian C gives its eigendecomposition.  Stops after a sweep in which no
  * element below the diagonal exceeded 1e-14 ||C||_F (QD_ERR_NOT_CONVERGED
  * after max_sweeps sweeps, outputs written).  h_sweeps: sweeps run. */

@@ -19,7 +19,7 @@ device:
  - Rayleigh-Ritz with a Hermitian M-orthonormal basis of [X P W] (Cholesky of
    the diagonally scaled Gram matrix while it is well conditioned, else SVQB);
    the projected non-Hermitian 3b x 3b eigenproblem goes to Schur form by a
-   Jacobi-like method on a 4-CTA cluster; the b Ritz pairs of smallest real
+   Jacobi-like method on an 8-CTA cluster; the b Ritz pairs of smallest real
    part are kept.
  - Mixed form: FP32 vectors and products until the relative residuals reach
    ``tol32`` (or stop improving), then FP64 vectors warm-started from them.

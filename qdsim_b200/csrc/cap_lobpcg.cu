@@ -21,7 +21,7 @@
 //                 similarity rotations, each zeroing the element below the
 //                 diagonal of its 2 x 2 block, in the parallel round-robin
 //                 order.  The matrix and Z live in the distributed shared
-//                 memory of a 4-CTA cluster (rows split between the CTAs).
+//                 memory of an 8-CTA cluster (rows split between the CTAs).
 //   Ritz pairs    the b eigenvalues of smallest real part, eigenvectors by
 //                 back-substitution in T, Y = B Z y, x^H M x = 1
 //   update        X = S Y, P = S[:, b:] Y[b:], AP, MP       cap_combine_kernel
@@ -46,8 +46,8 @@ namespace {
 
 constexpr int kMaxB = 48;            // largest block (3b <= 144)
 constexpr int kMaxU = 3 * kMaxB;     // leading dimension of every small matrix
-constexpr int kJC = 4;               // CTAs per cluster of the Schur kernel
-constexpr int kJRows = kMaxU / kJC;  // matrix rows per CTA (36)
+constexpr int kJC = 8;               // CTAs per cluster of the Schur kernel
+constexpr int kJRows = kMaxU / kJC;  // rows of Z per CTA (18)
 constexpr int kJThreads = 512;
 constexpr double kSchurTol = 1e-14;   // |c_qp| <= kSchurTol ||C||_F counts as zero
 constexpr int kSchurSweeps = 60;
@@ -163,19 +163,27 @@ cap_resid_kernel(int32_t n, int b, int ld, const T2 *__restrict__ AX, const T2 *
   }
 }
 
-// res_j = ||R_j|| / (max(||MX_j||, 1e-300) max(|theta_j|, eig_scale))
-__global__ void cap_resnorm_kernel(int nblk, int b, const double *__restrict__ part,
-                                   const double2 *__restrict__ theta, double eig_scale,
-                                   double *__restrict__ res) {
+// res_j = ||R_j|| / (max(||MX_j||, 1e-300) max(|theta_j|, eig_scale)); one
+// warp per sum (lanes over the CTA partials in a fixed order, then a fixed
+// shuffle tree)
+__global__ void __launch_bounds__(1024)
+cap_resnorm_kernel(int nblk, int b, const double *__restrict__ part,
+                   const double2 *__restrict__ theta, double eig_scale, double *__restrict__ res) {
+  __shared__ double s_sum[2 * kMaxB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = warp; q < 2 * b; q += 32) {
+    const int off = q < b ? q : kMaxB + (q - b);
+    double acc = 0.0;
+    for (int k = lane; k < nblk; k += 32) acc += part[size_t(k) * 2 * kMaxB + off];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) s_sum[q] = acc;
+  }
+  __syncthreads();
   const int c = threadIdx.x;
   if (c >= b) return;
-  double rn = 0.0, mn = 0.0;
-  for (int k = 0; k < nblk; ++k) {
-    rn += part[size_t(k) * 2 * kMaxB + c];
-    mn += part[size_t(k) * 2 * kMaxB + kMaxB + c];
-  }
   const double th = sqrt(cabs2(theta[c]));
-  res[c] = sqrt(rn) / (fmax(sqrt(mn), 1e-300) * fmax(th, eig_scale));
+  res[c] = sqrt(s_sum[c]) / (fmax(sqrt(s_sum[b + c]), 1e-300) * fmax(th, eig_scale));
 }
 
 // out[r][i] = R[r][act[i]] (the active residual columns, contiguous)
@@ -534,45 +542,80 @@ cap_small_gemm_kernel(int m, int nn, int k, const int *m_dev, const int *n_dev, 
 // round of the parallel round-robin order, every pair (p, q), p < q, gets
 // the unitary U whose first column is the eigenvector of the 2 x 2 block
 // [[c_pp, c_pq], [c_qp, c_qq]] for the eigenvalue nearer c_pp, and
-// C <- U^H C U, Z <- Z U, which zeroes c_qp.  A sweep is n-1 rounds (n
+// C <- U^H C U, Z <- Z U, which zeroes c_qp.  A sweep is N-1 rounds (N = n
 // rounded up to even with a decoupled zero row and column); the iteration
 // stops after a sweep in which no |c_qp| exceeded rel_tol ||C||_F.  For a
 // Hermitian input the result is its eigendecomposition (T diagonal).
 //
-// Cluster of kJC CTAs; CTA r owns rows [r RP, (r + 1) RP) of C and of Z
-// (RP = ceil(n_even / kJC)).  Per round: (1) the owner of pair k (k mod kJC)
-// reads the 2 x 2 block (rows p and q, local or in a peer CTA's shared
-// memory), forms U and writes it to every CTA; (2) it rotates rows p and q;
-// (3) every CTA rotates the columns of its own rows of C and Z.  Cluster
-// barriers separate the steps; every thread of every CTA passes the same
-// barriers (the loop bounds and the stop test are cluster-uniform).
+// Cluster of kJC CTAs.  The pairs are split into kJC contiguous ranges, and
+// CTA r keeps the rows of C of the indices paired in its range, so that a
+// pair's 2 x 2 block and both of its rows are local.  Round-robin order as
+// a ring: index N-1 stays in pair 0, the other indices move one place per
+// round (the first member of pair k+1 to pair k, the second member of pair
+// k-1 to pair k; pair 0's moving member to pair 1, the last pair's second
+// member becomes its first), so only the two rows at each range boundary
+// change CTA per round.  Z's rows are split statically (only its columns
+// rotate).  Per round:
+//   (1) warp 0 forms the rotations of the CTA's pairs and writes them to
+//       every CTA; the other warps rotate Z's columns by the previous round's
+//       rotations;
+//   (2) cluster barrier; each CTA applies U_a^H B U_b to every 2 x 2 block B
+//       of its rows (rows of pair a, columns of pair b);
+//   (3) the boundary rows go to the neighbours' landing rows; cluster
+//       barrier; each CTA moves the landed rows into the freed slots.
+// Every thread of every CTA passes the same barriers (the loop bounds and
+// the stop test are cluster-uniform).
 // ---------------------------------------------------------------------------
 struct Rot {
   double2 u1, u2;   // U = [[u1, -conj(u2)], [u2, conj(u1)]]
-  int on;
-  int pad;
+  int on, p, q, pad;
 };
 
-constexpr size_t kJSmem = 2 * size_t(kJRows) * kMaxU * sizeof(double2) + (kMaxU / 2) * sizeof(Rot) +
-                          4 * sizeof(double) + 4 * sizeof(int) + 64;
+constexpr int kJPairs = kMaxU / 2 / kJC;     // pairs per CTA (9)
+constexpr int kJSlots = 2 * kJPairs + 2;     // rows of C per CTA: pairs' rows + 2 landing rows
+constexpr int kLandL = 2 * kJPairs, kLandR = 2 * kJPairs + 1;
+constexpr size_t kJSmem = size_t(kJSlots) * kMaxU * sizeof(double2) +     // C rows
+                          size_t(kJRows) * kMaxU * sizeof(double2) +      // Z rows
+                          2 * (kMaxU / 2) * sizeof(Rot) +
+                          (2 * kJPairs + kJSlots + 4) * sizeof(int) + 2 * sizeof(double) + 64;
 
-__device__ __forceinline__ void rr_pair(int r, int k, int N, int &p, int &q) {
-  const int M = N - 1;
-  if (k == 0) {
-    p = M;
-    q = r;
-  } else {
-    p = (r + k) % M;
-    q = (r - k + M) % M;
+__device__ __forceinline__ Rot make_rot(double2 a, double2 bb, double2 c, double2 d, double thresh2,
+                                        int p, int q) {
+  Rot R;
+  R.u1 = make_double2(1.0, 0.0);
+  R.u2 = make_double2(0.0, 0.0);
+  R.on = 0;
+  R.p = p;
+  R.q = q;
+  R.pad = 0;
+  if (cabs2(c) > thresh2) {
+    // eigenvalue lambda of the 2 x 2 block nearer a: with h = (a - d)/2,
+    // disc = sqrt(h^2 + b c), lambda - a = b c / g, g the larger of h +- disc
+    // (entries are O(||C||), far from the FP64 range limits: plain formulas)
+    const double2 h = cscale(csub(a, d), 0.5);
+    const double2 z = cadd(cmul(h, h), cmul(bb, c));
+    const double r = sqrt(cabs2(z));
+    double2 disc = make_double2(0.0, 0.0);
+    if (r > 0.0) {
+      const double t = sqrt(0.5 * (r + fabs(z.x)));
+      const double v = 0.5 * z.y / t;
+      disc = z.x >= 0.0 ? make_double2(t, v) : make_double2(fabs(v), copysign(t, z.y));
+    }
+    const double2 g1 = cadd(h, disc), g2 = csub(h, disc);
+    const double2 g = cabs2(g1) >= cabs2(g2) ? g1 : g2;
+    const double gg = cabs2(g);
+    const double2 delta = gg > 0.0 ? cscale(cmul(cmul(bb, c), cconj(g)), 1.0 / gg) : make_double2(0.0, 0.0);
+    // eigenvector [lambda - d, c] = [2h + delta, c] (c != 0)
+    const double2 v1 = cadd(cscale(h, 2.0), delta), v2 = c;
+    const double inv = rsqrt(cabs2(v1) + cabs2(v2));
+    R.u1 = cscale(v1, inv);
+    R.u2 = cscale(v2, inv);
+    R.on = 1;
   }
-  if (p > q) {
-    const int t = p;
-    p = q;
-    q = t;
-  }
+  return R;
 }
 
-__global__ void __cluster_dims__(kJC, 1, 1) __launch_bounds__(kJThreads)
+__global__ void __cluster_dims__(kJC, 1, 1) __launch_bounds__(kJThreads, 1)
 cap_schur_kernel(int n_fix, const int *__restrict__ n_dev, const int *__restrict__ skip_if_set,
                  const double2 *__restrict__ Cin, int ldi, double2 *__restrict__ Tout,
                  double2 *__restrict__ Zout, int ldo, int max_sweeps, double rel_tol,
@@ -582,149 +625,228 @@ cap_schur_kernel(int n_fix, const int *__restrict__ n_dev, const int *__restrict
   if (skip_if_set && *skip_if_set) return;
   const int n = n_dev ? *n_dev : n_fix;
   const int N = n + (n & 1);
-  const int RP = (N + kJC - 1) / kJC;
+  const int M = N - 1;                       // the fixed index
+  const int npairs = N / 2, K = npairs - 1;  // K: last pair
+  const int P = (npairs + kJC - 1) / kJC;    // pairs per CTA
+  const int RZ = (N + kJC - 1) / kJC;        // Z rows per CTA
   const int rank = int(cluster.block_rank());
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   extern __shared__ __align__(16) unsigned char jsm[];
-  double2 *Cl = reinterpret_cast<double2 *>(jsm);
-  double2 *Zl = Cl + size_t(kJRows) * kMaxU;
-  Rot *rot = reinterpret_cast<Rot *>(Zl + size_t(kJRows) * kMaxU);
-  double *s_norm = reinterpret_cast<double *>(rot + kMaxU / 2);
-  int *s_cnt = reinterpret_cast<int *>(s_norm + 4);   // [2]: rotations this sweep (by parity)
-
-  const int row0 = rank * RP, nrow = max(0, min(RP, N - row0));
-  double nrm = 0.0;
-  for (int e = tid; e < nrow * N; e += kJThreads) {
-    const int li = e / N, j = e % N, i = row0 + li;
-    const double2 v = (i < n && j < n) ? Cin[size_t(i) * ldi + j] : make_double2(0.0, 0.0);
-    Cl[li * kMaxU + j] = v;
-    Zl[li * kMaxU + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
-    nrm += cabs2(v);
-  }
-  // CTA sum of |c|^2 (warp shuffles, then one atomic per warp in a fixed
-  // pattern is not needed: a shared array summed by thread 0 in warp order)
+  double2 *Cs = reinterpret_cast<double2 *>(jsm);
+  double2 *Zl = Cs + size_t(kJSlots) * kMaxU;
+  Rot *rot = reinterpret_cast<Rot *>(Zl + size_t(kJRows) * kMaxU);   // [2][kMaxU / 2]
+  int *pos = reinterpret_cast<int *>(rot + 2 * (kMaxU / 2));         // [2 kJPairs] slot of (pair, member)
+  int *idx = pos + 2 * kJPairs;                                       // [kJSlots] index held by a slot
+  int *s_cnt = idx + kJSlots;                                         // [2] rotations this sweep
+  double *s_norm = reinterpret_cast<double *>(s_cnt + 4);
   __shared__ double s_w[kJThreads / 32];
-#pragma unroll
-  for (int o = 16; o; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-  if ((tid & 31) == 0) s_w[tid >> 5] = nrm;
+  __shared__ int s_new[2 * kJPairs], s_fill[2][2];
+
+  const int k0 = rank * P, k1 = min(npairs, k0 + P), np = max(0, k1 - k0);
+  const int z0 = rank * RZ, nz = max(0, min(RZ, N - z0));
+  // round-0 positions: pair 0 = (M, 0), pair k = (k, M - k)
+  if (tid < 2 * np) {
+    const int k = k0 + tid / 2, m = tid & 1;
+    pos[tid] = tid;
+    idx[tid] = k == 0 ? (m == 0 ? M : 0) : (m == 0 ? k : M - k);
+  }
   if (tid == 0) {
     s_cnt[0] = s_cnt[1] = 0;
+    idx[kLandL] = idx[kLandR] = -1;
   }
   __syncthreads();
+  double nrm = 0.0;
+  for (int e = tid; e < 2 * np * N; e += kJThreads) {
+    const int sl = e / N, j = e % N, i = idx[sl];
+    const double2 v = (i < n && j < n) ? Cin[size_t(i) * ldi + j] : make_double2(0.0, 0.0);
+    Cs[sl * kMaxU + j] = v;
+    nrm += cabs2(v);
+  }
+  for (int e = tid; e < nz * N; e += kJThreads) {
+    const int li = e / N, j = e % N;
+    Zl[li * kMaxU + j] = make_double2(z0 + li == j ? 1.0 : 0.0, 0.0);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+  if (lane == 0) s_w[warp] = nrm;
+  __syncthreads();
   if (tid == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kJThreads / 32; ++w) s += s_w[w];
-    s_norm[0] = s;
+    double sacc = 0.0;
+    for (int w = 0; w < kJThreads / 32; ++w) sacc += s_w[w];
+    s_norm[0] = sacc;
   }
   cluster.sync();
   double fro2 = 0.0;
   for (int r = 0; r < kJC; ++r) fro2 += *cluster.map_shared_rank(s_norm, r);
-  const double thresh = rel_tol * sqrt(fro2);
+  const double thresh2 = rel_tol * rel_tol * fro2;
 
-  auto elem = [&](int i, int j) -> double2 * {   // element (i, j) of C, any CTA
-    const int owner = i / RP;
-    double2 *base = owner == rank ? Cl : cluster.map_shared_rank(Cl, owner);
-    return base + (i - owner * RP) * kMaxU + j;
+  // Z <- Z U for the rotations of one round (rotation table `par`)
+  // items (row, pair) spread evenly over threads t0..t0+nt-1; the quotient
+  // by npairs in single precision is exact for these small integers
+  const float inv_np = 1.0f / float(npairs);
+  auto rotate_z = [&](int par, int t0, int nt) {
+    for (int e = tid - t0; e < nz * npairs; e += nt) {
+      const int li = int((float(e) + 0.5f) * inv_np), k = e - li * npairs;
+      const Rot &R = rot[par * (kMaxU / 2) + k];
+      if (!R.on) continue;
+      double2 *z = Zl + li * kMaxU;
+      const double2 x = z[R.p], y = z[R.q];
+      z[R.p] = cadd(cmul(x, R.u1), cmul(y, R.u2));
+      z[R.q] = csub(cmul(y, cconj(R.u1)), cmul(x, cconj(R.u2)));
+    }
   };
 
-  const int npairs = N / 2;
   int sweeps = 0, converged = N < 2;
+  int g = 0;   // rounds run
   for (int sw = 0; sw < max_sweeps && N >= 2; ++sw) {
-    const int par = sw & 1;
-    for (int rr = 0; rr < N - 1; ++rr) {
-      // (1) rotations of my pairs, broadcast to every CTA
-      for (int k = rank + kJC * tid; k < npairs; k += kJC * kJThreads) {
-        int p, q;
-        rr_pair(rr, k, N, p, q);
-        const double2 a = *elem(p, p), bb = *elem(p, q), c = *elem(q, p), d = *elem(q, q);
-        Rot R;
-        R.u1 = make_double2(1.0, 0.0);
-        R.u2 = make_double2(0.0, 0.0);
-        R.on = 0;
-        R.pad = 0;
-        if (sqrt(cabs2(c)) > thresh) {
-          // eigenvalue lambda of the 2 x 2 block nearer a: with h = (a - d)/2,
-          // disc = sqrt(h^2 + b c), a - lambda = -b c / g, g the larger of h +- disc
-          const double2 h = cscale(csub(a, d), 0.5);
-          const double2 disc = csqrt(cadd(cmul(h, h), cmul(bb, c)));
-          const double2 g1 = cadd(h, disc), g2 = csub(h, disc);
-          const double2 g = cabs2(g1) >= cabs2(g2) ? g1 : g2;
-          const double2 delta = cabs2(g) > 0.0 ? cdiv(cmul(bb, c), g) : make_double2(0.0, 0.0);
-          // eigenvector [lambda - d, c] = [2h + delta, c] (c != 0)
-          double2 v1 = cadd(cscale(h, 2.0), delta), v2 = c;
-          const double nv = sqrt(cabs2(v1) + cabs2(v2));
-          v1 = cscale(v1, 1.0 / nv);
-          v2 = cscale(v2, 1.0 / nv);
-          R.u1 = v1;
-          R.u2 = v2;
-          R.on = 1;
-          atomicAdd(&s_cnt[par], 1);
+    const int cpar = sw & 1;
+    for (int rr = 0; rr < N - 1; ++rr, ++g) {
+      const int par = g & 1;
+      // (1) rotations of my pairs (warp 0), Z by the previous round (others)
+      if (warp == 0) {
+        if (lane < np) {
+          const int k = k0 + lane;
+          int sp = pos[2 * lane], sq = pos[2 * lane + 1];
+          int p = idx[sp], q = idx[sq];
+          if (p > q) {
+            const int t = p; p = q; q = t;
+            const int u = sp; sp = sq; sq = u;
+          }
+          const Rot R = make_rot(Cs[sp * kMaxU + p], Cs[sp * kMaxU + q], Cs[sq * kMaxU + p],
+                                 Cs[sq * kMaxU + q], thresh2, p, q);
+          if (R.on) atomicAdd(&s_cnt[cpar], 1);
+          for (int dst = 0; dst < kJC; ++dst) {
+            Rot *rp = dst == rank ? rot : cluster.map_shared_rank(rot, dst);
+            rp[par * (kMaxU / 2) + k] = R;
+          }
         }
-        for (int dst = 0; dst < kJC; ++dst) {
-          Rot *rp = dst == rank ? rot : cluster.map_shared_rank(rot, dst);
-          rp[k] = R;
+      } else if (g > 0) {
+        if (tid >= 64) rotate_z(par ^ 1, 64, kJThreads - 64);
+      }
+      cluster.sync();
+      // (2) 2 x 2 blocks of my rows: U_a^H B U_b
+      for (int e = tid; e < np * npairs; e += kJThreads) {
+        const int t = int((float(e) + 0.5f) * inv_np), kb = e - t * npairs;
+        const Rot &Ra = rot[par * (kMaxU / 2) + k0 + t];
+        const Rot &Rb = rot[par * (kMaxU / 2) + kb];
+        if (!Ra.on && !Rb.on) continue;
+        int sp = pos[2 * t], sq = pos[2 * t + 1];
+        if (idx[sp] != Ra.p) {
+          const int u = sp; sp = sq; sq = u;
+        }
+        double2 *rp = Cs + sp * kMaxU, *rq = Cs + sq * kMaxU;
+        double2 x0 = rp[Rb.p], x1 = rp[Rb.q], y0 = rq[Rb.p], y1 = rq[Rb.q];
+        if (Ra.on) {   // rows: [p; q] <- U_a^H [p; q]
+          const double2 nx0 = cadd(cmulc(Ra.u1, x0), cmulc(Ra.u2, y0));
+          const double2 nx1 = cadd(cmulc(Ra.u1, x1), cmulc(Ra.u2, y1));
+          const double2 ny0 = csub(cmul(Ra.u1, y0), cmul(Ra.u2, x0));
+          const double2 ny1 = csub(cmul(Ra.u1, y1), cmul(Ra.u2, x1));
+          x0 = nx0; x1 = nx1; y0 = ny0; y1 = ny1;
+        }
+        if (Rb.on) {   // columns: [p' q'] <- [p' q'] U_b
+          const double2 cu1 = cconj(Rb.u1), cu2 = cconj(Rb.u2);
+          const double2 nx0 = cadd(cmul(x0, Rb.u1), cmul(x1, Rb.u2));
+          const double2 nx1 = csub(cmul(x1, cu1), cmul(x0, cu2));
+          const double2 ny0 = cadd(cmul(y0, Rb.u1), cmul(y1, Rb.u2));
+          const double2 ny1 = csub(cmul(y1, cu1), cmul(y0, cu2));
+          x0 = nx0; x1 = nx1; y0 = ny0; y1 = ny1;
+        }
+        if (kb == k0 + t && Ra.on) y0 = make_double2(0.0, 0.0);   // the zeroed c_qp
+        rp[Rb.p] = x0;
+        rp[Rb.q] = x1;
+        rq[Rb.p] = y0;
+        rq[Rb.q] = y1;
+      }
+      __syncthreads();
+      // (3) ring shift: member 0 of my first pair goes left, member 1 of my
+      // last pair goes right (each to the neighbour's landing row)
+      const bool out_l = np > 0 && k0 >= 1, out_r = np > 0 && k1 - 1 < K;
+      if (out_l || out_r) {
+        for (int e = tid; e < 2 * N; e += kJThreads) {
+          const int side = e / N, j = e % N;
+          if (side == 0 ? !out_l : !out_r) continue;
+          const int src = side == 0 ? pos[0] : pos[2 * (np - 1) + 1];
+          const int dst_rank = side == 0 ? rank - 1 : rank + 1;
+          double2 *peer = cluster.map_shared_rank(Cs, dst_rank);
+          peer[(side == 0 ? kLandR : kLandL) * kMaxU + j] = Cs[src * kMaxU + j];
+          if (j == 0) cluster.map_shared_rank(idx, dst_rank)[side == 0 ? kLandR : kLandL] = idx[src];
+        }
+      }
+      if (K >= 1) {
+        // new slot of every position (k, m), k in my range (one thread each):
+        // the source position's slot if local, else a landing row, moved into
+        // the slot freed by the row that left on the same side
+        if (tid < 2) s_fill[tid][0] = -1;
+        __syncthreads();
+        if (tid < 2 * np) {
+          const int t = tid >> 1, m = tid & 1, k = k0 + t;
+          int sk, sm;   // source position
+          if (m == 0) {
+            if (k == 0) { sk = 0; sm = 0; }
+            else if (k < K) { sk = k + 1; sm = 0; }
+            else { sk = K; sm = 1; }
+          } else {
+            if (k == 0) { sk = 1; sm = 0; }
+            else if (k == 1) { sk = 0; sm = 1; }
+            else { sk = k - 1; sm = 1; }
+          }
+          int slot;
+          if (sk >= k0 && sk < k1) {
+            slot = pos[2 * (sk - k0) + sm];
+          } else if (sk < k0) {   // arrives from the left
+            slot = pos[0];
+            s_fill[0][0] = kLandL;
+            s_fill[0][1] = slot;
+          } else {                 // arrives from the right
+            slot = pos[2 * (np - 1) + 1];
+            s_fill[1][0] = kLandR;
+            s_fill[1][1] = slot;
+          }
+          s_new[tid] = slot;
         }
       }
       cluster.sync();
-      // (2) row rotations of my pairs: rows p, q <- U^H [row p; row q]
-      {
-        const int mine = (npairs - rank + kJC - 1) / kJC;   // pairs k = rank + kJC t
-        for (int e = tid; e < mine * N; e += kJThreads) {
-          const int k = rank + kJC * (e / N), j = e % N;
-          const Rot R = rot[k];
-          if (!R.on) continue;
-          int p, q;
-          rr_pair(rr, k, N, p, q);
-          double2 *cp = elem(p, j), *cq = elem(q, j);
-          const double2 x = *cp, y = *cq;
-          *cp = cadd(cmulc(R.u1, x), cmulc(R.u2, y));
-          *cq = csub(cmul(R.u1, y), cmul(R.u2, x));
+      // landed rows into the freed slots, then the new positions
+      if (K >= 1) {
+        for (int e = tid; e < 2 * N; e += kJThreads) {
+          const int side = e / N, j = e % N;
+          const int from = s_fill[side][0];
+          if (from < 0) continue;
+          const int to = s_fill[side][1];
+          Cs[to * kMaxU + j] = Cs[from * kMaxU + j];
+          if (j == 0) idx[to] = idx[from];
         }
+        if (tid < 2 * np) pos[tid] = s_new[tid];
       }
-      cluster.sync();
-      // (3) column rotations of my rows of C and Z: [col p, col q] <- [col p, col q] U
-      for (int e = tid; e < nrow * npairs; e += kJThreads) {
-        const int li = e / npairs, k = e % npairs;
-        const Rot R = rot[k];
-        if (!R.on) continue;
-        int p, q;
-        rr_pair(rr, k, N, p, q);
-        double2 *crow = Cl + li * kMaxU, *zrow = Zl + li * kMaxU;
-        const double2 cu1 = cconj(R.u1), cu2 = cconj(R.u2);
-        double2 x = crow[p], y = crow[q];
-        crow[p] = cadd(cmul(x, R.u1), cmul(y, R.u2));
-        crow[q] = csub(cmul(y, cu1), cmul(x, cu2));
-        if (row0 + li == q) crow[p] = make_double2(0.0, 0.0);   // the zeroed element
-        x = zrow[p];
-        y = zrow[q];
-        zrow[p] = cadd(cmul(x, R.u1), cmul(y, R.u2));
-        zrow[q] = csub(cmul(y, cu1), cmul(x, cu2));
-      }
-      cluster.sync();
+      __syncthreads();
     }
     ++sweeps;
     int total = 0;
-    for (int r = 0; r < kJC; ++r) total += cluster.map_shared_rank(s_cnt, r)[par];
+    for (int r = 0; r < kJC; ++r) total += cluster.map_shared_rank(s_cnt, r)[cpar];
     cluster.sync();   // every CTA has read the counters
-    if (tid == 0) s_cnt[par] = 0;
+    if (tid == 0) s_cnt[cpar] = 0;
     __syncthreads();
     if (total == 0) {
       converged = 1;
       break;
     }
   }
-  for (int e = tid; e < nrow * N; e += kJThreads) {
-    const int li = e / N, j = e % N, i = row0 + li;
-    if (i < n && j < n) {
-      Tout[size_t(i) * ldo + j] = Cl[li * kMaxU + j];
-      Zout[size_t(i) * ldo + j] = Zl[li * kMaxU + j];
-    }
+  if (g > 0) rotate_z((g - 1) & 1, 0, kJThreads);   // the last round's rotations
+  __syncthreads();
+  for (int e = tid; e < 2 * np * N; e += kJThreads) {
+    const int sl = e / N, j = e % N;
+    const int s_ = pos[sl], i = idx[s_];
+    if (i < n && j < n) Tout[size_t(i) * ldo + j] = Cs[s_ * kMaxU + j];
+  }
+  for (int e = tid; e < nz * N; e += kJThreads) {
+    const int li = e / N, j = e % N, i = z0 + li;
+    if (i < n && j < n) Zout[size_t(i) * ldo + j] = Zl[li * kMaxU + j];
   }
   if (rank == 0 && tid == 0 && sweeps_out) {
     sweeps_out[0] = sweeps;
     sweeps_out[1] = converged;
   }
-  cluster.sync();   // no CTA leaves while a peer may still read its memory
+  cluster.sync();   // no CTA leaves while a peer may still write to it
 }
 
 // ---------------------------------------------------------------------------
@@ -1182,7 +1304,7 @@ int lobpcg_run(const Problem &P, Work &w, Blocks &bl, int &cur, double tol, int 
     cap_resid_kernel<T2><<<kResBlocks, 256, 0, s>>>(n, b, ld, AS(cur), MS(cur), w.theta,
                                                     static_cast<T2 *>(w.R), w.rpart);
     QD_CHECK_LAUNCH();
-    cap_resnorm_kernel<<<1, 64, 0, s>>>(kResBlocks, b, w.rpart, w.theta, P.eig_scale, w.res);
+    cap_resnorm_kernel<<<1, 1024, 0, s>>>(kResBlocks, b, w.rpart, w.theta, P.eig_scale, w.res);
     QD_CHECK_LAUNCH();
     int hstatus = 0, hsweeps[2] = {0, 1};
     QD_CUDA_TRY(cudaMemcpyAsync(res.data(), w.res, b * sizeof(double), cudaMemcpyDeviceToHost, s));

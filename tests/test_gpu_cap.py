@@ -134,7 +134,7 @@ def test_cap_nearest20_at_config_size(cuda, precision):
 
 @pytest.mark.parametrize("n", [7, 48, 143, 144])
 def test_complex_schur_kernel_matches_restatement(cuda, n):
-    """qd_complex_schur (4-CTA cluster, matrix rows in distributed shared
+    """qd_complex_schur (8-CTA cluster, matrix rows in distributed shared
     memory) against its restatement and LAPACK on a Hermitian matrix with a
     non-Hermitian perturbation: unitary Z, upper triangular T, C = Z T Z^H,
     the eigenvalues, and the sweep count of the same rotation sequence."""
