@@ -5,6 +5,7 @@
     python kernels_bench.py interp [--points 16777216] [--gradient] [--sorted]
     python kernels_bench.py adjoint [--launches 10]
     python kernels_bench.py sc [--iters 6]
+    python kernels_bench.py cap_solve [--prec fp64|mixed] [--cells 400]
 
 ``cap_spmm``: ``qd_cap_spmm`` on the open-system pencil of P2 400x200 cells on
 200x100 nm (318,801 DOFs, 3.65M nonzeros) for a block of b complex columns;
@@ -22,6 +23,10 @@ dot with the four lowest eigenvectors from the GPU solve; prints ms per call.
 ``sc``: the batched self-consistent loop of the p-n junction (P1 300x100
 cells, 64 bias points, 10 states) for a few iterations; prints ms per
 iteration (densities, mixing, the batched eigensolve and PCG inside).
+``cap_solve``: one open-system solve (``qd_cap_lobpcg_solve``: the 20
+eigenvalues nearest -0.05 eV from the lowest 40, block 48) on P2 cells x
+cells/2 on 200x100 nm, after a 3-iteration warm-up solve; prints seconds,
+iterations and the largest Schur sweep count.
 The launch sequence is fixed, so a profiler can select launches by index.
 """
 from __future__ import annotations
@@ -156,10 +161,27 @@ def sc(iters: int, dev):
     return {"case": "p-n junction, 64 bias points", "ms_per_iteration": e0.elapsed_time(e1) / iters}
 
 
+def cap_solve(prec: str, cells: int, dev):
+    import time
+    from qdsim_b200.cap import CAPSolver
+    from qdsim_b200.workloads import c2_dot
+    d = c2_dot(0, nx=cells, ny=cells // 2)
+    solver = CAPSolver(d.mesh, d.c, d.V, d.W, device=dev)
+    solver.solve(k=20, sigma=-0.05, nev=40, b=48, precision=prec, max_iter=3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = solver.solve(k=20, sigma=-0.05, nev=40, b=48, precision=prec, tol=1e-9)
+    torch.cuda.synchronize()
+    return {"case": f"open system, P2 {cells}x{cells // 2} cells", "prec": prec,
+            "seconds": time.perf_counter() - t0, "iterations": res.info["iterations"],
+            "schur_sweeps_max": res.info["schur_sweeps_max"], "complete": res.info["complete"]}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["cap_spmm", "pcg", "interp", "adjoint", "sc"])
-    ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("case", choices=["cap_spmm", "pcg", "interp", "adjoint", "sc", "cap_solve"])
+    ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32", "mixed"])
+    ap.add_argument("--cells", type=int, default=400)
     ap.add_argument("--b", type=int, default=48)
     ap.add_argument("--launches", type=int, default=10)
     ap.add_argument("--iters", type=int, default=32)
@@ -178,6 +200,8 @@ def main(argv=None):
         r = adjoint(a.launches, dev)
     elif a.case == "sc":
         r = sc(a.iters, dev)
+    elif a.case == "cap_solve":
+        r = cap_solve("mixed" if a.prec == "mixed" else "fp64", a.cells, dev)
     else:
         r = interp(a.points, a.gradient, a.sorted, a.launches, dev)
     print(json.dumps(r))
