@@ -42,14 +42,19 @@ constexpr int kMaxAdj = 16;   // incident elements per row (pattern builder enfo
 // lanes (four rows per warp), P2 rows 16 (two per warp), P3 rows a warp.
 template <int K> struct RowShape;
 template <> struct RowShape<3> { static constexpr int LPR = 8, THREADS = 128; };
-template <> struct RowShape<6> { static constexpr int LPR = 16, THREADS = 256; };
-template <> struct RowShape<10> { static constexpr int LPR = 32, THREADS = 256; };
+template <> struct RowShape<6> { static constexpr int LPR = 16, THREADS = 128; };
+template <> struct RowShape<10> { static constexpr int LPR = 32, THREADS = 128; };
 
-template <int K>
+// One row's staged data: the incident elements' geometry and nodal V (W),
+// then the row's element-matrix entries (t, b) = row a_t of element t's H, M
+// (and Himag) at local column b, each computed once by one lane.
+template <int K, bool HAS_W>
 struct __align__(16) RowStage {
   double cA[kMaxAdj], A[kMaxAdj], g00[kMaxAdj], g01[kMaxAdj], g11[kMaxAdj];
   double V[kMaxAdj][K];
-  double W[kMaxAdj][K];
+  double W[HAS_W ? kMaxAdj : 1][K];
+  double he[kMaxAdj][K], me[kMaxAdj][K];
+  double we[HAS_W ? kMaxAdj : 1][K];
   int a[kMaxAdj];
 };
 
@@ -70,7 +75,7 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
   constexpr int LPR = RowShape<K>::LPR;
   constexpr int RPB = RowShape<K>::THREADS / LPR;   // rows in flight per block
   __shared__ __align__(16) double s_tab[NT];
-  __shared__ RowStage<K> s_stage[RPB];
+  __shared__ RowStage<K, HAS_W> s_stage[RPB];
   // Mr, Sxx, Sxy, Syy as stored; the potential table transposed to T[ab][l]
   // so that a contribution reads its K weights contiguously
   for (int i = threadIdx.x; i < NT; i += blockDim.x) {
@@ -85,7 +90,7 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
   const double *Mr = s_tab, *Sxx = s_tab + KK, *Sxy = s_tab + 2 * KK, *Syy = s_tab + 3 * KK;
   const double *T = s_tab + 4 * KK;
   const int seg = threadIdx.x / LPR, lane = threadIdx.x % LPR;
-  RowStage<K> &st = s_stage[seg];
+  RowStage<K, HAS_W> &st = s_stage[seg];
   // rows of one warp are independent: every shuffle and warp barrier names
   // only the lanes of this row's segment
   const unsigned mask = LPR == 32 ? 0xffffffffu
@@ -130,6 +135,63 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
       }
     }
     __syncwarp(mask);
+    // the row's element-matrix entries: lane per (element t, local column b)
+    for (int idx = lane; idx < m * K; idx += LPR) {
+      const int t = idx / K, b = idx - t * K;
+      const int a = st.a[t];
+      const int ab = a * K + b;
+      const double At = st.A[t];
+      double hk, mk, wk = 0.0;
+      if (mode == QD_ASM_FEM) {
+        hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]);
+        const double *tw = T + ab * K;
+        double vs = 0.0, ws = 0.0;
+        if constexpr (K % 2 == 0) {
+          const double2 *t2 = reinterpret_cast<const double2 *>(tw);
+          const double2 *v2 = reinterpret_cast<const double2 *>(st.V[t]);
+#pragma unroll
+          for (int l = 0; l < K / 2; ++l) {
+            const double2 tl = t2[l], vl = v2[l];
+            vs += vl.x * tl.x;
+            vs += vl.y * tl.y;
+          }
+          if constexpr (HAS_W) {
+            const double2 *w2 = reinterpret_cast<const double2 *>(st.W[t]);
+#pragma unroll
+            for (int l = 0; l < K / 2; ++l) {
+              const double2 tl = t2[l], wl = w2[l];
+              ws += wl.x * tl.x;
+              ws += wl.y * tl.y;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int l = 0; l < K; ++l) {
+            vs += st.V[t][l] * tw[l];
+            if constexpr (HAS_W) ws += st.W[t][l] * tw[l];
+          }
+        }
+        hk += At * vs;
+        wk = At * ws;
+        mk = At * Mr[ab];
+      } else if (mode == QD_ASM_REF_CYTHON) {
+        hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]);
+        if (a == b) hk += (a == 0 ? 1.0 : 2.0) * (st.V[t][0] * At / 3.0);
+        mk = At * Mr[ab];
+      } else if (mode == QD_ASM_REF_FIXED) {
+        hk = (st.cA[t] / 3.0) * (a == b ? 1.0 : 0.5);
+        if (a == b) hk += st.V[t][0] * At / 3.0;
+        mk = At * Mr[ab];
+      } else {
+        hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]) +
+             st.V[t][0] * At / 9.0;
+        mk = At / 9.0;
+      }
+      st.he[t][b] = hk;
+      st.me[t][b] = mk;
+      if constexpr (HAS_W) st.we[t][b] = wk;
+    }
+    __syncwarp(mask);
     const int rp = rowptr[r];
     const int L = rowptr[r + 1] - rp;
     const int cbase = cptr[r];
@@ -146,57 +208,14 @@ assemble_rows_kernel(int mode, int32_t n, const double2 *__restrict__ nodes,
       const int start = carry + incl - cnt;
       carry += __shfl_sync(mask, incl, LPR - 1, LPR);
       if (s < L) {
+        // the slot's contributions in the plan's order (bitwise reproducible)
         double h = 0.0, mm = 0.0, wi = 0.0;
         for (int q = 0; q < cnt; ++q) {
           const int id = contrib[cbase + start + q];
           const int t = id / K, b = id - t * K;
-          const int a = st.a[t];
-          const int ab = a * K + b;
-          const double At = st.A[t];
-          double hk;
-          if (mode == QD_ASM_FEM) {
-            hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]);
-            const double *tw = T + ab * K;
-            double vs = 0.0, ws = 0.0;
-            if constexpr (K % 2 == 0) {
-              const double2 *t2 = reinterpret_cast<const double2 *>(tw);
-              const double2 *v2 = reinterpret_cast<const double2 *>(st.V[t]);
-#pragma unroll
-              for (int l = 0; l < K / 2; ++l) {
-                const double2 tl = t2[l], vl = v2[l];
-                vs += vl.x * tl.x;
-                vs += vl.y * tl.y;
-              }
-              if (HAS_W) {
-                const double2 *w2 = reinterpret_cast<const double2 *>(st.W[t]);
-#pragma unroll
-                for (int l = 0; l < K / 2; ++l) {
-                  const double2 tl = t2[l], wl = w2[l];
-                  ws += wl.x * tl.x;
-                  ws += wl.y * tl.y;
-                }
-              }
-            } else {
-#pragma unroll
-              for (int l = 0; l < K; ++l) {
-                vs += st.V[t][l] * tw[l];
-                if (HAS_W) ws += st.W[t][l] * tw[l];
-              }
-            }
-            hk += At * vs;
-            wi -= At * ws;
-          } else if (mode == QD_ASM_REF_CYTHON) {
-            hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]);
-            if (a == b) hk += (a == 0 ? 1.0 : 2.0) * (st.V[t][0] * At / 3.0);
-          } else if (mode == QD_ASM_REF_FIXED) {
-            hk = (st.cA[t] / 3.0) * (a == b ? 1.0 : 0.5);
-            if (a == b) hk += st.V[t][0] * At / 3.0;
-          } else {
-            hk = st.cA[t] * (st.g00[t] * Sxx[ab] + st.g01[t] * Sxy[ab] + st.g11[t] * Syy[ab]) +
-                 st.V[t][0] * At / 9.0;
-          }
-          h += hk;
-          mm += mode == QD_ASM_REF_CPP ? At / 9.0 : At * Mr[ab];
+          h += st.he[t][b];
+          mm += st.me[t][b];
+          if constexpr (HAS_W) wi -= st.we[t][b];
         }
         H[rp + s] = h;
         M[rp + s] = mm;
