@@ -821,6 +821,219 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double rel, doub
   __syncthreads();
 }
 
+// The nsel lowest eigenpairs of the symmetric n x n matrix A (shared memory,
+// leading dimension ld; destroyed), by
+//   (1) Householder reduction to tridiagonal form T = H^T A H, the reflector
+//       vectors kept in A's columns below the subdiagonal (3 barriers per
+//       column; each thread forms the rank-2 update's scalar itself);
+//   (2) bisection on Sturm counts of T for eigenvalue j, one warp per
+//       eigenvalue, every lane testing one of 32 points of the current
+//       interval per round (33-way multisection, ~11 rounds to full
+//       precision);
+//   (3) inverse iteration on T - lambda_j I (Gaussian elimination with row
+//       interchanges, three steps from a fixed pseudo-random start), one
+//       thread per eigenvalue, then modified Gram-Schmidt over the nsel
+//       vectors in ascending order (orthonormal also inside clusters of close
+//       eigenvalues, whose vectors inverse iteration alone does not separate);
+//   (4) back-transformation Z = H Y, one warp per vector.
+// Eigenvalues ascending into ev[0..nsel), eigenvectors into Z's columns
+// 0..nsel-1 (ld).  work: 3 n nsel doubles; sw: 4 ld doubles (shared memory).
+// The eigenvalues are accurate to a few units of roundoff times ||A||, the
+// vectors orthonormal to roundoff.
+__device__ void tridiag_lowest_cta(double *A, double *Z, int n, int ld, int nsel, double *ev,
+                                   double *work, double *sw) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = nt >> 5;
+  double *sd = sw, *se = sw + ld, *sg = sw + 2 * ld, *sp = sw + 3 * ld;
+  __shared__ double s_lohi[3];   // Gershgorin bounds, pivot floor
+  // (1) tridiagonalisation
+  for (int k = 0; k + 2 < n; ++k) {
+    const int len = n - k - 1;
+    if (warp == 0) {
+      double sig = 0.0;
+      for (int i = lane; i < len; i += 32) {
+        const double x = A[(k + 1 + i) * ld + k];
+        sig += x * x;
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
+      if (lane == 0) {
+        const double x0 = A[(k + 1) * ld + k];
+        if (sig - x0 * x0 <= 1e-300 * fmax(1.0, sig)) {   // column already reduced
+          se[k] = x0;
+          sg[k] = 0.0;
+        } else {
+          const double alpha = -copysign(sqrt(sig), x0);
+          se[k] = alpha;
+          sg[k] = 1.0 / (sig - x0 * alpha);                 // 2 / v^T v
+          A[(k + 1) * ld + k] = x0 - alpha;                 // v = x - alpha e_1
+        }
+      }
+    }
+    __syncthreads();
+    const double g = sg[k];
+    if (g == 0.0) continue;                                  // uniform
+    // p = g A_sub v
+    for (int i = tid; i < len; i += nt) {
+      const double *row = A + (k + 1 + i) * ld + (k + 1);
+      double acc = 0.0;
+      for (int j = 0; j < len; ++j) acc += row[j] * A[(k + 1 + j) * ld + k];
+      sp[i] = g * acc;
+    }
+    __syncthreads();
+    // A_sub -= v q^T + q v^T, q = p - K v, K = g (v^T p) / 2
+    double K = 0.0;
+    for (int j = 0; j < len; ++j) K += A[(k + 1 + j) * ld + k] * sp[j];
+    K *= 0.5 * g;
+    for (int e = tid; e < len * len; e += nt) {
+      const int i = e / len, j = e - i * len;
+      const double vi = A[(k + 1 + i) * ld + k], vj = A[(k + 1 + j) * ld + k];
+      A[(k + 1 + i) * ld + (k + 1 + j)] += 2.0 * K * vi * vj - vi * sp[j] - sp[i] * vj;
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += nt) {
+    sd[i] = A[i * ld + i];
+    if (i == n - 2) se[i] = A[(n - 1) * ld + (n - 2)];
+    if (i >= n - 2) sg[i] = 0.0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double lo = 1e300, hi = -1e300, emax = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double r = (i > 0 ? fabs(se[i - 1]) : 0.0) + (i + 1 < n ? fabs(se[i]) : 0.0);
+      lo = fmin(lo, sd[i] - r);
+      hi = fmax(hi, sd[i] + r);
+      if (i + 1 < n) emax = fmax(emax, se[i] * se[i]);
+    }
+    const double w = hi - lo;
+    s_lohi[0] = lo - 1e-14 * w - 1e-300;
+    s_lohi[1] = hi + 1e-14 * w + 1e-300;
+    s_lohi[2] = 1e-290 * fmax(1.0, emax);
+  }
+  __syncthreads();
+  // (2) bisection
+  const double pivmin = s_lohi[2];
+  auto sturm = [&](double x) {
+    double q = sd[0] - x;
+    int c = q < 0.0;
+    for (int i = 1; i < n; ++i) {
+      if (fabs(q) < pivmin) q = -pivmin;
+      q = (sd[i] - x) - se[i - 1] * se[i - 1] / q;
+      c += q < 0.0;
+    }
+    return c;
+  };
+  for (int j = warp; j < nsel; j += nwarps) {
+    double lo = s_lohi[0], hi = s_lohi[1];
+    for (int round = 0; round < 24; ++round) {
+      const double step = (hi - lo) / 33.0;
+      const double x = lo + double(lane + 1) * step;
+      const unsigned m = __ballot_sync(0xffffffffu, sturm(x) >= j + 1);
+      const int l = m ? __ffs(m) - 1 : 32;
+      const double xl = __shfl_sync(0xffffffffu, x, l > 0 ? l - 1 : 0);
+      const double xh = __shfl_sync(0xffffffffu, x, l < 32 ? l : 31);
+      const double nlo = l > 0 ? xl : lo, nhi = l < 32 ? xh : hi;
+      lo = nlo;
+      hi = nhi;
+      if (hi - lo <= 4.440892098500626e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
+    }
+    if (lane == 0) ev[j] = 0.5 * (lo + hi);
+  }
+  __syncthreads();
+  // (3) inverse iteration, one thread per eigenvalue, vector in Z's column j
+  if (tid < nsel) {
+    const int j = tid;
+    double *dg = work + 3 * n * j, *su = dg + n, *su2 = su + n;
+    double tn = 0.0;
+    for (int i = 0; i < n; ++i) tn = fmax(tn, fmax(fabs(sd[i]), i + 1 < n ? fabs(se[i]) : 0.0));
+    const double tiny = 2.220446049250313e-16 * fmax(tn, 1e-300);
+    const double lam = ev[j];
+    for (int i = 0; i < n; ++i)
+      Z[i * ld + j] = double((uint32_t(j + 1) * 2654435761u + uint32_t(i) * 40503u) % 1000u) / 1000.0 + 0.5;
+    for (int it = 0; it < 3; ++it) {
+      for (int i = 0; i < n; ++i) {
+        dg[i] = sd[i] - lam;
+        su[i] = i + 1 < n ? se[i] : 0.0;
+        su2[i] = 0.0;
+      }
+      for (int i = 0; i + 1 < n; ++i) {
+        const double b = se[i];
+        double *y = Z + j;
+        if (fabs(b) > fabs(dg[i])) {          // interchange rows i and i + 1
+          const double r0 = b, r1 = dg[i + 1], r2 = su[i + 1];
+          const double s0 = dg[i], s1 = su[i];
+          dg[i] = r0;
+          su[i] = r1;
+          su2[i] = r2;
+          const double t = y[i * ld];
+          y[i * ld] = y[(i + 1) * ld];
+          y[(i + 1) * ld] = t;
+          const double mlt = s0 / r0;
+          dg[i + 1] = s1 - mlt * r1;
+          su[i + 1] = -mlt * r2;
+          y[(i + 1) * ld] -= mlt * y[i * ld];
+        } else {
+          const double piv = dg[i] != 0.0 ? dg[i] : tiny;
+          dg[i] = piv;
+          const double mlt = b / piv;
+          dg[i + 1] -= mlt * su[i];
+          y[(i + 1) * ld] -= mlt * y[i * ld];
+        }
+      }
+      if (dg[n - 1] == 0.0) dg[n - 1] = tiny;
+      double nrm = 0.0;
+      for (int i = n - 1; i >= 0; --i) {
+        double sacc = Z[i * ld + j];
+        if (i + 1 < n) sacc -= su[i] * Z[(i + 1) * ld + j];
+        if (i + 2 < n) sacc -= su2[i] * Z[(i + 2) * ld + j];
+        const double x = sacc / (dg[i] != 0.0 ? dg[i] : tiny);
+        Z[i * ld + j] = x;
+        nrm += x * x;
+      }
+      const double inv = rsqrt(fmax(nrm, 1e-300));
+      for (int i = 0; i < n; ++i) Z[i * ld + j] *= inv;
+    }
+  }
+  __syncthreads();
+  // modified Gram-Schmidt in ascending order (warp 0)
+  if (warp == 0) {
+    for (int j = 0; j < nsel; ++j) {
+      for (int i = 0; i < j; ++i) {
+        double dt = 0.0;
+        for (int r = lane; r < n; r += 32) dt += Z[r * ld + i] * Z[r * ld + j];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) dt += __shfl_xor_sync(0xffffffffu, dt, o);
+        for (int r = lane; r < n; r += 32) Z[r * ld + j] -= dt * Z[r * ld + i];
+        __syncwarp();
+      }
+      double nr = 0.0;
+      for (int r = lane; r < n; r += 32) nr += Z[r * ld + j] * Z[r * ld + j];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) nr += __shfl_xor_sync(0xffffffffu, nr, o);
+      const double inv = rsqrt(fmax(nr, 1e-300));
+      for (int r = lane; r < n; r += 32) Z[r * ld + j] *= inv;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // (4) Z = H Y: reflectors applied last first, one warp per vector
+  for (int c = warp; c < nsel; c += nwarps) {
+    for (int k = n - 3; k >= 0; --k) {
+      const double g = sg[k];
+      if (g == 0.0) continue;
+      double dt = 0.0;
+      for (int r = k + 1 + lane; r < n; r += 32) dt += A[r * ld + k] * Z[r * ld + c];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) dt += __shfl_xor_sync(0xffffffffu, dt, o);
+      dt *= g;
+      for (int r = k + 1 + lane; r < n; r += 32) Z[r * ld + c] -= dt * A[r * ld + k];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
 // Rayleigh-Ritz on span[X W P] by SVQB: with D the diagonal scaling of the
 // basis Gram B, eigendecompose D B D = U S U^T, drop directions with
 // S < tau max(S) (near-dependent or null columns, e.g. a preconditioned
@@ -839,6 +1052,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   double *sD = sZ + m * m;     // m    column scaling
   double *sE = sD + m;         // m    eigenvalues
   double *sR = sE + m;         // B    relative residuals
+  double *sW = sR + B;         // 4m   scratch of the tridiagonal eigensolver
   __shared__ int s_flag, s_r, s_keep[kMaxM], s_sel[kMaxM];
   __shared__ double s_red[256];
   __shared__ double s_c[kMaxM / 2 + 1], s_s[kMaxM / 2 + 1];
@@ -1067,19 +1281,11 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     }
   }
   __syncthreads();
-  // 4. standard eigenproblem of size r; eigenvectors into sA
-  jacobi_cta(sB, sA, r, m, jrel, s_red, s_c, s_s, s_p, s_q);
-  if (tid < r) sE[tid] = sB[tid * m + tid];
-  __syncthreads();
-  if (tid < r) {
-    const double e = sE[tid];
-    int rank = 0;
-    for (int j = 0; j < r; ++j) {
-      const double f = sE[j];
-      rank += (f < e) || (f == e && j < tid);
-    }
-    s_sel[rank] = tid;
-  }
+  // 4. the B lowest eigenpairs of the standard problem of size r: values
+  //    ascending into sE, vectors into sA's first B columns (sZ is free
+  //    scratch now)
+  tridiag_lowest_cta(sB, sA, r, m, B, sE, sZ, sW);
+  if (tid < B) s_sel[tid] = tid;
   __syncthreads();
   // 5. Y = D Q Z[:, sel]  (m x B)
   double *Y = coef + size_t(d) * m * B;
@@ -1902,7 +2108,7 @@ struct Layout {
 
 size_t rr_smem_bytes(int B) {
   const int m = 3 * B;
-  return size_t(4 * m * m + 2 * m + B) * sizeof(double);
+  return size_t(4 * m * m + 2 * m + B + 4 * m) * sizeof(double);
 }
 
 int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nchunks,
