@@ -825,27 +825,31 @@ __device__ void jacobi_cta(double *A, double *V, int n, int ld, double rel, doub
 // leading dimension ld; destroyed), by
 //   (1) Householder reduction to tridiagonal form T = H^T A H, the reflector
 //       vectors kept in A's columns below the subdiagonal (3 barriers per
-//       column; each thread forms the rank-2 update's scalar itself);
-//   (2) bisection on Sturm counts of T for eigenvalue j, one warp per
-//       eigenvalue, every lane testing one of 32 points of the current
-//       interval per round (33-way multisection, ~11 rounds to full
-//       precision);
+//       column; 8 lanes per row for the matrix-vector product, the rank-2
+//       update's scalar reduced by every warp for itself);
+//   (2) bisection on Sturm counts of T for all nsel eigenvalues at once, a
+//       group of L = min(32, blockDim / nsel) threads per eigenvalue testing
+//       L points of its interval per round ((L+1)-way multisection);
 //   (3) inverse iteration on T - lambda_j I (Gaussian elimination with row
-//       interchanges, three steps from a fixed pseudo-random start), one
-//       thread per eigenvalue, then modified Gram-Schmidt over the nsel
-//       vectors in ascending order (orthonormal also inside clusters of close
-//       eigenvalues, whose vectors inverse iteration alone does not separate);
-//   (4) back-transformation Z = H Y, one warp per vector.
+//       interchanges, two steps from a fixed pseudo-random start), one
+//       thread per eigenvalue, then classical Gram-Schmidt applied twice
+//       over the nsel vectors in ascending order (orthonormal also inside
+//       clusters of close eigenvalues, which inverse iteration alone does
+//       not separate);
+//   (4) back-transformation Z = H Y, 16 lanes per vector.
 // Eigenvalues ascending into ev[0..nsel), eigenvectors into Z's columns
-// 0..nsel-1 (ld).  work: 3 n nsel doubles; sw: 4 ld doubles (shared memory).
-// The eigenvalues are accurate to a few units of roundoff times ||A||, the
-// vectors orthonormal to roundoff.
+// 0..nsel-1 (ld).  work: 3 n nsel doubles; sw: 4 ld + blockDim + 3 nsel
+// doubles (shared memory); nsel <= 16, blockDim >= 16 nsel.  The eigenvalues
+// are accurate to a few units of roundoff times ||A||, the vectors
+// orthonormal to roundoff.
 __device__ void tridiag_lowest_cta(double *A, double *Z, int n, int ld, int nsel, double *ev,
                                    double *work, double *sw) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-  const int nwarps = nt >> 5;
   double *sd = sw, *se = sw + ld, *sg = sw + 2 * ld, *sp = sw + 3 * ld;
+  double *sx = sw + 4 * ld;            // [nt] per-thread scratch (counts, dots)
+  double *slo = sx + nt, *shi = slo + nsel, *sdt = shi + nsel;   // [nsel] each
   __shared__ double s_lohi[3];   // Gershgorin bounds, pivot floor
+  __shared__ int s_open[2];   // intervals still open, by round parity
   // (1) tridiagonalisation
   for (int k = 0; k + 2 < n; ++k) {
     const int len = n - k - 1;
@@ -873,17 +877,25 @@ __device__ void tridiag_lowest_cta(double *A, double *Z, int n, int ld, int nsel
     __syncthreads();
     const double g = sg[k];
     if (g == 0.0) continue;                                  // uniform
-    // p = g A_sub v
-    for (int i = tid; i < len; i += nt) {
-      const double *row = A + (k + 1 + i) * ld + (k + 1);
+    // p = g A_sub v, 8 lanes per row
+    for (int i0 = 0; i0 < len; i0 += nt / 8) {
+      const int i = i0 + tid / 8, sub = tid & 7;
       double acc = 0.0;
-      for (int j = 0; j < len; ++j) acc += row[j] * A[(k + 1 + j) * ld + k];
-      sp[i] = g * acc;
+      if (i < len) {
+        const double *row = A + (k + 1 + i) * ld + (k + 1);
+        for (int j = sub; j < len; j += 8) acc += row[j] * A[(k + 1 + j) * ld + k];
+      }
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+      if (i < len && sub == 0) sp[i] = g * acc;
     }
     __syncthreads();
-    // A_sub -= v q^T + q v^T, q = p - K v, K = g (v^T p) / 2
+    // A_sub -= v q^T + q v^T, q = p - K v, K = g (v^T p) / 2 (each warp sums it)
     double K = 0.0;
-    for (int j = 0; j < len; ++j) K += A[(k + 1 + j) * ld + k] * sp[j];
+    for (int j = lane; j < len; j += 32) K += A[(k + 1 + j) * ld + k] * sp[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) K += __shfl_xor_sync(0xffffffffu, K, o);
     K *= 0.5 * g;
     for (int e = tid; e < len * len; e += nt) {
       const int i = e / len, j = e - i * len;
@@ -911,35 +923,53 @@ __device__ void tridiag_lowest_cta(double *A, double *Z, int n, int ld, int nsel
     s_lohi[1] = hi + 1e-14 * w + 1e-300;
     s_lohi[2] = 1e-290 * fmax(1.0, emax);
   }
+  for (int i = tid; i + 1 < n; i += nt) sp[i] = se[i] * se[i];   // e_i^2
   __syncthreads();
-  // (2) bisection
+  // (2) bisection, all eigenvalues at once
   const double pivmin = s_lohi[2];
-  auto sturm = [&](double x) {
-    double q = sd[0] - x;
-    int c = q < 0.0;
-    for (int i = 1; i < n; ++i) {
-      if (fabs(q) < pivmin) q = -pivmin;
-      q = (sd[i] - x) - se[i - 1] * se[i - 1] / q;
-      c += q < 0.0;
-    }
-    return c;
-  };
-  for (int j = warp; j < nsel; j += nwarps) {
-    double lo = s_lohi[0], hi = s_lohi[1];
-    for (int round = 0; round < 24; ++round) {
-      const double step = (hi - lo) / 33.0;
-      const double x = lo + double(lane + 1) * step;
-      const unsigned m = __ballot_sync(0xffffffffu, sturm(x) >= j + 1);
-      const int l = m ? __ffs(m) - 1 : 32;
-      const double xl = __shfl_sync(0xffffffffu, x, l > 0 ? l - 1 : 0);
-      const double xh = __shfl_sync(0xffffffffu, x, l < 32 ? l : 31);
-      const double nlo = l > 0 ? xl : lo, nhi = l < 32 ? xh : hi;
-      lo = nlo;
-      hi = nhi;
-      if (hi - lo <= 4.440892098500626e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
-    }
-    if (lane == 0) ev[j] = 0.5 * (lo + hi);
+  const int L = min(32, nt / nsel);
+  const int grp = tid / L, lt = tid - grp * L;
+  if (tid < nsel) {
+    slo[tid] = s_lohi[0];
+    shi[tid] = s_lohi[1];
   }
+  __syncthreads();
+  for (int round = 0; round < 64; ++round) {
+    if (grp < nsel) {
+      const double lo = slo[grp], hi = shi[grp];
+      const double x = lo + double(lt + 1) * ((hi - lo) / double(L + 1));
+      double q = sd[0] - x;
+      int c = q < 0.0;
+      for (int i = 1; i < n; ++i) {
+        if (fabs(q) < pivmin) q = -pivmin;
+        q = (sd[i] - x) - sp[i - 1] / q;
+        c += q < 0.0;
+      }
+      sx[tid] = double(c);
+    }
+    if (round == 0 && tid == 0) s_open[0] = 0;
+    __syncthreads();
+    if (tid == 0) s_open[(round + 1) & 1] = 0;   // last read a round ago
+    if (tid < nsel) {
+      const int j = tid;
+      const double lo = slo[j], hi = shi[j], step = (hi - lo) / double(L + 1);
+      int l = L;
+      for (int t = 0; t < L; ++t)
+        if (sx[j * L + t] >= double(j + 1)) {
+          l = t;
+          break;
+        }
+      const double nlo = l > 0 ? lo + double(l) * step : lo;
+      const double nhi = l < L ? lo + double(l + 1) * step : hi;
+      slo[j] = nlo;
+      shi[j] = nhi;
+      if (nhi - nlo > 4.440892098500626e-16 * fmax(fabs(nlo), fabs(nhi)) + 1e-300)
+        atomicAdd(&s_open[round & 1], 1);
+    }
+    __syncthreads();
+    if (s_open[round & 1] == 0) break;                        // uniform
+  }
+  if (tid < nsel) ev[tid] = 0.5 * (slo[tid] + shi[tid]);
   __syncthreads();
   // (3) inverse iteration, one thread per eigenvalue, vector in Z's column j
   if (tid < nsel) {
@@ -951,7 +981,7 @@ __device__ void tridiag_lowest_cta(double *A, double *Z, int n, int ld, int nsel
     const double lam = ev[j];
     for (int i = 0; i < n; ++i)
       Z[i * ld + j] = double((uint32_t(j + 1) * 2654435761u + uint32_t(i) * 40503u) % 1000u) / 1000.0 + 0.5;
-    for (int it = 0; it < 3; ++it) {
+    for (int it = 0; it < 2; ++it) {
       for (int i = 0; i < n; ++i) {
         dg[i] = sd[i] - lam;
         su[i] = i + 1 < n ? se[i] : 0.0;
@@ -996,38 +1026,51 @@ __device__ void tridiag_lowest_cta(double *A, double *Z, int n, int ld, int nsel
     }
   }
   __syncthreads();
-  // modified Gram-Schmidt in ascending order (warp 0)
-  if (warp == 0) {
-    for (int j = 0; j < nsel; ++j) {
-      for (int i = 0; i < j; ++i) {
+  // classical Gram-Schmidt, twice per vector, in ascending order: warp w
+  // forms the coefficients against vectors i = w, w + 8, ..., all threads
+  // subtract, warp 0 normalises
+  for (int j = 1; j < nsel; ++j) {
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int i = warp; i < j; i += nt / 32) {
         double dt = 0.0;
         for (int r = lane; r < n; r += 32) dt += Z[r * ld + i] * Z[r * ld + j];
 #pragma unroll
         for (int o = 16; o; o >>= 1) dt += __shfl_xor_sync(0xffffffffu, dt, o);
-        for (int r = lane; r < n; r += 32) Z[r * ld + j] -= dt * Z[r * ld + i];
-        __syncwarp();
+        if (lane == 0) sdt[i] = dt;
       }
+      __syncthreads();
+      for (int r = tid; r < n; r += nt) {
+        double v = Z[r * ld + j];
+        for (int i = 0; i < j; ++i) v -= sdt[i] * Z[r * ld + i];
+        Z[r * ld + j] = v;
+      }
+      __syncthreads();
+    }
+    if (warp == 0) {
       double nr = 0.0;
       for (int r = lane; r < n; r += 32) nr += Z[r * ld + j] * Z[r * ld + j];
 #pragma unroll
       for (int o = 16; o; o >>= 1) nr += __shfl_xor_sync(0xffffffffu, nr, o);
       const double inv = rsqrt(fmax(nr, 1e-300));
       for (int r = lane; r < n; r += 32) Z[r * ld + j] *= inv;
-      __syncwarp();
     }
+    __syncthreads();
   }
-  __syncthreads();
-  // (4) Z = H Y: reflectors applied last first, one warp per vector
-  for (int c = warp; c < nsel; c += nwarps) {
+  // (4) Z = H Y: reflectors applied last first, 16 lanes per vector
+  {
+    const int c = tid >> 4, l16 = tid & 15;
+    const bool live = c < nsel;
     for (int k = n - 3; k >= 0; --k) {
       const double g = sg[k];
-      if (g == 0.0) continue;
+      if (g == 0.0) continue;                                // uniform
       double dt = 0.0;
-      for (int r = k + 1 + lane; r < n; r += 32) dt += A[r * ld + k] * Z[r * ld + c];
+      if (live)
+        for (int r = k + 1 + l16; r < n; r += 16) dt += A[r * ld + k] * Z[r * ld + c];
 #pragma unroll
-      for (int o = 16; o; o >>= 1) dt += __shfl_xor_sync(0xffffffffu, dt, o);
+      for (int o = 8; o; o >>= 1) dt += __shfl_xor_sync(0xffffffffu, dt, o);
       dt *= g;
-      for (int r = k + 1 + lane; r < n; r += 32) Z[r * ld + c] -= dt * A[r * ld + k];
+      if (live)
+        for (int r = k + 1 + l16; r < n; r += 16) Z[r * ld + c] -= dt * A[r * ld + k];
       __syncwarp();
     }
   }
@@ -1052,7 +1095,7 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   double *sD = sZ + m * m;     // m    column scaling
   double *sE = sD + m;         // m    eigenvalues
   double *sR = sE + m;         // B    relative residuals
-  double *sW = sR + B;         // 4m   scratch of the tridiagonal eigensolver
+  double *sW = sR + B;         // 4m + 256 + 3B  scratch of the tridiagonal eigensolver
   __shared__ int s_flag, s_r, s_keep[kMaxM], s_sel[kMaxM];
   __shared__ double s_red[256];
   __shared__ double s_c[kMaxM / 2 + 1], s_s[kMaxM / 2 + 1];
@@ -1073,11 +1116,26 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
   // kSafety covers ||r||_{M^-1} exceeding ||r|| / ||M x|| for residuals in the
   // high modes of M).
   if (s.have_res) {
+    // chunk sums of the residual norms: 8 fixed groups of chunks per column,
+    // then the groups in order
+    {
+      const int col = tid % B, grpc = tid / B;
+      if (grpc < 8) {
+        double rr = 0.0, mx = 0.0;
+        for (int c = s.chunk0 + grpc; c < s.chunk1; c += 8) {
+          rr += norms[size_t(c) * 2 * B + col];
+          mx += norms[size_t(c) * 2 * B + B + col];
+        }
+        sW[grpc * 2 * B + col] = rr;
+        sW[grpc * 2 * B + B + col] = mx;
+      }
+    }
+    __syncthreads();
     if (tid < B) {
       double rr = 0.0, mx = 0.0;
-      for (int c = s.chunk0; c < s.chunk1; ++c) {
-        rr += norms[size_t(c) * 2 * B + tid];
-        mx += norms[size_t(c) * 2 * B + B + tid];
+      for (int g = 0; g < 8; ++g) {
+        rr += sW[g * 2 * B + tid];
+        mx += sW[g * 2 * B + B + tid];
       }
       const double at = fmax(fmax(fabs(th[tid]), prm.eig_scale), 1e-300);
       const double ares = sqrt(rr / fmax(mx, 1e-300));
@@ -2108,7 +2166,7 @@ struct Layout {
 
 size_t rr_smem_bytes(int B) {
   const int m = 3 * B;
-  return size_t(4 * m * m + 2 * m + B + 4 * m) * sizeof(double);
+  return size_t(4 * m * m + 2 * m + B + 4 * m + 256 + 3 * B) * sizeof(double);
 }
 
 int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nchunks,
