@@ -602,8 +602,10 @@ def algorithmic_bytes(hb, counts, k_block, mixed=True):
 
     Per dot and launch (n rows, z nonzeros, block B; counts[:, 0] and
     counts[:, 3] count both SpMM launches of an iteration):
-      FP32 phase (vectors 4 bytes, matrix values an 8-byte FP32 (H, M) pair):
-        spmm   2 (z (4 + 8) + 4 n) + 3 n B 4 gathered + 7 n B 4 written
+      FP32 phase (vectors 4 bytes, matrix values an 8-byte FP32 (H, M) pair;
+      the products of X and P read 2-byte staged positions for the column
+      indices, those of W the 4-byte indices):
+        spmm   z (2 + 8) + z (4 + 8) + 8 n + 3 n B 4 gathered + 7 n B 4 written
         gram   9 n B 4 read;  dst (2 4 + 12) n B;  ortho 14 n B 4;  update 5 n B 4
       FP64 phase of the plain form (vectors 8, values 16): the same with 8 / 16
       finishing phase of the mixed form (X, HX, MX FP64; W, P and their
@@ -631,7 +633,8 @@ def algorithmic_bytes(hb, counts, k_block, mixed=True):
                  "ortho": gr * 72 * n * B, "update": up * 28 * n * B})
             continue
         s, v = (4.0, 8.0) if ph == 0 else (8.0, 16.0)
-        add({"spmm": it * (2 * (z * (4 + v) + 4 * n) + 3 * n * B * s + 7 * n * B * s),
+        csr = z * (2 + v) + z * (4 + v) if ph == 0 else 2 * z * (4 + v)
+        add({"spmm": it * (csr + 8 * n + 3 * n * B * s + 7 * n * B * s),
              "gram": gr * 9 * n * B * s, "dst_precond": gr * n * B * (2 * s + 12),
              "ortho": gr * 14 * n * B * s, "update": up * 5 * n * B * s})
     return out

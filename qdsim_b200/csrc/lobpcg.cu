@@ -280,27 +280,401 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 }
 
 // ---------------------------------------------------------------------------
-// FP32-phase SpMM with the CSR streamed through shared memory.
-// Each sub-tile of 64 rows needs the column indices and (H, M) pairs of the
-// nonzero range [rowptr[a], rowptr[b]); both ranges are fetched by 1-D bulk
-// copies (rounded out to 16-byte boundaries; the workspace copies `col32`
-// and `hm32` carry the slack) into a 3-stage mbarrier pipeline, so that the
-// only global access left in the nonzero loop is the gather of a vector row.
-// A sub-tile with more than kCsrCap nonzeros reads the CSR from global memory.
+// FP32-phase SpMM with every operand of a sub-tile staged in shared memory.
+// A sub-tile of 64 rows needs the nonzeros [rowptr[a], rowptr[b]) and the
+// vector rows its columns name.  On a lattice those rows form a few runs (one
+// per lattice line of the stencil: five for a P2 sub-tile inside one line,
+// about 260 rows in all), so a plan built once per solve (stage_plan_kernel)
+// lists each sub-tile's runs of rows and rewrites every column index as a
+// position in the staged copy (16-bit).  The kernel then fetches, per
+// sub-tile, the positions, the FP32 (H, M) pairs and the runs of X (and P) by
+// 1-D bulk copies into a 2-stage mbarrier pipeline, and every gather of the
+// nonzero loop is a shared-memory load.  A sub-tile with more nonzeros, runs
+// or rows than a stage holds reads everything from global memory instead
+// (same arithmetic, same results).
 // XP: products of X and P with the residual W = HX - MX Theta and per-chunk
-// norms; otherwise the products of one block (W -> HW, MW).
+// norms; otherwise the products of one block (W -> HW, MW).  The solver uses
+// this form for the products of X and P (two CTAs of 384 threads per SM) and
+// spmm32_kernel below for those of W: with one block per row the staged form
+// keeps fewer warps resident than the gathering form (four CTAs per SM) and
+// measured slower.
 // ---------------------------------------------------------------------------
 constexpr int kCsrSub = 64;                 // rows per sub-tile
-constexpr int kCsrCap = kCsrSub * 20;       // staged nonzeros per sub-tile
-constexpr int kCsrStages = 3;
-struct CsrStage {
-  static constexpr int COL = kCsrCap + 8;   // int32 slots (16-byte rounding slack)
-  static constexpr int HM = kCsrCap + 4;    // float2 slots
+constexpr int kCsrCap = 1024;               // staged nonzeros per sub-tile
+constexpr int kStageRows = 384;             // staged vector rows per sub-tile
+constexpr int kMaxSeg = 7;                  // runs of rows per sub-tile
+constexpr int kCsrStages = 2;
+
+// The staging plan of one sub-tile: nseg < 0 if it is read from global
+// memory; else runs [lo[s], lo[s] + len[s]) stored one after another.
+struct SubPlan {
+  int nseg, total;
+  int lo[kMaxSeg];
+  int len[kMaxSeg];
+};
+static_assert(sizeof(SubPlan) == 64, "one 64-byte record per sub-tile");
+
+template <int B, int NBLK> struct SpmmStage {
+  static constexpr int POS = kCsrCap + 16;        // uint16 slots (16-byte rounding slack)
+  static constexpr int HM = kCsrCap + 4;          // float2 slots
+  // Consecutive staged blocks are 12 floats further apart than their size:
+  // with B = 12, rows j of X and P then fall on disjoint banks, so the
+  // warp-wide gathers (three threads per row and block) are conflict-free.
+  static constexpr int SKEW = 12;
+  static constexpr size_t POS_OFF = 0;
+  static constexpr size_t HM_OFF = size_t(POS) * 2;
+  static constexpr size_t ROW_OFF = HM_OFF + size_t(HM) * 8;
+  static constexpr size_t BLK = size_t(kStageRows * B + SKEW) * 4;
+  static constexpr size_t STAGE = ROW_OFF + NBLK * BLK;
+  static constexpr size_t META_OFF = kCsrStages * STAGE;
+  // barriers, then per stage: position base, pair base, staged flag, and
+  // the offset from a row of the sub-tile itself to its staged position
+  static constexpr size_t BYTES = META_OFF + kCsrStages * 8 + kCsrStages * 4 * 4;
+  static_assert(HM_OFF % 16 == 0 && ROW_OFF % 16 == 0 && BLK % 16 == 0 && STAGE % 16 == 0,
+                "bulk-copy destinations must be 16-byte aligned");
+};
+
+// One warp per sub-tile (chunk c, sub-tile i at record c * spc + i): the runs
+// of the column indices of its nonzeros and their staged positions.  Runs are
+// found as maximal runs of touched 8-row blocks (so gaps of fewer than 8
+// untouched rows are staged with them), then trimmed to the smallest and
+// largest column they hold.
+__global__ void __launch_bounds__(256)
+stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__restrict__ rowptr,
+                  const int32_t *__restrict__ col, SubPlan *__restrict__ plan,
+                  uint16_t *__restrict__ pos16) {
+  constexpr int NW = 64;   // bitmap words per warp: 2048 blocks of 8 rows
+  __shared__ uint32_t s_bits[8][NW];
+  __shared__ int s_start[8][kMaxSeg];
+  __shared__ int s_lo[8][kMaxSeg], s_hi[8][kMaxSeg], s_off[8][kMaxSeg];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t = int64_t(blockIdx.x) * 8 + w;
+  if (t >= int64_t(nchunks) * spc) return;   // whole warps; only warp syncs below
+  const Chunk ch = chunks[t / spc];
+  const int a = ch.begin + int(t % spc) * kCsrSub;
+  SubPlan *out = plan + t;
+  if (a >= ch.end) {
+    if (lane == 0) out->nseg = -1;
+    return;
+  }
+  const int b = min(a + kCsrSub, ch.end);
+  const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
+  int cmin = INT_MAX, cmax = INT_MIN;
+  for (int p = q0 + lane; p < q1; p += 32) {
+    const int j = __ldg(col + p);
+    cmin = min(cmin, j);
+    cmax = max(cmax, j);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+    cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  }
+  bool ok = q1 > q0 && q1 - q0 <= kCsrCap && int64_t(cmax) - cmin < int64_t(NW) * 32 * 8;
+  if (ok) {
+    for (int k = lane; k < NW; k += 32) s_bits[w][k] = 0u;
+    __syncwarp();
+    for (int p = q0 + lane; p < q1; p += 32) {
+      const int blk = (__ldg(col + p) - cmin) >> 3;
+      atomicOr(&s_bits[w][blk >> 5], 1u << (blk & 31));
+    }
+    __syncwarp();
+    // lane l holds blocks [64 l, 64 l + 64); a run starts at a touched block
+    // whose predecessor is untouched
+    const uint64_t v = uint64_t(s_bits[w][2 * lane]) | (uint64_t(s_bits[w][2 * lane + 1]) << 32);
+    const uint64_t prev_top = __shfl_up_sync(0xffffffffu, v >> 63, 1);
+    const uint64_t starts = v & ~((v << 1) | (lane > 0 ? prev_top : 0ull));
+    const int cnt = __popcll(starts);
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int nseg = __shfl_sync(0xffffffffu, incl, 31);
+    ok = nseg <= kMaxSeg;
+    if (ok) {
+      int e = incl - cnt;
+      for (uint64_t s = starts; s; s &= s - 1) s_start[w][e++] = 64 * lane + __ffsll(s) - 1;
+      if (lane < nseg) {
+        s_lo[w][lane] = INT_MAX;
+        s_hi[w][lane] = INT_MIN;
+      }
+      __syncwarp();
+      for (int p = q0 + lane; p < q1; p += 32) {
+        const int j = __ldg(col + p), blk = (j - cmin) >> 3;
+        int sg = 0;
+        while (sg + 1 < nseg && s_start[w][sg + 1] <= blk) ++sg;
+        atomicMin(&s_lo[w][sg], j);
+        atomicMax(&s_hi[w][sg], j);
+      }
+      __syncwarp();
+      int total = 0;
+      int own = 0;   // the sub-tile's own rows lie in one run (their diagonal entries)
+      if (lane == 0) {
+        for (int sg = 0; sg < nseg; ++sg) {
+          s_off[w][sg] = total;
+          total += s_hi[w][sg] - s_lo[w][sg] + 1;
+          own |= s_lo[w][sg] <= a && b - 1 <= s_hi[w][sg];
+        }
+      }
+      total = __shfl_sync(0xffffffffu, total, 0);
+      own = __shfl_sync(0xffffffffu, own, 0);
+      __syncwarp();
+      ok = total <= kStageRows && own;
+      if (ok) {
+        for (int p = q0 + lane; p < q1; p += 32) {
+          const int j = __ldg(col + p), blk = (j - cmin) >> 3;
+          int sg = 0;
+          while (sg + 1 < nseg && s_start[w][sg + 1] <= blk) ++sg;
+          pos16[p] = uint16_t(s_off[w][sg] + j - s_lo[w][sg]);
+        }
+        if (lane < nseg) {
+          out->lo[lane] = s_lo[w][lane];
+          out->len[lane] = s_hi[w][lane] - s_lo[w][lane] + 1;
+        }
+        if (lane == 0) {
+          out->nseg = nseg;
+          out->total = total;
+        }
+      }
+    }
+  }
+  if (!ok && lane == 0) out->nseg = -1;
+}
+
+template <int B, bool XP>
+__global__ void __launch_bounds__(64 * (B / 4) * (XP ? 2 : 1), XP ? (B <= 12 ? 2 : 1) : 3)
+spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
+               const int32_t *__restrict__ col32, const uint16_t *__restrict__ pos16,
+               const SubPlan *__restrict__ plan, int spc, const float2 *__restrict__ hm32,
+               const float *__restrict__ rs32, double sh, double smv,
+               const double *__restrict__ theta, const float *__restrict__ X,
+               const float *__restrict__ P, float *__restrict__ HX, float *__restrict__ MX,
+               float *__restrict__ HP, float *__restrict__ MP, float *__restrict__ W,
+               double *__restrict__ norms, int *wait_err, int ph) {
+  constexpr int G = B / 4;
+  constexpr int G2 = XP ? 2 * G : G;
+  constexpr int NT = kCsrSub * G2;
+  constexpr int NBLK = XP ? 2 : 1;
+  using SS = SpmmStage<B, NBLK>;
+  static_assert(!XP || size_t(NT) * 8 * sizeof(double) <= SS::META_OFF,
+                "the norm slots reuse the stage buffers");
+  extern __shared__ __align__(128) unsigned char dsm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(dsm + SS::META_OFF);
+  int *s_pbase = reinterpret_cast<int *>(full + kCsrStages);
+  int *s_hbase = s_pbase + kCsrStages;
+  int *s_staged = s_hbase + kCsrStages;
+  int *s_obase = s_staged + kCsrStages;
+  __shared__ double s_th[B];
+
+  // ph: the phase whose dots this launch serves (the products of X and P only
+  // in the FP32 phase; W's products also in the mixed form's finishing phase)
+  const Chunk ch = chunks[blockIdx.x];
+  const DotState &sd = st[ch.dot];
+  if (!sd.run[ph]) return;
+  const bool with_p = sd.has_p != 0;
+  const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == sd.chunk0)
+    const_cast<DotState *>(st)[ch.dot].launches[ph][0]++;
+  if (XP && tid < B) s_th[tid] = theta[size_t(ch.dot) * B + tid];
+  const int sub = tid / G2, gg = tid % G2;
+  const bool isx = gg < G;
+  const int g = isx ? gg : gg - G;
+  // FP64 sums of squares of this thread's rows (problems posed in SI units
+  // have squared residuals far below FP32's range): r^2, (Mx)^2 per column
+  double red[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) red[c] = 0.0;
+  const int nsub = (ch.end - ch.begin + kCsrSub - 1) / kCsrSub;
+  if (tid == 0) {
+    for (int i = 0; i < kCsrStages; ++i) qd::tc::mbar_init(&full[i], 1);
+    qd::tc::fence_mbar_init();
+  }
+  __syncthreads();
+  const int nblk = (XP && with_p) ? 2 : 1;   // blocks staged (P only once populated)
+  auto issue = [&](int i) {   // thread 0
+    const int sst = i % kCsrStages;
+    unsigned char *sb = dsm + size_t(sst) * SS::STAGE;
+    const SubPlan *pl = plan + size_t(blockIdx.x) * spc + i;
+    const int nseg = pl->nseg;
+    if (nseg >= 0) {
+      const int a = ch.begin + i * kCsrSub, b = min(a + kCsrSub, ch.end);
+      const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
+      const int pb = q0 & ~7, pe = (q1 + 7) & ~7;
+      const int hb = q0 & ~1, he = (q1 + 1) & ~1;
+      s_pbase[sst] = pb;
+      s_hbase[sst] = hb;
+      s_staged[sst] = 1;
+      const uint32_t pbytes = uint32_t(pe - pb) * 2u, hbytes = uint32_t(he - hb) * 8u;
+      const uint32_t rbytes = uint32_t(pl->total) * B * 4u;
+      qd::tc::mbar_arrive_expect_tx(&full[sst], pbytes + hbytes + nblk * rbytes);
+      qd::tc::bulk_g2s(sb + SS::POS_OFF, pos16 + pb, pbytes, &full[sst]);
+      qd::tc::bulk_g2s(sb + SS::HM_OFF, hm32 + hb, hbytes, &full[sst]);
+      int off = 0, obase = 0;
+      for (int sg = 0; sg < nseg; ++sg) {
+        const int lo = pl->lo[sg], len = pl->len[sg];
+        if (a >= lo && a < lo + len) obase = off - lo;   // the run of the sub-tile's own rows
+        for (int k = 0; k < nblk; ++k)
+          qd::tc::bulk_g2s(sb + SS::ROW_OFF + k * SS::BLK + size_t(off) * B * 4,
+                           (k ? P : X) + size_t(lo) * B, uint32_t(len) * B * 4u, &full[sst]);
+        off += len;
+      }
+      s_obase[sst] = obase;
+    } else {
+      s_staged[sst] = 0;
+      qd::tc::mbar_arrive_expect_tx(&full[sst], 0);
+    }
+  };
+  if (tid == 0)
+    for (int i = 0; i < kCsrStages && i < nsub; ++i) issue(i);
+  bool ok = true;
+  for (int i = 0; i < nsub; ++i) {
+    const int sst = i % kCsrStages;
+    // the sub-tile's rows in two halves of one parity each (even offsets,
+    // then odd): on the row-major lattice of a P2 mesh, rows two apart have
+    // the same stencil, so the k-th neighbours gathered by one warp lie close
+    const int ofs = sub < kCsrSub / 2 ? 2 * sub : 2 * (sub - kCsrSub / 2) + 1;
+    const int r = ch.begin + i * kCsrSub + ofs;
+    const bool live = r < ch.end;
+    int p0 = 0, p1 = 0;
+    float rs = 0.f;
+    if (live) {
+      p0 = __ldg(rowptr + r);
+      p1 = __ldg(rowptr + r + 1);
+      rs = __ldg(rs32 + r);
+    }
+    ok = qd::tc::mbar_wait(&full[sst], (i / kCsrStages) & 1, qd::kPipeWaitNs) && ok;
+    if (ok && live) {
+      if (XP && !isx && !with_p) {
+        const double z[4] = {0, 0, 0, 0};
+        qd::V4<float>::store(HP + size_t(r) * B + 4 * g, z);
+        qd::V4<float>::store(MP + size_t(r) * B + 4 * g, z);
+      } else {
+        const int blk = (XP && !isx) ? 1 : 0;
+        const float *src = blk ? P : X;
+        const bool staged = s_staged[sst] != 0;
+        const unsigned char *sb = dsm + size_t(sst) * SS::STAGE;
+        const float *rows =
+            reinterpret_cast<const float *>(sb + SS::ROW_OFF + blk * SS::BLK) + 4 * g;
+        // FP32 arithmetic, H differenced against the row's own entry:
+        //   (H x)_i = sum_j H_ij (x_j - x_i) + (sum_j H_ij) x_i
+        // The stiffness part of H has (near) zero row sums, so the terms are
+        // small where x is smooth and FP32 accumulation stays ~1e-6 accurate
+        // relative to H x (undifferenced, the terms exceed H x by up to 1e4).
+        const float4 xi =
+            staged ? *reinterpret_cast<const float4 *>(rows + (r + s_obase[sst]) * B)
+                   : __ldg(reinterpret_cast<const float4 *>(src + size_t(r) * B + 4 * g));
+        float h[4] = {0.f, 0.f, 0.f, 0.f}, m[4] = {0.f, 0.f, 0.f, 0.f};
+        auto row = [&](auto getx, auto getv) {
+#pragma unroll 4
+          for (int p = p0; p < p1; ++p) {
+            const float2 v = getv(p);
+            const float4 xj = getx(p);
+            h[0] = fmaf(v.x, xj.x - xi.x, h[0]);
+            h[1] = fmaf(v.x, xj.y - xi.y, h[1]);
+            h[2] = fmaf(v.x, xj.z - xi.z, h[2]);
+            h[3] = fmaf(v.x, xj.w - xi.w, h[3]);
+            m[0] = fmaf(v.y, xj.x, m[0]);
+            m[1] = fmaf(v.y, xj.y, m[1]);
+            m[2] = fmaf(v.y, xj.z, m[2]);
+            m[3] = fmaf(v.y, xj.w, m[3]);
+          }
+        };
+        if (staged) {
+          const uint16_t *ps = reinterpret_cast<const uint16_t *>(sb + SS::POS_OFF) - s_pbase[sst];
+          const float2 *hs = reinterpret_cast<const float2 *>(sb + SS::HM_OFF) - s_hbase[sst];
+          row([&](int p) { return *reinterpret_cast<const float4 *>(rows + int(ps[p]) * B); },
+              [&](int p) { return hs[p]; });
+        } else {
+          row([&](int p) {
+                return __ldg(reinterpret_cast<const float4 *>(src + size_t(__ldg(col32 + p)) * B +
+                                                              4 * g));
+              },
+              [&](int p) { return __ldg(hm32 + p); });
+        }
+        h[0] = fmaf(rs, xi.x, h[0]);
+        h[1] = fmaf(rs, xi.y, h[1]);
+        h[2] = fmaf(rs, xi.z, h[2]);
+        h[3] = fmaf(rs, xi.w, h[3]);
+        const size_t o = size_t(r) * B + 4 * g;
+        // back to the matrices' own scale (powers of two: exact)
+        const float fsh = float(sh), fsm = float(smv);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          h[c] *= fsh;
+          m[c] *= fsm;
+        }
+        if (XP && isx) {
+          double res[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            // residual from the stored (rounded) products, as the iteration sees them
+            const double hq = double(h[c]), mq = double(m[c]);
+            res[c] = hq - s_th[4 * g + c] * mq;
+            red[2 * c] += res[c] * res[c];
+            red[2 * c + 1] += mq * mq;
+          }
+          *reinterpret_cast<float4 *>(HX + o) = make_float4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<float4 *>(MX + o) = make_float4(m[0], m[1], m[2], m[3]);
+          qd::V4<float>::store(W + o, res);
+        } else {
+          float *oh = XP ? HP : HX, *om = XP ? MP : MX;
+          *reinterpret_cast<float4 *>(oh + o) = make_float4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<float4 *>(om + o) = make_float4(m[0], m[1], m[2], m[3]);
+        }
+      }
+    }
+    __syncthreads();   // stage sst consumed
+    if (tid == 0 && ok && i + kCsrStages < nsub) issue(i + kCsrStages);
+  }
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicOr(wait_err, 1);
+      for (int i = max(0, nsub - kCsrStages); i < nsub; ++i)
+        qd::tc::mbar_wait(&full[i % kCsrStages], (i / kCsrStages) & 1, qd::kPipeWaitNs);
+    }
+    return;
+  }
+  if (XP) {
+    // per-chunk column norms (fixed-order reduction over the CTA's rows); the
+    // slots [8][threads] take the stage buffers, whose copies have all landed
+    double *s_red = reinterpret_cast<double *>(dsm);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s_red[c * NT + tid] = red[c];
+    __syncthreads();
+    if (tid < B) {
+      const int j = tid, gj = j / 4, cj = j % 4;
+      double a = 0.0, b = 0.0;
+      for (int sr = 0; sr < kCsrSub; ++sr) {
+        const int t = sr * G2 + gj;
+        a += s_red[(2 * cj) * NT + t];
+        b += s_red[(2 * cj + 1) * NT + t];
+      }
+      norms[size_t(blockIdx.x) * 2 * B + j] = a;
+      norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32-phase SpMM with the CSR streamed through shared memory and the vector
+// rows gathered from global memory (L1/L2).  Each sub-tile of 64 rows needs
+// the column indices and (H, M) pairs of the nonzero range [rowptr[a],
+// rowptr[b]); both ranges are fetched by 1-D bulk copies (rounded out to
+// 16-byte boundaries; the workspace copies `col32` and `hm32` carry the
+// slack) into a 3-stage mbarrier pipeline.  A sub-tile with more than
+// kGatherCap nonzeros reads the CSR from global memory.  Same products and
+// arguments as spmm32s_kernel; the solver uses this form for W's products.
+// ---------------------------------------------------------------------------
+constexpr int kGatherCap = kCsrSub * 20;    // staged nonzeros per sub-tile
+constexpr int kGatherStages = 3;
+struct GatherStage {
+  static constexpr int COL = kGatherCap + 8;   // int32 slots (16-byte rounding slack)
+  static constexpr int HM = kGatherCap + 4;    // float2 slots
   static constexpr size_t COL_OFF = 0;
-  static constexpr size_t HM_OFF = size_t(kCsrStages) * COL * 4;
-  static constexpr size_t META_OFF = HM_OFF + size_t(kCsrStages) * HM * 8;
+  static constexpr size_t HM_OFF = size_t(kGatherStages) * COL * 4;
+  static constexpr size_t META_OFF = HM_OFF + size_t(kGatherStages) * HM * 8;
   // barriers, then per stage: col base, hm base, staged flag
-  static constexpr size_t BYTES = META_OFF + kCsrStages * 8 + kCsrStages * 3 * 4;
+  static constexpr size_t BYTES = META_OFF + kGatherStages * 8 + kGatherStages * 3 * 4;
 };
 
 template <int B, bool XP>
@@ -315,14 +689,14 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
   constexpr int G = B / 4;
   constexpr int G2 = XP ? 2 * G : G;
   constexpr int NT = kCsrSub * G2;
-  using CS = CsrStage;
+  using CS = GatherStage;
   extern __shared__ __align__(128) unsigned char dsm[];
   int32_t *s_col = reinterpret_cast<int32_t *>(dsm + CS::COL_OFF);
   float2 *s_hm = reinterpret_cast<float2 *>(dsm + CS::HM_OFF);
   uint64_t *full = reinterpret_cast<uint64_t *>(dsm + CS::META_OFF);
-  int *s_cbase = reinterpret_cast<int *>(full + kCsrStages);
-  int *s_hbase = s_cbase + kCsrStages;
-  int *s_staged = s_hbase + kCsrStages;
+  int *s_cbase = reinterpret_cast<int *>(full + kGatherStages);
+  int *s_hbase = s_cbase + kGatherStages;
+  int *s_staged = s_hbase + kGatherStages;
   __shared__ double s_th[B];
   __shared__ double s_red[XP ? NT * 8 : 1];
 
@@ -347,15 +721,15 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
   }
   const int nsub = (ch.end - ch.begin + kCsrSub - 1) / kCsrSub;
   if (tid == 0) {
-    for (int i = 0; i < kCsrStages; ++i) qd::tc::mbar_init(&full[i], 1);
+    for (int i = 0; i < kGatherStages; ++i) qd::tc::mbar_init(&full[i], 1);
     qd::tc::fence_mbar_init();
   }
   __syncthreads();
   auto issue = [&](int i) {   // thread 0
-    const int sst = i % kCsrStages;
+    const int sst = i % kGatherStages;
     const int a = ch.begin + i * kCsrSub, b = min(a + kCsrSub, ch.end);
     const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
-    if (q1 - q0 <= kCsrCap) {
+    if (q1 - q0 <= kGatherCap) {
       const int cb = q0 & ~3, ce = (q1 + 3) & ~3;
       const int hb = q0 & ~1, he = (q1 + 1) & ~1;
       s_cbase[sst] = cb;
@@ -371,10 +745,10 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
     }
   };
   if (tid == 0)
-    for (int i = 0; i < kCsrStages && i < nsub; ++i) issue(i);
+    for (int i = 0; i < kGatherStages && i < nsub; ++i) issue(i);
   bool ok = true;
   for (int i = 0; i < nsub; ++i) {
-    const int sst = i % kCsrStages;
+    const int sst = i % kGatherStages;
     // the sub-tile's rows in two halves of one parity each (even offsets,
     // then odd): on the row-major lattice of a P2 mesh, rows two apart have
     // the same stencil, so the k-th neighbours gathered by one warp lie close
@@ -386,7 +760,7 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
       p0 = __ldg(rowptr + r);
       p1 = __ldg(rowptr + r + 1);
     }
-    ok = qd::tc::mbar_wait(&full[sst], (i / kCsrStages) & 1, qd::kPipeWaitNs) && ok;
+    ok = qd::tc::mbar_wait(&full[sst], (i / kGatherStages) & 1, qd::kPipeWaitNs) && ok;
     if (ok && live) {
       if (XP && !isx && !with_p) {
         const double z[4] = {0, 0, 0, 0};
@@ -459,13 +833,13 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
       }
     }
     __syncthreads();   // stage sst consumed
-    if (tid == 0 && ok && i + kCsrStages < nsub) issue(i + kCsrStages);
+    if (tid == 0 && ok && i + kGatherStages < nsub) issue(i + kGatherStages);
   }
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
       atomicOr(wait_err, 1);
-      for (int i = max(0, nsub - kCsrStages); i < nsub; ++i)
-        qd::tc::mbar_wait(&full[i % kCsrStages], (i / kCsrStages) & 1, qd::kPipeWaitNs);
+      for (int i = max(0, nsub - kGatherStages); i < nsub; ++i)
+        qd::tc::mbar_wait(&full[i % kGatherStages], (i / kGatherStages) & 1, qd::kPipeWaitNs);
     }
     return;
   }
@@ -2159,6 +2533,9 @@ struct Layout {
   int njac;              // chunks of such dots
   float2 *hm32;          // FP32 (H, M) pairs per nonzero (mixed precision only)
   int32_t *col32;        // copy of the column indices with bulk-copy slack (mixed only)
+  uint16_t *pos16;       // staged position of every nonzero's column (mixed only)
+  SubPlan *plan;         // staging plan per 64-row sub-tile (mixed only)
+  int spc;               // sub-tiles per chunk
   float *rs32;           // row sums of the FP32 H values, summed in FP64 (mixed only)
   int *hm_exp;           // largest binary exponents of |H| and |M|
   double hm_sh, hm_sm;   // 2^exponent: scale of the FP32 pairs
@@ -2170,7 +2547,7 @@ size_t rr_smem_bytes(int B) {
 }
 
 int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nchunks,
-          int64_t ntx, int64_t nty, bool mixed, bool jacobi, Layout &L) {
+          int chunk_rows, int64_t ntx, int64_t nty, bool mixed, bool jacobi, Layout &L) {
   const int m = 3 * B;
   L.chunks = ar.take<Chunk>(nchunks);
   L.row_off = ar.take<int32_t>(n_dots + 1);
@@ -2193,6 +2570,9 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   L.hm32 = mixed ? ar.take<float2>(size_t(nnz) + 2) : nullptr;
   L.col32 = mixed ? ar.take<int32_t>(size_t(nnz) + 4) : nullptr;
   L.rs32 = mixed ? ar.take<float>(size_t(n_rows)) : nullptr;
+  L.spc = chunk_rows / kCsrSub;
+  L.pos16 = mixed ? ar.take<uint16_t>(size_t(nnz) + 16) : nullptr;
+  L.plan = mixed ? ar.take<SubPlan>(size_t(nchunks) * L.spc) : nullptr;
   L.hm_exp = ar.take<int>(2);
   L.hm_sh = L.hm_sm = 1.0;
   L.dinv = jacobi ? ar.take<double>(size_t(n_rows)) : nullptr;
@@ -2266,9 +2646,10 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   qd::prof_begin(qd::PK_SPMM, s);
   const auto A = MatFor<TV>::make(L, H, M);
   if constexpr (sizeof(TV) == 4) {
-    if (smem_attr<spmm32_kernel<B, true>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
-    spmm32_kernel<B, true><<<L.nchunks, 128 * G, CsrStage::BYTES, s>>>(
-        L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.X, b.P,
+    if (smem_attr<spmm32s_kernel<B, true>>(SpmmStage<B, 2>::BYTES) != cudaSuccess)
+      return QD_ERR_CUDA;
+    spmm32s_kernel<B, true><<<L.nchunks, 128 * G, SpmmStage<B, 2>::BYTES, s>>>(
+        L.chunks, L.st, rowptr, L.col32, L.pos16, L.plan, L.spc, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.X, b.P,
         b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err, 0);
   } else {
     spmm_xp_kernel<TV, TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A,
@@ -2313,8 +2694,8 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
   if constexpr (sizeof(TV) == 4) {
-    if (smem_attr<spmm32_kernel<B, false>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
-    spmm32_kernel<B, false><<<L.nchunks, 64 * G, CsrStage::BYTES, s>>>(
+    if (smem_attr<spmm32_kernel<B, false>>(GatherStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
+    spmm32_kernel<B, false><<<L.nchunks, 64 * G, GatherStage::BYTES, s>>>(
         L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W,
         nullptr, b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, 0);
   } else {
@@ -2400,8 +2781,8 @@ int phase_sequence_mx(const Layout &L, const Bufs<float> &b, const Bufs<double> 
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
-  if (smem_attr<spmm32_kernel<B, false>>(CsrStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
-  spmm32_kernel<B, false><<<L.nchunks, 64 * G, CsrStage::BYTES, s>>>(
+  if (smem_attr<spmm32_kernel<B, false>>(GatherStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
+  spmm32_kernel<B, false><<<L.nchunks, 64 * G, GatherStage::BYTES, s>>>(
       L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W, nullptr,
       b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, 1);
   qd::prof_end(qd::PK_SPMM, s);
@@ -2624,13 +3005,13 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   {
     qd::Arena need(nullptr, 0);
     Layout tmp;
-    carve(need, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, jacobi, tmp);
+    carve(need, n_dots, n_rows, nnz, B, nchunks, chunk_rows, ntx, nty, mixed_mode, jacobi, tmp);
     if (need.used > work_bytes) return QD_ERR_WORKSPACE;
   }
   if (reinterpret_cast<uintptr_t>(d_work) % 256 != 0) return QD_ERR_WORKSPACE;
   qd::Arena ar(d_work, work_bytes);
   Layout L;
-  carve(ar, n_dots, n_rows, nnz, B, nchunks, ntx, nty, mixed_mode, jacobi, L);
+  carve(ar, n_dots, n_rows, nnz, B, nchunks, chunk_rows, ntx, nty, mixed_mode, jacobi, L);
   if (mixed_mode) {
     const int init[2] = {INT_MIN, INT_MIN};
     int e2[2];
@@ -2690,6 +3071,12 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   }
   QD_CUDA_TRY(cudaMemcpyAsync(L.chunks, chunks.data(), chunks.size() * sizeof(Chunk),
                               cudaMemcpyHostToDevice, s));
+  if (mixed_mode) {
+    const int64_t nsubs = int64_t(nchunks) * L.spc;
+    stage_plan_kernel<<<int((nsubs + 7) / 8), 256, 0, s>>>(L.chunks, nchunks, L.spc, d_rowptr,
+                                                           d_col, L.plan, L.pos16);
+    QD_CHECK_LAUNCH();
+  }
   if (L.njac > 0) {
     jacobi_diag_kernel<<<int(chunks.size()), 256, 0, s>>>(L.chunks, d_rowptr, d_col, d_H, L.dinv);
     QD_CHECK_LAUNCH();
@@ -2785,8 +3172,8 @@ extern "C" int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total,
   if (h_prec) qd::dst_tiles(n_dots, h_prec, b, nullptr, &ntx, nullptr, &nty);
   qd::Arena ar(nullptr, 0);
   Layout L;
-  carve(ar, n_dots, n_rows_total, nnz_total, b, nchunks, ntx, nty, prec_mode == QD_PREC_MIXED,
-        needs_jacobi(n_dots, h_prec), L);
+  carve(ar, n_dots, n_rows_total, nnz_total, b, nchunks, chunk_rows_of(opts), ntx, nty,
+        prec_mode == QD_PREC_MIXED, needs_jacobi(n_dots, h_prec), L);
   *bytes = ar.used;
   return QD_OK;
 }
