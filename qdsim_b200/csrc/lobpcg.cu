@@ -302,13 +302,15 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 constexpr int kCsrSub = 64;                 // rows per sub-tile
 constexpr int kCsrCap = 1024;               // staged nonzeros per sub-tile
 constexpr int kStageRows = 384;             // staged vector rows per sub-tile
-constexpr int kMaxSeg = 7;                  // runs of rows per sub-tile
+constexpr int kMaxSeg = 6;                  // runs of rows per sub-tile
 constexpr int kCsrStages = 2;
+constexpr int kPlanSlots = 4;               // staged plan records (ring)
 
 // The staging plan of one sub-tile: nseg < 0 if it is read from global
-// memory; else runs [lo[s], lo[s] + len[s]) stored one after another.
+// memory; else its nonzeros [q0, q1) and runs [lo[s], lo[s] + len[s]) of
+// vector rows, stored one after another (total rows).
 struct SubPlan {
-  int nseg, total;
+  int nseg, total, q0, q1;
   int lo[kMaxSeg];
   int len[kMaxSeg];
 };
@@ -434,6 +436,8 @@ stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__re
         if (lane == 0) {
           out->nseg = nseg;
           out->total = total;
+          out->q0 = q0;
+          out->q1 = q1;
         }
       }
     }
@@ -465,6 +469,7 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   int *s_staged = s_hbase + kCsrStages;
   int *s_obase = s_staged + kCsrStages;
   __shared__ double s_th[B];
+  __shared__ __align__(16) SubPlan s_plan[kPlanSlots];
 
   // ph: the phase whose dots this launch serves (the products of X and P only
   // in the FP32 phase; W's products also in the mixed form's finishing phase)
@@ -491,41 +496,55 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   }
   __syncthreads();
   const int nblk = (XP && with_p) ? 2 : 1;   // blocks staged (P only once populated)
-  auto issue = [&](int i) {   // thread 0
+  // Thread 0 issues sub-tile i's copies from its plan record pl; each stage
+  // also brings in the record of the sub-tile issued after it (i + stages),
+  // so that no global load stands between a sub-tile's barrier and the next
+  // issue.
+  const SubPlan *plan_c = plan + size_t(blockIdx.x) * spc;
+  auto issue = [&](int i, const SubPlan &pl) {   // thread 0
     const int sst = i % kCsrStages;
     unsigned char *sb = dsm + size_t(sst) * SS::STAGE;
-    const SubPlan *pl = plan + size_t(blockIdx.x) * spc + i;
-    const int nseg = pl->nseg;
+    const int nseg = pl.nseg;
+    const bool next = i + kCsrStages < nsub;
+    const uint32_t pr = next ? uint32_t(sizeof(SubPlan)) : 0u;
     if (nseg >= 0) {
-      const int a = ch.begin + i * kCsrSub, b = min(a + kCsrSub, ch.end);
-      const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
+      const int a = ch.begin + i * kCsrSub;
+      const int q0 = pl.q0, q1 = pl.q1;
       const int pb = q0 & ~7, pe = (q1 + 7) & ~7;
       const int hb = q0 & ~1, he = (q1 + 1) & ~1;
       s_pbase[sst] = pb;
       s_hbase[sst] = hb;
       s_staged[sst] = 1;
       const uint32_t pbytes = uint32_t(pe - pb) * 2u, hbytes = uint32_t(he - hb) * 8u;
-      const uint32_t rbytes = uint32_t(pl->total) * B * 4u;
-      qd::tc::mbar_arrive_expect_tx(&full[sst], pbytes + hbytes + nblk * rbytes);
+      const uint32_t rbytes = uint32_t(pl.total) * B * 4u;
+      int off = 0, obase = 0;
+      for (int sg = 0; sg < nseg; ++sg) {   // the run of the sub-tile's own rows
+        const int lo = pl.lo[sg], len = pl.len[sg];
+        if (a >= lo && a < lo + len) obase = off - lo;
+        off += len;
+      }
+      s_obase[sst] = obase;
+      qd::tc::mbar_arrive_expect_tx(&full[sst], pbytes + hbytes + nblk * rbytes + pr);
       qd::tc::bulk_g2s(sb + SS::POS_OFF, pos16 + pb, pbytes, &full[sst]);
       qd::tc::bulk_g2s(sb + SS::HM_OFF, hm32 + hb, hbytes, &full[sst]);
-      int off = 0, obase = 0;
+      off = 0;
       for (int sg = 0; sg < nseg; ++sg) {
-        const int lo = pl->lo[sg], len = pl->len[sg];
-        if (a >= lo && a < lo + len) obase = off - lo;   // the run of the sub-tile's own rows
+        const int lo = pl.lo[sg], len = pl.len[sg];
         for (int k = 0; k < nblk; ++k)
           qd::tc::bulk_g2s(sb + SS::ROW_OFF + k * SS::BLK + size_t(off) * B * 4,
                            (k ? P : X) + size_t(lo) * B, uint32_t(len) * B * 4u, &full[sst]);
         off += len;
       }
-      s_obase[sst] = obase;
     } else {
       s_staged[sst] = 0;
-      qd::tc::mbar_arrive_expect_tx(&full[sst], 0);
+      qd::tc::mbar_arrive_expect_tx(&full[sst], pr);
     }
+    if (next)
+      qd::tc::bulk_g2s(&s_plan[(i + kCsrStages) % kPlanSlots], plan_c + i + kCsrStages,
+                       uint32_t(sizeof(SubPlan)), &full[sst]);
   };
   if (tid == 0)
-    for (int i = 0; i < kCsrStages && i < nsub; ++i) issue(i);
+    for (int i = 0; i < kCsrStages && i < nsub; ++i) issue(i, plan_c[i]);
   bool ok = true;
   for (int i = 0; i < nsub; ++i) {
     const int sst = i % kCsrStages;
@@ -624,7 +643,8 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
       }
     }
     __syncthreads();   // stage sst consumed
-    if (tid == 0 && ok && i + kCsrStages < nsub) issue(i + kCsrStages);
+    if (tid == 0 && ok && i + kCsrStages < nsub)
+      issue(i + kCsrStages, s_plan[(i + kCsrStages) % kPlanSlots]);
   }
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
@@ -725,10 +745,16 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
     qd::tc::fence_mbar_init();
   }
   __syncthreads();
-  auto issue = [&](int i) {   // thread 0
-    const int sst = i % kGatherStages;
+  // Thread 0 issues sub-tile i's copies for its nonzeros [q0, q1); it loads
+  // the bounds of the sub-tile it issues next at the top of each sub-tile, so
+  // that the issue after a sub-tile's barrier waits on no global load.
+  auto bounds = [&](int i, int &q0, int &q1) {
     const int a = ch.begin + i * kCsrSub, b = min(a + kCsrSub, ch.end);
-    const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
+    q0 = __ldg(rowptr + a);
+    q1 = __ldg(rowptr + b);
+  };
+  auto issue = [&](int i, int q0, int q1) {   // thread 0
+    const int sst = i % kGatherStages;
     if (q1 - q0 <= kGatherCap) {
       const int cb = q0 & ~3, ce = (q1 + 3) & ~3;
       const int hb = q0 & ~1, he = (q1 + 1) & ~1;
@@ -745,10 +771,16 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
     }
   };
   if (tid == 0)
-    for (int i = 0; i < kGatherStages && i < nsub; ++i) issue(i);
+    for (int i = 0; i < kGatherStages && i < nsub; ++i) {
+      int q0, q1;
+      bounds(i, q0, q1);
+      issue(i, q0, q1);
+    }
   bool ok = true;
   for (int i = 0; i < nsub; ++i) {
     const int sst = i % kGatherStages;
+    int nq0 = 0, nq1 = 0;   // bounds of sub-tile i + stages (thread 0)
+    if (tid == 0 && i + kGatherStages < nsub) bounds(i + kGatherStages, nq0, nq1);
     // the sub-tile's rows in two halves of one parity each (even offsets,
     // then odd): on the row-major lattice of a P2 mesh, rows two apart have
     // the same stencil, so the k-th neighbours gathered by one warp lie close
@@ -833,7 +865,7 @@ spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict
       }
     }
     __syncthreads();   // stage sst consumed
-    if (tid == 0 && ok && i + kGatherStages < nsub) issue(i + kGatherStages);
+    if (tid == 0 && ok && i + kGatherStages < nsub) issue(i + kGatherStages, nq0, nq1);
   }
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
