@@ -38,12 +38,12 @@ UNIT = "eigenpairs/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "sweep256.npz")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
-# DRAM traffic over algorithmic bytes per kernel kind, from ncu captures of
+# DRAM traffic over algorithmic bytes per kernel kind, from an ncu capture of
 # the first 24 dots of the sweep (dram__bytes_read.sum + dram__bytes_write.sum
-# of the FP32-phase SpMM launches divided by their algorithmic bytes: 498.2 of
-# 529.7 MB for the products of X and P, 326.9 of 332.2 MB for those of W); the
+# of the FP32-phase SpMM launches divided by their algorithmic bytes: 497.3 of
+# 529.7 MB for the products of X and P, 274.8 of 305.7 MB for those of W); the
 # roofline's `traffic` is the algorithmic bytes per launch times this ratio.
-TRAFFIC_RATIO = {"spmm": 0.957}
+TRAFFIC_RATIO = {"spmm": 0.924}
 KIND_NAMES = ["spmm", "gram", "rayleigh_ritz", "update", "assemble", "pcg", "adjoint",
               "dst_precond", "ortho", "other"]
 
@@ -603,15 +603,14 @@ def algorithmic_bytes(hb, counts, k_block, mixed=True):
 
     Per dot and launch (n rows, z nonzeros, block B; counts[:, 0] and
     counts[:, 3] count both SpMM launches of an iteration):
-      FP32 phase (vectors 4 bytes, matrix values an 8-byte FP32 (H, M) pair;
-      the products of X and P read 2-byte staged positions for the column
-      indices, those of W the 4-byte indices):
-        spmm   z (2 + 8) + z (4 + 8) + 8 n + 3 n B 4 gathered + 7 n B 4 written
+      FP32 phase (vectors 4 bytes, matrix values an 8-byte FP32 (H, M) pair,
+      column indices as 2-byte staged positions):
+        spmm   2 (z (2 + 8) + 4 n) + 3 n B 4 gathered + 7 n B 4 written
         gram   9 n B 4 read;  dst (2 4 + 12) n B;  ortho 14 n B 4;  update 5 n B 4
       FP64 phase of the plain form (vectors 8, values 16): the same with 8 / 16
       finishing phase of the mixed form (X, HX, MX FP64; W, P and their
       products FP32; X's products from the FP64 values, W's from the pairs):
-        spmm   z (4 + 16) + z (4 + 8) + 8 n + n B (8 + 4 + 2 8 + 3 4 + 4 + 2 4)
+        spmm   z (4 + 16) + z (2 + 8) + 8 n + n B (8 + 4 + 2 8 + 3 4 + 4 + 2 4)
         gram   n B (3 8 + 6 4);  dst (2 4 + 12) n B
         ortho  n B (8 + 2 4) + n B (3 8 + 4 4 + 4 4);  update n B (8 + 2 4 + 8 + 4)
     """
@@ -629,12 +628,12 @@ def algorithmic_bytes(hb, counts, k_block, mixed=True):
         gr = counts[:, ph * 3 + 1]
         up = counts[:, ph * 3 + 2]
         if ph == 1 and mixed:
-            add({"spmm": it * (32 * z + 8 * n + 52 * n * B),
+            add({"spmm": it * (30 * z + 8 * n + 52 * n * B),
                  "gram": gr * 48 * n * B, "dst_precond": gr * 20 * n * B,
                  "ortho": gr * 72 * n * B, "update": up * 28 * n * B})
             continue
         s, v = (4.0, 8.0) if ph == 0 else (8.0, 16.0)
-        csr = z * (2 + v) + z * (4 + v) if ph == 0 else 2 * z * (4 + v)
+        csr = 2 * z * ((2 if ph == 0 else 4) + v)
         add({"spmm": it * (csr + 8 * n + 3 * n * B * s + 7 * n * B * s),
              "gram": gr * 9 * n * B * s, "dst_precond": gr * n * B * (2 * s + 12),
              "ortho": gr * 14 * n * B * s, "update": up * 5 * n * B * s})

@@ -281,27 +281,22 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
 
 // ---------------------------------------------------------------------------
 // FP32-phase SpMM with every operand of a sub-tile staged in shared memory.
-// A sub-tile of 64 rows needs the nonzeros [rowptr[a], rowptr[b]) and the
+// A sub-tile of rows [a, b) needs the nonzeros [rowptr[a], rowptr[b]) and the
 // vector rows its columns name.  On a lattice those rows form a few runs (one
-// per lattice line of the stencil: five for a P2 sub-tile inside one line,
-// about 260 rows in all), so a plan built once per solve (stage_plan_kernel)
-// lists each sub-tile's runs of rows and rewrites every column index as a
-// position in the staged copy (16-bit).  The kernel then fetches, per
-// sub-tile, the positions, the FP32 (H, M) pairs and the runs of X (and P) by
-// 1-D bulk copies into a 2-stage mbarrier pipeline, and every gather of the
-// nonzero loop is a shared-memory load.  A sub-tile with more nonzeros, runs
-// or rows than a stage holds reads everything from global memory instead
-// (same arithmetic, same results).
+// per lattice line of the stencil: five for a P2 sub-tile of 64 rows inside
+// one line, about 260 rows in all), so a plan built once per solve
+// (stage_plan_kernel) lists each sub-tile's runs of rows and rewrites every
+// column index as a position in the staged copy (16-bit).  The kernel then
+// fetches, per sub-tile, the positions, the FP32 (H, M) pairs and the runs of
+// X (and P) by 1-D bulk copies into a 2-stage mbarrier pipeline, and every
+// gather of the nonzero loop is a shared-memory load.  A sub-tile with more
+// nonzeros, runs or rows than a stage holds reads everything from global
+// memory instead (same arithmetic, same results).
 // XP: products of X and P with the residual W = HX - MX Theta and per-chunk
-// norms; otherwise the products of one block (W -> HW, MW).  The solver uses
-// this form for the products of X and P (two CTAs of 384 threads per SM) and
-// spmm32_kernel below for those of W: with one block per row the staged form
-// keeps fewer warps resident than the gathering form (four CTAs per SM) and
-// measured slower.
+// norms, in sub-tiles of 64 rows (six threads per row); otherwise the
+// products of one block (W -> HW, MW) in sub-tiles of 128 rows (three threads
+// per row).  Either way a CTA has 32 B threads and two fit on an SM (B <= 12).
 // ---------------------------------------------------------------------------
-constexpr int kCsrSub = 64;                 // rows per sub-tile
-constexpr int kCsrCap = 1024;               // staged nonzeros per sub-tile
-constexpr int kStageRows = 384;             // staged vector rows per sub-tile
 constexpr int kMaxSeg = 6;                  // runs of rows per sub-tile
 constexpr int kCsrStages = 2;
 constexpr int kPlanSlots = 4;               // staged plan records (ring)
@@ -316,9 +311,21 @@ struct SubPlan {
 };
 static_assert(sizeof(SubPlan) == 64, "one 64-byte record per sub-tile");
 
-template <int B, int NBLK> struct SpmmStage {
-  static constexpr int POS = kCsrCap + 16;        // uint16 slots (16-byte rounding slack)
-  static constexpr int HM = kCsrCap + 4;          // float2 slots
+// Sub-tiles of SUBR rows: staged nonzeros and vector rows per sub-tile (on a
+// P2 lattice at most 896 / 342 for 64 rows and 1792 / 649 for 128).
+template <int SUBR> struct StageCap;
+template <> struct StageCap<64> {
+  static constexpr int NNZ = 1024, ROWS = 384;
+};
+template <> struct StageCap<128> {
+  static constexpr int NNZ = 2048, ROWS = 672;
+};
+
+template <int B, int NBLK, int SUBR> struct SpmmStage {
+  static constexpr int CAP = StageCap<SUBR>::NNZ;
+  static constexpr int ROWS = StageCap<SUBR>::ROWS;
+  static constexpr int POS = CAP + 16;            // uint16 slots (16-byte rounding slack)
+  static constexpr int HM = CAP + 4;              // float2 slots
   // Consecutive staged blocks are 12 floats further apart than their size:
   // with B = 12, rows j of X and P then fall on disjoint banks, so the
   // warp-wide gathers (three threads per row and block) are conflict-free.
@@ -326,7 +333,7 @@ template <int B, int NBLK> struct SpmmStage {
   static constexpr size_t POS_OFF = 0;
   static constexpr size_t HM_OFF = size_t(POS) * 2;
   static constexpr size_t ROW_OFF = HM_OFF + size_t(HM) * 8;
-  static constexpr size_t BLK = size_t(kStageRows * B + SKEW) * 4;
+  static constexpr size_t BLK = size_t(ROWS * B + SKEW) * 4;
   static constexpr size_t STAGE = ROW_OFF + NBLK * BLK;
   static constexpr size_t META_OFF = kCsrStages * STAGE;
   // barriers, then per stage: position base, pair base, staged flag, and
@@ -336,11 +343,13 @@ template <int B, int NBLK> struct SpmmStage {
                 "bulk-copy destinations must be 16-byte aligned");
 };
 
-// One warp per sub-tile (chunk c, sub-tile i at record c * spc + i): the runs
+// One warp per sub-tile of SUBR rows (chunk c, sub-tile i at record
+// c * spc + i): the runs
 // of the column indices of its nonzeros and their staged positions.  Runs are
 // found as maximal runs of touched 8-row blocks (so gaps of fewer than 8
 // untouched rows are staged with them), then trimmed to the smallest and
 // largest column they hold.
+template <int SUBR>
 __global__ void __launch_bounds__(256)
 stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__restrict__ rowptr,
                   const int32_t *__restrict__ col, SubPlan *__restrict__ plan,
@@ -353,13 +362,13 @@ stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__re
   const int64_t t = int64_t(blockIdx.x) * 8 + w;
   if (t >= int64_t(nchunks) * spc) return;   // whole warps; only warp syncs below
   const Chunk ch = chunks[t / spc];
-  const int a = ch.begin + int(t % spc) * kCsrSub;
+  const int a = ch.begin + int(t % spc) * SUBR;
   SubPlan *out = plan + t;
   if (a >= ch.end) {
     if (lane == 0) out->nseg = -1;
     return;
   }
-  const int b = min(a + kCsrSub, ch.end);
+  const int b = min(a + SUBR, ch.end);
   const int q0 = __ldg(rowptr + a), q1 = __ldg(rowptr + b);
   int cmin = INT_MAX, cmax = INT_MIN;
   for (int p = q0 + lane; p < q1; p += 32) {
@@ -371,7 +380,8 @@ stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__re
     cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
     cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
   }
-  bool ok = q1 > q0 && q1 - q0 <= kCsrCap && int64_t(cmax) - cmin < int64_t(NW) * 32 * 8;
+  bool ok = q1 > q0 && q1 - q0 <= StageCap<SUBR>::NNZ &&
+            int64_t(cmax) - cmin < int64_t(NW) * 32 * 8;
   if (ok) {
     for (int k = lane; k < NW; k += 32) s_bits[w][k] = 0u;
     __syncwarp();
@@ -421,7 +431,7 @@ stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__re
       total = __shfl_sync(0xffffffffu, total, 0);
       own = __shfl_sync(0xffffffffu, own, 0);
       __syncwarp();
-      ok = total <= kStageRows && own;
+      ok = total <= StageCap<SUBR>::ROWS && own;
       if (ok) {
         for (int p = q0 + lane; p < q1; p += 32) {
           const int j = __ldg(col + p), blk = (j - cmin) >> 3;
@@ -446,7 +456,7 @@ stage_plan_kernel(const Chunk *chunks, int nchunks, int spc, const int32_t *__re
 }
 
 template <int B, bool XP>
-__global__ void __launch_bounds__(64 * (B / 4) * (XP ? 2 : 1), XP ? (B <= 12 ? 2 : 1) : 3)
+__global__ void __launch_bounds__(32 * B, B <= 12 ? 2 : 1)
 spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
                const int32_t *__restrict__ col32, const uint16_t *__restrict__ pos16,
                const SubPlan *__restrict__ plan, int spc, const float2 *__restrict__ hm32,
@@ -457,9 +467,10 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
                double *__restrict__ norms, int *wait_err, int ph) {
   constexpr int G = B / 4;
   constexpr int G2 = XP ? 2 * G : G;
-  constexpr int NT = kCsrSub * G2;
+  constexpr int SUBR = XP ? 64 : 128;   // rows per sub-tile: 32 B threads either way
+  constexpr int NT = SUBR * G2;
   constexpr int NBLK = XP ? 2 : 1;
-  using SS = SpmmStage<B, NBLK>;
+  using SS = SpmmStage<B, NBLK, SUBR>;
   static_assert(!XP || size_t(NT) * 8 * sizeof(double) <= SS::META_OFF,
                 "the norm slots reuse the stage buffers");
   extern __shared__ __align__(128) unsigned char dsm[];
@@ -489,7 +500,7 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   double red[8];
 #pragma unroll
   for (int c = 0; c < 8; ++c) red[c] = 0.0;
-  const int nsub = (ch.end - ch.begin + kCsrSub - 1) / kCsrSub;
+  const int nsub = (ch.end - ch.begin + SUBR - 1) / SUBR;
   if (tid == 0) {
     for (int i = 0; i < kCsrStages; ++i) qd::tc::mbar_init(&full[i], 1);
     qd::tc::fence_mbar_init();
@@ -508,7 +519,7 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
     const bool next = i + kCsrStages < nsub;
     const uint32_t pr = next ? uint32_t(sizeof(SubPlan)) : 0u;
     if (nseg >= 0) {
-      const int a = ch.begin + i * kCsrSub;
+      const int a = ch.begin + i * SUBR;
       const int q0 = pl.q0, q1 = pl.q1;
       const int pb = q0 & ~7, pe = (q1 + 7) & ~7;
       const int hb = q0 & ~1, he = (q1 + 1) & ~1;
@@ -551,8 +562,8 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
     // the sub-tile's rows in two halves of one parity each (even offsets,
     // then odd): on the row-major lattice of a P2 mesh, rows two apart have
     // the same stencil, so the k-th neighbours gathered by one warp lie close
-    const int ofs = sub < kCsrSub / 2 ? 2 * sub : 2 * (sub - kCsrSub / 2) + 1;
-    const int r = ch.begin + i * kCsrSub + ofs;
+    const int ofs = sub < SUBR / 2 ? 2 * sub : 2 * (sub - SUBR / 2) + 1;
+    const int r = ch.begin + i * SUBR + ofs;
     const bool live = r < ch.end;
     int p0 = 0, p1 = 0;
     float rs = 0.f;
@@ -664,7 +675,7 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
     if (tid < B) {
       const int j = tid, gj = j / 4, cj = j % 4;
       double a = 0.0, b = 0.0;
-      for (int sr = 0; sr < kCsrSub; ++sr) {
+      for (int sr = 0; sr < SUBR; ++sr) {
         const int t = sr * G2 + gj;
         a += s_red[(2 * cj) * NT + t];
         b += s_red[(2 * cj + 1) * NT + t];
@@ -672,220 +683,6 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
       norms[size_t(blockIdx.x) * 2 * B + j] = a;
       norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
     }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// FP32-phase SpMM with the CSR streamed through shared memory and the vector
-// rows gathered from global memory (L1/L2).  Each sub-tile of 64 rows needs
-// the column indices and (H, M) pairs of the nonzero range [rowptr[a],
-// rowptr[b]); both ranges are fetched by 1-D bulk copies (rounded out to
-// 16-byte boundaries; the workspace copies `col32` and `hm32` carry the
-// slack) into a 3-stage mbarrier pipeline.  A sub-tile with more than
-// kGatherCap nonzeros reads the CSR from global memory.  Same products and
-// arguments as spmm32s_kernel; the solver uses this form for W's products.
-// ---------------------------------------------------------------------------
-constexpr int kGatherCap = kCsrSub * 20;    // staged nonzeros per sub-tile
-constexpr int kGatherStages = 3;
-struct GatherStage {
-  static constexpr int COL = kGatherCap + 8;   // int32 slots (16-byte rounding slack)
-  static constexpr int HM = kGatherCap + 4;    // float2 slots
-  static constexpr size_t COL_OFF = 0;
-  static constexpr size_t HM_OFF = size_t(kGatherStages) * COL * 4;
-  static constexpr size_t META_OFF = HM_OFF + size_t(kGatherStages) * HM * 8;
-  // barriers, then per stage: col base, hm base, staged flag
-  static constexpr size_t BYTES = META_OFF + kGatherStages * 8 + kGatherStages * 3 * 4;
-};
-
-template <int B, bool XP>
-__global__ void __launch_bounds__(64 * (B / 4) * (XP ? 2 : 1), XP ? 3 : 6)
-spmm32_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
-              const int32_t *__restrict__ col32, const float2 *__restrict__ hm32,
-              const float *__restrict__ rs32, double sh, double smv,
-              const double *__restrict__ theta, const float *__restrict__ X,
-              const float *__restrict__ P, float *__restrict__ HX, float *__restrict__ MX,
-              float *__restrict__ HP, float *__restrict__ MP, float *__restrict__ W,
-              double *__restrict__ norms, int *wait_err, int ph) {
-  constexpr int G = B / 4;
-  constexpr int G2 = XP ? 2 * G : G;
-  constexpr int NT = kCsrSub * G2;
-  using CS = GatherStage;
-  extern __shared__ __align__(128) unsigned char dsm[];
-  int32_t *s_col = reinterpret_cast<int32_t *>(dsm + CS::COL_OFF);
-  float2 *s_hm = reinterpret_cast<float2 *>(dsm + CS::HM_OFF);
-  uint64_t *full = reinterpret_cast<uint64_t *>(dsm + CS::META_OFF);
-  int *s_cbase = reinterpret_cast<int *>(full + kGatherStages);
-  int *s_hbase = s_cbase + kGatherStages;
-  int *s_staged = s_hbase + kGatherStages;
-  __shared__ double s_th[B];
-  __shared__ double s_red[XP ? NT * 8 : 1];
-
-  // ph: the phase whose dots this launch serves (the products of X and P only
-  // in the FP32 phase; W's products also in the mixed form's finishing phase)
-  const Chunk ch = chunks[blockIdx.x];
-  const DotState &sd = st[ch.dot];
-  if (!sd.run[ph]) return;
-  const bool with_p = sd.has_p != 0;
-  const int tid = threadIdx.x;
-  if (tid == 0 && blockIdx.x == sd.chunk0)
-    const_cast<DotState *>(st)[ch.dot].launches[ph][0]++;
-  if (XP && tid < B) s_th[tid] = theta[size_t(ch.dot) * B + tid];
-  const int sub = tid / G2, gg = tid % G2;
-  const bool isx = gg < G;
-  const int g = isx ? gg : gg - G;
-  // norm slots, layout [8][threads]: consecutive threads hit consecutive banks
-  double *my_red = XP ? s_red + tid : nullptr;
-  if (XP) {
-#pragma unroll
-    for (int c = 0; c < 8; ++c) my_red[c * NT] = 0.0;
-  }
-  const int nsub = (ch.end - ch.begin + kCsrSub - 1) / kCsrSub;
-  if (tid == 0) {
-    for (int i = 0; i < kGatherStages; ++i) qd::tc::mbar_init(&full[i], 1);
-    qd::tc::fence_mbar_init();
-  }
-  __syncthreads();
-  // Thread 0 issues sub-tile i's copies for its nonzeros [q0, q1); it loads
-  // the bounds of the sub-tile it issues next at the top of each sub-tile, so
-  // that the issue after a sub-tile's barrier waits on no global load.
-  auto bounds = [&](int i, int &q0, int &q1) {
-    const int a = ch.begin + i * kCsrSub, b = min(a + kCsrSub, ch.end);
-    q0 = __ldg(rowptr + a);
-    q1 = __ldg(rowptr + b);
-  };
-  auto issue = [&](int i, int q0, int q1) {   // thread 0
-    const int sst = i % kGatherStages;
-    if (q1 - q0 <= kGatherCap) {
-      const int cb = q0 & ~3, ce = (q1 + 3) & ~3;
-      const int hb = q0 & ~1, he = (q1 + 1) & ~1;
-      s_cbase[sst] = cb;
-      s_hbase[sst] = hb;
-      s_staged[sst] = 1;
-      const uint32_t cbytes = uint32_t(ce - cb) * 4u, hbytes = uint32_t(he - hb) * 8u;
-      qd::tc::mbar_arrive_expect_tx(&full[sst], cbytes + hbytes);
-      if (cbytes) qd::tc::bulk_g2s(s_col + sst * CS::COL, col32 + cb, cbytes, &full[sst]);
-      if (hbytes) qd::tc::bulk_g2s(s_hm + sst * CS::HM, hm32 + hb, hbytes, &full[sst]);
-    } else {
-      s_staged[sst] = 0;
-      qd::tc::mbar_arrive_expect_tx(&full[sst], 0);
-    }
-  };
-  if (tid == 0)
-    for (int i = 0; i < kGatherStages && i < nsub; ++i) {
-      int q0, q1;
-      bounds(i, q0, q1);
-      issue(i, q0, q1);
-    }
-  bool ok = true;
-  for (int i = 0; i < nsub; ++i) {
-    const int sst = i % kGatherStages;
-    int nq0 = 0, nq1 = 0;   // bounds of sub-tile i + stages (thread 0)
-    if (tid == 0 && i + kGatherStages < nsub) bounds(i + kGatherStages, nq0, nq1);
-    // the sub-tile's rows in two halves of one parity each (even offsets,
-    // then odd): on the row-major lattice of a P2 mesh, rows two apart have
-    // the same stencil, so the k-th neighbours gathered by one warp lie close
-    const int ofs = sub < kCsrSub / 2 ? 2 * sub : 2 * (sub - kCsrSub / 2) + 1;
-    const int r = ch.begin + i * kCsrSub + ofs;
-    const bool live = r < ch.end;
-    int p0 = 0, p1 = 0;
-    if (live) {
-      p0 = __ldg(rowptr + r);
-      p1 = __ldg(rowptr + r + 1);
-    }
-    ok = qd::tc::mbar_wait(&full[sst], (i / kGatherStages) & 1, qd::kPipeWaitNs) && ok;
-    if (ok && live) {
-      if (XP && !isx && !with_p) {
-        const double z[4] = {0, 0, 0, 0};
-        qd::V4<float>::store(HP + size_t(r) * B + 4 * g, z);
-        qd::V4<float>::store(MP + size_t(r) * B + 4 * g, z);
-      } else {
-        const float *src = (XP && !isx) ? P : X;
-        // FP32 arithmetic, H differenced against the row's own entry:
-        //   (H x)_i = sum_j H_ij (x_j - x_i) + (sum_j H_ij) x_i
-        // The stiffness part of H has (near) zero row sums, so the terms are
-        // small where x is smooth and FP32 accumulation stays ~1e-6 accurate
-        // relative to H x (undifferenced, the terms exceed H x by up to 1e4).
-        const float4 xi = __ldg(reinterpret_cast<const float4 *>(src + size_t(r) * B + 4 * g));
-        float h[4] = {0.f, 0.f, 0.f, 0.f}, m[4] = {0.f, 0.f, 0.f, 0.f};
-        auto row = [&](auto getc, auto getv) {
-#pragma unroll 4
-          for (int p = p0; p < p1; ++p) {
-            const int j = getc(p);
-            const float2 v = getv(p);
-            const float4 xj = __ldg(reinterpret_cast<const float4 *>(src + size_t(j) * B + 4 * g));
-            h[0] = fmaf(v.x, xj.x - xi.x, h[0]);
-            h[1] = fmaf(v.x, xj.y - xi.y, h[1]);
-            h[2] = fmaf(v.x, xj.z - xi.z, h[2]);
-            h[3] = fmaf(v.x, xj.w - xi.w, h[3]);
-            m[0] = fmaf(v.y, xj.x, m[0]);
-            m[1] = fmaf(v.y, xj.y, m[1]);
-            m[2] = fmaf(v.y, xj.z, m[2]);
-            m[3] = fmaf(v.y, xj.w, m[3]);
-          }
-        };
-        if (s_staged[sst]) {
-          const int32_t *cs = s_col + sst * CS::COL;
-          const float2 *hs = s_hm + sst * CS::HM;
-          const int cb = s_cbase[sst], hb = s_hbase[sst];
-          row([&](int p) { return cs[p - cb]; }, [&](int p) { return hs[p - hb]; });
-        } else {
-          row([&](int p) { return __ldg(col32 + p); }, [&](int p) { return __ldg(hm32 + p); });
-        }
-        const float rs = __ldg(rs32 + r);
-        h[0] = fmaf(rs, xi.x, h[0]);
-        h[1] = fmaf(rs, xi.y, h[1]);
-        h[2] = fmaf(rs, xi.z, h[2]);
-        h[3] = fmaf(rs, xi.w, h[3]);
-        const size_t o = size_t(r) * B + 4 * g;
-        // back to the matrices' own scale (powers of two: exact)
-        const float fsh = float(sh), fsm = float(smv);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          h[c] *= fsh;
-          m[c] *= fsm;
-        }
-        if (XP && isx) {
-          double res[4];
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            // residual from the stored (rounded) products, as the iteration sees them
-            const double hq = double(h[c]), mq = double(m[c]);
-            res[c] = hq - s_th[4 * g + c] * mq;
-            my_red[(2 * c) * NT] += res[c] * res[c];
-            my_red[(2 * c + 1) * NT] += mq * mq;
-          }
-          *reinterpret_cast<float4 *>(HX + o) = make_float4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<float4 *>(MX + o) = make_float4(m[0], m[1], m[2], m[3]);
-          qd::V4<float>::store(W + o, res);
-        } else {
-          float *oh = XP ? HP : HX, *om = XP ? MP : MX;
-          *reinterpret_cast<float4 *>(oh + o) = make_float4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<float4 *>(om + o) = make_float4(m[0], m[1], m[2], m[3]);
-        }
-      }
-    }
-    __syncthreads();   // stage sst consumed
-    if (tid == 0 && ok && i + kGatherStages < nsub) issue(i + kGatherStages, nq0, nq1);
-  }
-  if (__syncthreads_or(!ok)) {
-    if (tid == 0) {
-      atomicOr(wait_err, 1);
-      for (int i = max(0, nsub - kGatherStages); i < nsub; ++i)
-        qd::tc::mbar_wait(&full[i % kGatherStages], (i / kGatherStages) & 1, qd::kPipeWaitNs);
-    }
-    return;
-  }
-  if (XP && tid < B) {
-    // per-chunk column norms (fixed-order reduction over the CTA's rows)
-    const int j = tid, gj = j / 4, cj = j % 4;
-    double a = 0.0, b = 0.0;
-    for (int sr = 0; sr < kCsrSub; ++sr) {
-      const int t = sr * G2 + gj;
-      a += s_red[(2 * cj) * NT + t];
-      b += s_red[(2 * cj + 1) * NT + t];
-    }
-    norms[size_t(blockIdx.x) * 2 * B + j] = a;
-    norms[size_t(blockIdx.x) * 2 * B + B + j] = b;
   }
 }
 
@@ -2565,9 +2362,12 @@ struct Layout {
   int njac;              // chunks of such dots
   float2 *hm32;          // FP32 (H, M) pairs per nonzero (mixed precision only)
   int32_t *col32;        // copy of the column indices with bulk-copy slack (mixed only)
-  uint16_t *pos16;       // staged position of every nonzero's column (mixed only)
-  SubPlan *plan;         // staging plan per 64-row sub-tile (mixed only)
-  int spc;               // sub-tiles per chunk
+  uint16_t *pos16;       // staged position of every nonzero's column (mixed only):
+  SubPlan *plan;         //   64-row sub-tiles (products of X and P), plan per sub-tile
+  int spc;               //   sub-tiles per chunk
+  uint16_t *pos16w;      // the same for 128-row sub-tiles (products of W)
+  SubPlan *planw;
+  int spcw;
   float *rs32;           // row sums of the FP32 H values, summed in FP64 (mixed only)
   int *hm_exp;           // largest binary exponents of |H| and |M|
   double hm_sh, hm_sm;   // 2^exponent: scale of the FP32 pairs
@@ -2602,9 +2402,12 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   L.hm32 = mixed ? ar.take<float2>(size_t(nnz) + 2) : nullptr;
   L.col32 = mixed ? ar.take<int32_t>(size_t(nnz) + 4) : nullptr;
   L.rs32 = mixed ? ar.take<float>(size_t(n_rows)) : nullptr;
-  L.spc = chunk_rows / kCsrSub;
+  L.spc = (chunk_rows + 63) / 64;
   L.pos16 = mixed ? ar.take<uint16_t>(size_t(nnz) + 16) : nullptr;
   L.plan = mixed ? ar.take<SubPlan>(size_t(nchunks) * L.spc) : nullptr;
+  L.spcw = (chunk_rows + 127) / 128;
+  L.pos16w = mixed ? ar.take<uint16_t>(size_t(nnz) + 16) : nullptr;
+  L.planw = mixed ? ar.take<SubPlan>(size_t(nchunks) * L.spcw) : nullptr;
   L.hm_exp = ar.take<int>(2);
   L.hm_sh = L.hm_sm = 1.0;
   L.dinv = jacobi ? ar.take<double>(size_t(n_rows)) : nullptr;
@@ -2667,6 +2470,18 @@ struct Bufs {
   }
 };
 
+// FP32 products of W (HW, MW) for the dots iterating in phase ph.
+template <int B>
+int spmm32_w(const Layout &L, const int32_t *rowptr, const float *W, float *HW, float *MW,
+             int ph, cudaStream_t s) {
+  constexpr size_t bytes = SpmmStage<B, 1, 128>::BYTES;
+  if (smem_attr<spmm32s_kernel<B, false>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+  spmm32s_kernel<B, false><<<L.nchunks, 32 * B, bytes, s>>>(
+      L.chunks, L.st, rowptr, L.col32, L.pos16w, L.planw, L.spcw, L.hm32, L.rs32, L.hm_sh,
+      L.hm_sm, L.theta, W, nullptr, HW, MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, ph);
+  return QD_OK;
+}
+
 // Everything of one iteration up to the Rayleigh-Ritz step, for the dots in
 // the phase of precision TV.
 template <typename TV, int B>
@@ -2678,11 +2493,11 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   qd::prof_begin(qd::PK_SPMM, s);
   const auto A = MatFor<TV>::make(L, H, M);
   if constexpr (sizeof(TV) == 4) {
-    if (smem_attr<spmm32s_kernel<B, true>>(SpmmStage<B, 2>::BYTES) != cudaSuccess)
-      return QD_ERR_CUDA;
-    spmm32s_kernel<B, true><<<L.nchunks, 128 * G, SpmmStage<B, 2>::BYTES, s>>>(
-        L.chunks, L.st, rowptr, L.col32, L.pos16, L.plan, L.spc, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.X, b.P,
-        b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err, 0);
+    constexpr size_t bytes = SpmmStage<B, 2, 64>::BYTES;
+    if (smem_attr<spmm32s_kernel<B, true>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
+    spmm32s_kernel<B, true><<<L.nchunks, 32 * B, bytes, s>>>(
+        L.chunks, L.st, rowptr, L.col32, L.pos16, L.plan, L.spc, L.hm32, L.rs32, L.hm_sh,
+        L.hm_sm, L.theta, b.X, b.P, b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err, 0);
   } else {
     spmm_xp_kernel<TV, TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A,
                                                             L.theta, b.X, b.P, b.HX, b.MX,
@@ -2726,10 +2541,7 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
   if constexpr (sizeof(TV) == 4) {
-    if (smem_attr<spmm32_kernel<B, false>>(GatherStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
-    spmm32_kernel<B, false><<<L.nchunks, 64 * G, GatherStage::BYTES, s>>>(
-        L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W,
-        nullptr, b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, 0);
+    if (spmm32_w<B>(L, rowptr, b.W, b.HW, b.MW, 0, s) != QD_OK) return QD_ERR_CUDA;
   } else {
     spmm_chunk_kernel<TV, B><<<L.nchunks, 64 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A, b.W,
                                                           b.HW, b.MW);
@@ -2813,10 +2625,7 @@ int phase_sequence_mx(const Layout &L, const Bufs<float> &b, const Bufs<double> 
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_SPMM, s);
-  if (smem_attr<spmm32_kernel<B, false>>(GatherStage::BYTES) != cudaSuccess) return QD_ERR_CUDA;
-  spmm32_kernel<B, false><<<L.nchunks, 64 * G, GatherStage::BYTES, s>>>(
-      L.chunks, L.st, rowptr, L.col32, L.hm32, L.rs32, L.hm_sh, L.hm_sm, L.theta, b.W, nullptr,
-      b.HW, b.MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, 1);
+  if (spmm32_w<B>(L, rowptr, b.W, b.HW, b.MW, 1, s) != QD_OK) return QD_ERR_CUDA;
   qd::prof_end(qd::PK_SPMM, s);
   QD_CHECK_LAUNCH();
   qd::prof_begin(qd::PK_GRAM, s);
@@ -3104,9 +2913,12 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   QD_CUDA_TRY(cudaMemcpyAsync(L.chunks, chunks.data(), chunks.size() * sizeof(Chunk),
                               cudaMemcpyHostToDevice, s));
   if (mixed_mode) {
-    const int64_t nsubs = int64_t(nchunks) * L.spc;
-    stage_plan_kernel<<<int((nsubs + 7) / 8), 256, 0, s>>>(L.chunks, nchunks, L.spc, d_rowptr,
-                                                           d_col, L.plan, L.pos16);
+    const int64_t nsubs = int64_t(nchunks) * L.spc, nsubw = int64_t(nchunks) * L.spcw;
+    stage_plan_kernel<64><<<int((nsubs + 7) / 8), 256, 0, s>>>(L.chunks, nchunks, L.spc,
+                                                               d_rowptr, d_col, L.plan, L.pos16);
+    QD_CHECK_LAUNCH();
+    stage_plan_kernel<128><<<int((nsubw + 7) / 8), 256, 0, s>>>(
+        L.chunks, nchunks, L.spcw, d_rowptr, d_col, L.planw, L.pos16w);
     QD_CHECK_LAUNCH();
   }
   if (L.njac > 0) {
