@@ -121,8 +121,11 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
               const int32_t *__restrict__ row_off, const uint16_t *__restrict__ mats, int B,
               int rows_max, const TI *__restrict__ in, TO *__restrict__ out, int *err) {
   const GemmTile t = tiles[blockIdx.x];
-  if (active && !active[size_t(t.dot) * active_stride]) return;
+  // the dot's flag, descriptor and row offset in one round of loads
+  const int run = active ? active[size_t(t.dot) * active_stride] : 1;
   const qd_dst_prec d = desc[t.dot];
+  const int32_t roff = row_off[t.dot];
+  if (!run) return;
   const int dim = YPASS ? d.ny : d.nx;
   const int other = YPASS ? d.nx : d.ny;
   const int ncols = other * B;
@@ -130,7 +133,7 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   const int rows = min(kTcRows, tc_rpad(dim) - t.m0);   // multiple of 16
   const uint32_t tcols = tc_tmem_cols(rows);
   const uint16_t *S = mats + (YPASS ? d.sy_off : d.sx_off) + int64_t(t.m0) * KS * kTcK;
-  const size_t base = size_t(row_off[t.dot]) * B;
+  const size_t base = size_t(roff) * B;
 
   extern __shared__ __align__(1024) uint8_t sm[];
   const TcSmem lay(rows_max);
@@ -175,8 +178,20 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   const uint32_t lboB = uint32_t(rows) * 16u;     // (rows / 8) core matrices x 128 bytes
   const uint32_t bbytes = uint32_t(rows) * 128u;  // one B slab
   const uint32_t bstage = lay.b_off[1] - lay.b_off[0];
-  int issued = 0;   // slabs whose copy and MMAs thread 0 has issued
+  int issued = 0;    // slabs whose MMAs thread 0 has issued
+  int bissued = 0;   // slabs whose operand-B copy thread 0 has issued
   bool fail = false;
+  // Operand B of slab s + 1 is fetched as soon as the MMAs of slab s - 1 (the
+  // last reader of its stage) are done, right after slab s's MMAs are issued,
+  // so that the copy lands while the threads stage operand A of slab s + 1.
+  auto issue_b = [&](int s) {   // thread 0
+    const int st = s & 1;
+    tc::mbar_arrive_expect_tx(&bar_full[st], bbytes);
+    tc::bulk_g2s(sm + lay.b_off[0] + st * bstage, S + size_t(s) * rows * kTcK, bbytes,
+                 &bar_full[st]);
+    bissued = s + 1;
+  };
+  if (tid == 0) issue_b(0);
   // A slab: the thread's adjacent columns pn, pn + 1 and K chunks pg, pg + 4
   // (8 consecutive k each), both columns of a k loaded with one access (B is
   // even and n0 a multiple of 128, so an even n and n + 1 are adjacent in both
@@ -206,11 +221,6 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
   for (int s = 0; s < KS; ++s) {
     const int st = s & 1;
     if (s >= 2 && !tc::mbar_wait(&bar_mma[st], ((s - 2) >> 1) & 1, kTcWaitNs)) fail = true;
-    if (tid == 0 && !fail) {
-      tc::mbar_arrive_expect_tx(&bar_full[st], bbytes);
-      tc::bulk_g2s(sm + lay.b_off[0] + st * bstage, S + size_t(s) * rows * kTcK, bbytes,
-                   &bar_full[st]);
-    }
     const uint32_t sA = sA0 + uint32_t(st) * kTcABytes, sB = sB0 + uint32_t(st) * bstage;
     uint8_t *a_st = sm + lay.a_off[0] + st * kTcABytes;
 #pragma unroll
@@ -247,6 +257,13 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
           }
         }
         tc::mma_commit(&bar_mma[st]);
+        if (s + 1 < KS) {
+          // stage (s + 1) & 1 was last read by the MMAs of slab s - 1
+          if (s >= 1 && !tc::mbar_wait(&bar_mma[(s + 1) & 1], ((s - 1) >> 1) & 1, kTcWaitNs))
+            fail = true;
+          else
+            issue_b(s + 1);
+        }
       }
     }
   }
@@ -288,12 +305,12 @@ dst_tc_kernel(const GemmTile *__restrict__ tiles, const int *__restrict__ active
       atomicOr(err, 1);
       // let this CTA's own bulk copies and MMAs finish before its shared
       // memory and TMEM are released: the last phase armed on each barrier
-      // (slabs issued-1 and issued-2; a commit covers all earlier MMAs)
-      for (int u = issued - 2; u < issued; ++u) {
-        if (u < 0) continue;
-        tc::mbar_wait(&bar_full[u & 1], (u >> 1) & 1, kTcWaitNs);
-        tc::mbar_wait(&bar_mma[u & 1], (u >> 1) & 1, kTcWaitNs);
-      }
+      // (copies of slabs bissued-1 and bissued-2, MMAs of slabs issued-1 and
+      // issued-2; a commit covers all earlier MMAs)
+      for (int u = bissued - 2; u < bissued; ++u)
+        if (u >= 0) tc::mbar_wait(&bar_full[u & 1], (u >> 1) & 1, kTcWaitNs);
+      for (int u = issued - 2; u < issued; ++u)
+        if (u >= 0) tc::mbar_wait(&bar_mma[u & 1], (u >> 1) & 1, kTcWaitNs);
     }
   }
   tc::fence_before_sync();
