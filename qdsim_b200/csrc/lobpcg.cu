@@ -1433,13 +1433,21 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
     if (usable) {
       for (int idx = tid; idx < m * m; idx += nt) sZ[idx] = sB[idx];
       __syncthreads();
+      // A direction of P whose pivot falls below the floor lies within
+      // sqrt(floor) of the span of the columns before it: it is dropped (its
+      // column takes no part in the elimination); a small pivot of X or W
+      // sends the basis to SVQB.
       bool ok = true;
+      int r = 0;   // kept columns, in order, in s_keep
       for (int k = 0; k < mu; ++k) {
         const double piv = sZ[k * m + k];   // final since the previous barrier
         if (!(piv > pivot_floor)) {         // every thread reads the same value
+          if (k >= 2 * B) continue;
           ok = false;
           break;
         }
+        if (tid == 0) s_keep[r] = k;
+        ++r;
         const double ip = 1.0 / piv;
         const int R = mu - k - 1;
         for (int idx = tid; idx < R * R; idx += nt) {
@@ -1449,34 +1457,36 @@ rr_kernel(DotState *st, const double *partial, const double *norms, double *thet
         __syncthreads();
       }
       if (ok) {
-        // L[k][k] = sqrt(piv_k), L[i][k] = sZ[i][k] / sqrt(piv_k); 1/L[k][k] in sE
-        if (tid < mu) sE[tid] = rsqrt(sZ[tid * m + tid]);
+        __syncthreads();   // s_keep complete
+        // L of the kept columns (r x r): L[c][c] = sqrt(piv), L[i][c] =
+        // Z[K_i][K_c] / sqrt(piv_c) into sT; 1/L[c][c] in sE
+        if (tid < r) sE[tid] = rsqrt(sZ[s_keep[tid] * m + s_keep[tid]]);
         __syncthreads();
-        for (int idx = tid; idx < mu * mu; idx += nt) {
-          const int i = idx / mu, k = idx % mu;
-          if (k < i) sZ[i * m + k] *= sE[k];
+        for (int idx = tid; idx < r * r; idx += nt) {
+          const int i = idx / r, c = idx % r;
+          if (c < i) sT[i * m + c] = sZ[s_keep[i] * m + s_keep[c]] * sE[c];
         }
         __syncthreads();
-        if (tid < mu) sZ[tid * m + tid] = 1.0 / sE[tid];
-        __syncthreads();
         // L^-1 (lower) into sB, one column per thread
-        if (tid < mu) {
+        if (tid < r) {
           const int j = tid;
           for (int i = 0; i < j; ++i) sB[i * m + j] = 0.0;
           sB[j * m + j] = sE[j];
-          for (int i = j + 1; i < mu; ++i) {
+          for (int i = j + 1; i < r; ++i) {
             double sum = 0.0;
-            for (int l = j; l < i; ++l) sum += sZ[i * m + l] * sB[l * m + j];
+            for (int l = j; l < i; ++l) sum += sT[i * m + l] * sB[l * m + j];
             sB[i * m + j] = -sum * sE[i];
           }
         }
         __syncthreads();
-        // Q = L^-T (rows >= mu are unused directions)
-        for (int idx = tid; idx < m * m; idx += nt) {
-          const int i = idx / m, c = idx % m;
-          sT[idx] = (i < mu && c < mu && c >= i) ? sB[c * m + i] : 0.0;
+        // Q = L^-T on the kept rows (m x r; dropped and unused rows zero)
+        for (int idx = tid; idx < m * m; idx += nt) sT[idx] = 0.0;
+        __syncthreads();
+        for (int idx = tid; idx < r * r; idx += nt) {
+          const int i = idx / r, c = idx % r;
+          if (c >= i) sT[s_keep[i] * m + c] = sB[c * m + i];
         }
-        if (tid == 0) s_r = mu;
+        if (tid == 0) s_r = r;
         __syncthreads();
         chol = true;
       } else {
@@ -1652,32 +1662,33 @@ update_kernel(const Chunk *chunks, const DotState *st, const double *coef, TV *X
   pipe.finish(ok, wait_err);
 }
 
-// M-orthogonalisation of W and P against X, in memory:
-//   C_W = X^T M W = (MX)^T W,  C_P = (MX)^T P   (X is M-orthonormal)
-//   W <- W - X C_W,  P <- P - X C_P,  HP <- HP - HX C_P,  MP <- MP - MX C_P.
+// M-orthogonalisation of W against X, in memory:
+//   C_W = X^T M W = (MX)^T W  (X is M-orthonormal),  W <- W - X C_W.
 // Near convergence the preconditioned residual is dominated by a component
 // along X and the useful correction is 1e-6..1e-8 of it; removed here by an
 // elementwise subtraction it stays accurate, whereas inside the small
 // Rayleigh-Ritz problem it would sit below the resolution of the Gram matrix
-// and the iteration stalls.
-template <typename TV, int B> using OgPipe = qd::BlockPipe<TV, B, 3, (sizeof(TV) == 8 ? 32 : 64), 4>;
+// and the iteration stalls.  P = [W P] Y_wp is built from directions already
+// M-orthogonal to the previous X, so its component along the new X is of the
+// order of |P|^2 and the Rayleigh-Ritz step resolves it.
+template <typename TV, int B> using OgPipe = qd::BlockPipe<TV, B, 2, (sizeof(TV) == 8 ? 32 : 64), 4>;
 template <int B> struct OgCfg {
   static constexpr int NQ = B / 4;
-  static constexpr int NT = 2 * NQ * NQ;     // 4x4 output blocks of MX^T W and MX^T P
+  static constexpr int NT = NQ * NQ;         // 4x4 output blocks of MX^T W
   static constexpr int RG = 256 / NT;        // row groups
   static constexpr size_t RED_BYTES = size_t(RG) * NT * 16 * sizeof(double);
 };
 
-// Per chunk: partial = [MX^T W, MX^T P] (B x B each, FP64).  Each thread owns
-// a 4x4 output block for one row group, accumulating in TV within a sub-tile
-// and in FP64 across sub-tiles; the row groups are summed in a fixed order.
+// Per chunk: partial = MX^T W (B x B, FP64).  Each thread owns a 4x4 output
+// block for one row group, accumulating in TV within a sub-tile and in FP64
+// across sub-tiles; the row groups are summed in a fixed order.
 template <typename TV, int B>
 __global__ void __launch_bounds__(256)
 ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const TV *W,
-                  const TV *P, double *partial, int *wait_err) {
+                  double *partial, int *wait_err) {
   using PP = OgPipe<TV, B>;
   using C = OgCfg<B>;
-  constexpr int NQ = C::NQ, NT = C::NT, RG = C::RG, NOUT = 2 * B * B;
+  constexpr int NQ = C::NQ, NT = C::NT, RG = C::RG, NOUT = B * B;
   extern __shared__ __align__(128) unsigned char dsm[];
   double *red = reinterpret_cast<double *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
@@ -1686,13 +1697,13 @@ ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const T
   const int tid = threadIdx.x;
   const bool worker = tid < NT * RG;
   const int task = tid % NT, rg = tid / NT;
-  const int which = task / (NQ * NQ), bi = (task % (NQ * NQ)) / NQ, bj = task % NQ;
+  const int bi = task / NQ, bj = task % NQ;
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  const TV *src[3] = {MX, W, P};
+  const TV *src[2] = {MX, W};
   PP pipe;
   pipe.init(dsm, src, ch.begin, ch.end);
   bool ok = true;
@@ -1700,7 +1711,7 @@ ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const T
     ok = pipe.wait(i) && ok;
     if (ok && worker) {
       const int nr = pipe.rows(i);
-      const TV *tm = pipe.tile(i, 0) + 4 * bi, *tr = pipe.tile(i, 1 + which) + 4 * bj;
+      const TV *tm = pipe.tile(i, 0) + 4 * bi, *tr = pipe.tile(i, 1) + 4 * bj;
       TV t[4][4];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
@@ -1732,57 +1743,49 @@ ortho_gram_kernel(const Chunk *chunks, const DotState *st, const TV *MX, const T
   __syncthreads();
   double *out = partial + size_t(blockIdx.x) * NOUT;
   for (int e = tid; e < NOUT; e += blockDim.x) {
-    const int w = e / (B * B), ij = e % (B * B), i = ij / B, j = ij % B;
-    const int tk = w * NQ * NQ + (i / 4) * NQ + (j / 4), ab = (i % 4) * 4 + (j % 4);
+    const int i = e / B, j = e % B;
+    const int tk = (i / 4) * NQ + (j / 4), ab = (i % 4) * 4 + (j % 4);
     double v = 0.0;
     for (int g = 0; g < RG; ++g) v += red[(size_t(g) * NT + tk) * 16 + ab];
     out[e] = v;
   }
 }
 
-// W <- W - X C_W;  with P: P <- P - X C_P, HP <- HP - HX C_P, MP <- MP - MX C_P.
-template <typename TV, int B> using OaPipe = qd::BlockPipe<TV, B, 7, (sizeof(TV) == 8 ? 16 : 32), 4>;
+// W <- W - X C_W.
+template <typename TV, int B> using OaPipe = qd::BlockPipe<TV, B, 2, (sizeof(TV) == 8 ? 32 : 64), 4>;
 
 template <typename TV, int B>
 __global__ void __launch_bounds__(256)
 ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, const TV *X,
-                   const TV *HX, const TV *MX, TV *W, TV *P, TV *HP, TV *MP, int *wait_err) {
+                   TV *W, int *wait_err) {
   using PP = OaPipe<TV, B>;
-  constexpr int NOUT = 2 * B * B;
+  constexpr int NOUT = B * B;
   extern __shared__ __align__(128) unsigned char dsm[];
   TV *sC = reinterpret_cast<TV *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
   if (!sd.run[sizeof(TV) == 8]) return;
-  const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
   for (int e = tid; e < NOUT; e += blockDim.x) sC[e] = TV(csum[size_t(ch.dot) * NOUT + e]);
-  const TV *src[7] = {X, HX, MX, W, P, HP, MP};
+  const TV *src[2] = {X, W};
   PP pipe;
   pipe.init(dsm, src, ch.begin, ch.end);   // its barrier also publishes sC
   // Elements step by a multiple of B, so each thread keeps one column j and
-  // holds that column of C_W and C_P in registers (threads past the multiple
-  // idle).
+  // holds that column of C_W in registers (threads past the multiple idle).
   const int nthr = (int(blockDim.x) / B) * B;
   const int j = tid % B;
   const bool owner = tid < nthr;
-  TV cw[B], cp[B];
+  TV cw[B];
 #pragma unroll
-  for (int q = 0; q < B; ++q) {
-    cw[q] = sC[q * B + j];
-    cp[q] = sC[B * B + q * B + j];
-  }
+  for (int q = 0; q < B; ++q) cw[q] = sC[q * B + j];
   bool ok = true;
   for (int i = 0; i < pipe.nsub; ++i) {
     ok = pipe.wait(i) && ok;
     if (ok && owner) {
       const int nr = pipe.rows(i), r0 = pipe.row0(i);
-      const TV *tx = pipe.tile(i, 0), *thx = pipe.tile(i, 1), *tmx = pipe.tile(i, 2);
-      const TV *tw = pipe.tile(i, 3), *tp = pipe.tile(i, 4), *thp = pipe.tile(i, 5),
-               *tmp = pipe.tile(i, 6);
+      const TV *tx = pipe.tile(i, 0), *tw = pipe.tile(i, 1);
       for (int e = tid; e < nr * B; e += nthr) {
         const int row = e / B;
-        const size_t o = size_t(r0) * B + e;
         TV dw = 0;
 #pragma unroll
         for (int q4 = 0; q4 < B; q4 += 4) {
@@ -1791,27 +1794,7 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
 #pragma unroll
           for (int u = 0; u < 4; ++u) dw = fma(t[u], cw[q4 + u], dw);
         }
-        W[o] = tw[e] - dw;
-        if (with_p) {
-          TV dp = 0, dhp = 0, dmp = 0;
-#pragma unroll
-          for (int q4 = 0; q4 < B; q4 += 4) {
-            TV t0[4], t1[4], t2[4];
-            lds4(tx + row * B + q4, t0);
-            lds4(thx + row * B + q4, t1);
-            lds4(tmx + row * B + q4, t2);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const TV c = cp[q4 + u];
-              dp = fma(t0[u], c, dp);
-              dhp = fma(t1[u], c, dhp);
-              dmp = fma(t2[u], c, dmp);
-            }
-          }
-          P[o] = tp[e] - dp;
-          HP[o] = thp[e] - dhp;
-          MP[o] = tmp[e] - dmp;
-        }
+        W[size_t(r0) * B + e] = tw[e] - dw;
       }
     }
     pipe.release(i, ok);
@@ -1829,15 +1812,15 @@ ortho_apply_kernel(const Chunk *chunks, const DotState *st, const double *csum, 
 // ---------------------------------------------------------------------------
 
 // Per chunk: partial = [MX^T W, MX^T P] (B x B each) with FP64 MX and FP32 W, P.
-template <int B> using OgMxPipe = qd::MixedPipe<double, 1, float, 2, B, 32, 4>;
+template <int B> using OgMxPipe = qd::MixedPipe<double, 1, float, 1, B, 32, 4>;
 
 template <int B>
 __global__ void __launch_bounds__(256)
 ortho_gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *MX, const float *W,
-                     const float *P, double *partial, int *wait_err) {
+                     double *partial, int *wait_err) {
   using PP = OgMxPipe<B>;
   using C = OgCfg<B>;
-  constexpr int NQ = C::NQ, NT = C::NT, RG = C::RG, NOUT = 2 * B * B;
+  constexpr int NQ = C::NQ, NT = C::NT, RG = C::RG, NOUT = B * B;
   extern __shared__ __align__(128) unsigned char dsm[];
   double *red = reinterpret_cast<double *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
@@ -1845,13 +1828,13 @@ ortho_gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *MX, 
   const int tid = threadIdx.x;
   const bool worker = tid < NT * RG;
   const int task = tid % NT, rg = tid / NT;
-  const int which = task / (NQ * NQ), bi = (task % (NQ * NQ)) / NQ, bj = task % NQ;
+  const int bi = task / NQ, bj = task % NQ;
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  const void *src[3] = {MX, W, P};
+  const void *src[2] = {MX, W};
   PP pipe;
   pipe.init(dsm, src, ch.begin, ch.end);
   bool ok = true;
@@ -1860,7 +1843,7 @@ ortho_gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *MX, 
     if (ok && worker) {
       const int nr = pipe.rows(i);
       const double *tm = pipe.tx(i, 0) + 4 * bi;
-      const float *tr = pipe.tw(i, which) + 4 * bj;
+      const float *tr = pipe.tw(i, 0) + 4 * bj;
       for (int row = rg; row < nr; row += RG) {
         double x[4];
         float y[4];
@@ -1884,57 +1867,50 @@ ortho_gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *MX, 
   __syncthreads();
   double *out = partial + size_t(blockIdx.x) * NOUT;
   for (int e = tid; e < NOUT; e += blockDim.x) {
-    const int w = e / (B * B), ij = e % (B * B), i = ij / B, j = ij % B;
-    const int tk = w * NQ * NQ + (i / 4) * NQ + (j / 4), ab = (i % 4) * 4 + (j % 4);
+    const int i = e / B, j = e % B;
+    const int tk = (i / 4) * NQ + (j / 4), ab = (i % 4) * 4 + (j % 4);
     double v = 0.0;
     for (int g = 0; g < RG; ++g) v += red[(size_t(g) * NT + tk) * 16 + ab];
     out[e] = v;
   }
 }
 
-// W <- W - X C_W; with P: P <- P - X C_P, HP <- HP - HX C_P, MP <- MP - MX C_P,
-// FP64 arithmetic on the exact FP32 inputs, each result rounded once to FP32
-// (relative to itself: the cancellation happens before the rounding).
-template <int B> using OaMxPipe = qd::MixedPipe<double, 3, float, 4, B, 16, 4>;
+// W <- W - X C_W, FP64 arithmetic on the exact FP32 inputs, the result
+// rounded once to FP32 (relative to itself: the cancellation happens before
+// the rounding).
+template <int B> using OaMxPipe = qd::MixedPipe<double, 1, float, 1, B, 32, 4>;
 
 template <int B>
 __global__ void __launch_bounds__(256)
 ortho_apply_mx_kernel(const Chunk *chunks, const DotState *st, const double *csum,
-                      const double *X, const double *HX, const double *MX, float *W, float *P,
-                      float *HP, float *MP, int *wait_err) {
+                      const double *X, float *W, int *wait_err) {
   using PP = OaMxPipe<B>;
-  constexpr int NOUT = 2 * B * B;
+  constexpr int NOUT = B * B;
   extern __shared__ __align__(128) unsigned char dsm[];
   double *sC = reinterpret_cast<double *>(dsm + PP::BYTES);
   const Chunk ch = chunks[blockIdx.x];
   const DotState &sd = st[ch.dot];
   if (!sd.run[1]) return;
-  const bool with_p = sd.has_p != 0;
   const int tid = threadIdx.x;
   for (int e = tid; e < NOUT; e += blockDim.x) sC[e] = csum[size_t(ch.dot) * NOUT + e];
-  const void *src[7] = {X, HX, MX, W, P, HP, MP};
+  const void *src[2] = {X, W};
   PP pipe;
   pipe.init(dsm, src, ch.begin, ch.end);   // its barrier also publishes sC
   const int nthr = (int(blockDim.x) / B) * B;
   const int j = tid % B;
   const bool owner = tid < nthr;
-  double cw[B], cp[B];
+  double cw[B];
 #pragma unroll
-  for (int q = 0; q < B; ++q) {
-    cw[q] = sC[q * B + j];
-    cp[q] = sC[B * B + q * B + j];
-  }
+  for (int q = 0; q < B; ++q) cw[q] = sC[q * B + j];
   bool ok = true;
   for (int i = 0; i < pipe.nsub; ++i) {
     ok = pipe.wait(i) && ok;
     if (ok && owner) {
       const int nr = pipe.rows(i), r0 = pipe.row0(i);
-      const double *tx = pipe.tx(i, 0), *thx = pipe.tx(i, 1), *tmx = pipe.tx(i, 2);
-      const float *tw = pipe.tw(i, 0), *tp = pipe.tw(i, 1), *thp = pipe.tw(i, 2),
-                  *tmp = pipe.tw(i, 3);
+      const double *tx = pipe.tx(i, 0);
+      const float *tw = pipe.tw(i, 0);
       for (int e = tid; e < nr * B; e += nthr) {
         const int row = e / B;
-        const size_t o = size_t(r0) * B + e;
         double dw = 0.0;
 #pragma unroll
         for (int q4 = 0; q4 < B; q4 += 4) {
@@ -1943,27 +1919,7 @@ ortho_apply_mx_kernel(const Chunk *chunks, const DotState *st, const double *csu
 #pragma unroll
           for (int u = 0; u < 4; ++u) dw = fma(t[u], cw[q4 + u], dw);
         }
-        W[o] = float(double(tw[e]) - dw);
-        if (with_p) {
-          double dp = 0.0, dhp = 0.0, dmp = 0.0;
-#pragma unroll
-          for (int q4 = 0; q4 < B; q4 += 4) {
-            double t0[4], t1[4], t2[4];
-            lds4(tx + row * B + q4, t0);
-            lds4(thx + row * B + q4, t1);
-            lds4(tmx + row * B + q4, t2);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const double c = cp[q4 + u];
-              dp = fma(t0[u], c, dp);
-              dhp = fma(t1[u], c, dhp);
-              dmp = fma(t2[u], c, dmp);
-            }
-          }
-          P[o] = float(double(tp[e]) - dp);
-          HP[o] = float(double(thp[e]) - dhp);
-          MP[o] = float(double(tmp[e]) - dmp);
-        }
+        W[size_t(r0) * B + e] = float(double(tw[e]) - dw);
       }
     }
     pipe.release(i, ok);
@@ -2524,18 +2480,18 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   {
     constexpr size_t bytes = OgPipe<TV, B>::BYTES + OgCfg<B>::RED_BYTES;
     if (smem_attr<ortho_gram_kernel<TV, B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
-    ortho_gram_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, b.MX, b.W, b.P,
+    ortho_gram_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, b.MX, b.W,
                                                            L.partial, L.wait_err);
   }
   QD_CHECK_LAUNCH();
-  dot_reduce_kernel<<<dim3((2 * B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, PH, L.partial,
-                                                                         2 * B * B, L.dotsum);
+  dot_reduce_kernel<<<dim3((B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, PH, L.partial,
+                                                                     B * B, L.dotsum);
   QD_CHECK_LAUNCH();
   {
-    constexpr size_t bytes = OaPipe<TV, B>::BYTES + 2 * B * B * sizeof(TV);
+    constexpr size_t bytes = OaPipe<TV, B>::BYTES + B * B * sizeof(TV);
     if (smem_attr<ortho_apply_kernel<TV, B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
-    ortho_apply_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(
-        L.chunks, L.st, L.dotsum, b.X, b.HX, b.MX, b.W, b.P, b.HP, b.MP, L.wait_err);
+    ortho_apply_kernel<TV, B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, L.dotsum, b.X,
+                                                            b.W, L.wait_err);
   }
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
@@ -2608,19 +2564,18 @@ int phase_sequence_mx(const Layout &L, const Bufs<float> &b, const Bufs<double> 
   {
     constexpr size_t bytes = OgMxPipe<B>::BYTES + OgCfg<B>::RED_BYTES;
     if (smem_attr<ortho_gram_mx_kernel<B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
-    ortho_gram_mx_kernel<B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, x64.MX, b.W, b.P,
+    ortho_gram_mx_kernel<B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, x64.MX, b.W,
                                                           L.partial, L.wait_err);
   }
   QD_CHECK_LAUNCH();
-  dot_reduce_kernel<<<dim3((2 * B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, 1, L.partial,
-                                                                         2 * B * B, L.dotsum);
+  dot_reduce_kernel<<<dim3((B * B + 255) / 256, n_dots), 256, 0, s>>>(L.st, 1, L.partial,
+                                                                     B * B, L.dotsum);
   QD_CHECK_LAUNCH();
   {
-    constexpr size_t bytes = OaMxPipe<B>::BYTES + 2 * B * B * sizeof(double);
+    constexpr size_t bytes = OaMxPipe<B>::BYTES + B * B * sizeof(double);
     if (smem_attr<ortho_apply_mx_kernel<B>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
     ortho_apply_mx_kernel<B><<<L.nchunks, 256, bytes, s>>>(L.chunks, L.st, L.dotsum, x64.X,
-                                                           x64.HX, x64.MX, b.W, b.P, b.HP,
-                                                           b.MP, L.wait_err);
+                                                           b.W, L.wait_err);
   }
   qd::prof_end(qd::PK_ORTHO, s);
   QD_CHECK_LAUNCH();
