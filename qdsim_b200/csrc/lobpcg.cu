@@ -1943,7 +1943,7 @@ gram_mx_kernel(const Chunk *chunks, const DotState *st, const double *X, const f
                int *wait_err) {
   using C = GramCfg<double, B>;
   using PP = GramMxPipe<B>;
-  constexpr int m = C::m, NB = C::NB, NT = C::NT, NT2 = C::NT2, RG = C::RG;
+  constexpr int m = C::m, NT = C::NT, NT2 = C::NT2, RG = C::RG;
   extern __shared__ __align__(128) unsigned char dsm[];
   const Chunk ch = chunks[blockIdx.x];
   if (!st[ch.dot].run[1]) return;
