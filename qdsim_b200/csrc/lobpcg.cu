@@ -222,7 +222,12 @@ spmm_xp_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   double *my_red = s_red + threadIdx.x;
 #pragma unroll
   for (int c = 0; c < 8; ++c) my_red[c * NTX] = 0.0;
-  for (int r = ch.begin + sub; r < ch.end; r += RPP) {
+  // rows in sub-tiles of RPP, each taken in two halves of one parity (even
+  // offsets, then odd): on the row-major lattice of a P2 mesh rows two apart
+  // share their stencil, so the rows of one warp have the same number of
+  // nonzeros and neighbouring columns
+  const int ofs = sub < RPP / 2 ? 2 * sub : 2 * (sub - RPP / 2) + 1;
+  for (int r = ch.begin + ofs; r < ch.end; r += RPP) {
     if (!isx && !with_p) {
       double z[4] = {0, 0, 0, 0};
       qd::V4<TP>::store(HP + size_t(r) * B + 4 * g, z);
