@@ -17,11 +17,14 @@
 //   spmm_xp: explicit HX, MX, HP, MP (FP64 accumulation), residual
 //            W = HX - MX Theta and its per-column norms
 //   precond: W = T W (DST preconditioner, when the dot has a lattice)
+//   ortho  : W = W - X (MX)^T W (M-orthogonal to X)
 //   spmm   : HW = H W, MW = M W
 //   gram   : per chunk, A_c = S^T HS and B_c = S^T MS (3B x 3B)
 //   rr     : per dot (one CTA): convergence test, A = sum_c A_c, B = sum_c B_c,
-//            SVQB orthonormalisation of the basis and a cyclic Jacobi
-//            eigensolve, Ritz coefficients Y -- all FP64 in shared memory
+//            orthonormal basis (Cholesky dropping dependent P directions, or
+//            SVQB), the B lowest Ritz pairs (tridiagonalisation, bisection,
+//            inverse iteration), Ritz coefficients Y -- all FP64 in shared
+//            memory
 //   update : X = S Y, P = [W P] Y_wp
 // Recomputing the products of X and P every iteration (instead of updating
 // them with the Ritz coefficients) keeps the residual consistent with X even
