@@ -126,3 +126,18 @@ def test_sweep_pipeline_steps_match_batch(cuda):
     for s in range(steps):
         assert np.array_equal(outE[s].numpy(), E_ref), s
         assert np.array_equal(outX[s].numpy(), X_ref), s
+
+
+def test_p3_mixed_staged_and_gathered_subtiles(cuda):
+    """P3 dot (30 x 15 cells, 3,916 DOFs) in mixed precision.  Its stencil spans
+    seven lattice lines, so about half of the FP32 SpMM's sub-tiles (64 rows for
+    X and P, 128 rows for W) exceed the staged runs and read their operands
+    from global memory while the others are staged in shared memory; the
+    eigenvalues of both paths together against the oracle."""
+    om, c, V = O.dot_config_sweep(3, order=3, nx=30)
+    ref = O.assemble(om, c, V)
+    E0 = O.eig_lowest(ref.H, ref.M, 8, O.sigma_below(V))[0]
+    prob, res = _solve_single(cuda, om, c, V, 8, "mixed", b=12)
+    assert res.status == 0, res.info
+    rel = np.abs(res.E[0] - E0) / np.abs(E0)
+    assert rel.max() <= 1e-9, (rel, res.info)
