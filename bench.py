@@ -606,13 +606,13 @@ def algorithmic_bytes(hb, counts, k_block, mixed=True):
       FP32 phase (vectors 4 bytes, matrix values an 8-byte FP32 (H, M) pair,
       column indices as 2-byte staged positions):
         spmm   2 (z (2 + 8) + 4 n) + 3 n B 4 gathered + 7 n B 4 written
-        gram   9 n B 4 read;  dst (2 4 + 12) n B;  ortho 14 n B 4;  update 5 n B 4
+        gram   9 n B 4 read;  dst (2 4 + 12) n B;  ortho 5 n B 4;  update 5 n B 4
       FP64 phase of the plain form (vectors 8, values 16): the same with 8 / 16
       finishing phase of the mixed form (X, HX, MX FP64; W, P and their
       products FP32; X's products from the FP64 values, W's from the pairs):
         spmm   z (4 + 16) + z (2 + 8) + 8 n + n B (8 + 4 + 2 8 + 3 4 + 4 + 2 4)
         gram   n B (3 8 + 6 4);  dst (2 4 + 12) n B
-        ortho  n B (8 + 2 4) + n B (3 8 + 4 4 + 4 4);  update n B (8 + 2 4 + 8 + 4)
+        ortho  n B (8 + 4) + n B (8 + 4 + 4);  update n B (8 + 2 4 + 8 + 4)
     """
     z = np.asarray(hb.nnz_per_dot, dtype=np.float64)
     n = np.asarray(hb.rows_per_dot, dtype=np.float64)
@@ -630,13 +630,13 @@ def algorithmic_bytes(hb, counts, k_block, mixed=True):
         if ph == 1 and mixed:
             add({"spmm": it * (30 * z + 8 * n + 52 * n * B),
                  "gram": gr * 48 * n * B, "dst_precond": gr * 20 * n * B,
-                 "ortho": gr * 72 * n * B, "update": up * 28 * n * B})
+                 "ortho": gr * 28 * n * B, "update": up * 28 * n * B})
             continue
         s, v = (4.0, 8.0) if ph == 0 else (8.0, 16.0)
         csr = 2 * z * ((2 if ph == 0 else 4) + v)
         add({"spmm": it * (csr + 8 * n + 3 * n * B * s + 7 * n * B * s),
              "gram": gr * 9 * n * B * s, "dst_precond": gr * n * B * (2 * s + 12),
-             "ortho": gr * 14 * n * B * s, "update": up * 5 * n * B * s})
+             "ortho": gr * 5 * n * B * s, "update": up * 5 * n * B * s})
     return out
 
 
