@@ -186,7 +186,16 @@ typedef struct {
  *                (levels near zero energy); <= 0: purely relative
  *   chunk_rows   rows per chunk, the CTA unit of every row-parallel kernel
  *                (SpMM, Gram, orthogonalisation, update) and of the per-chunk
- *                partial sums; a multiple of 64 in [256, 8192], else 1024 */
+ *                partial sums; a multiple of 64 in [256, 8192], else 1024
+ *   setup_cached nonzero: the caller asserts that d_work, d_rowptr and d_col
+ *                (and their contents) are those of the previous call with
+ *                this workspace and that nothing else used the workspace
+ *                since; the call then reads no value back during its set-up
+ *                and does not copy host tables identical to that call's
+ *                (repeated solves of one batch shape, e.g. a sweep pipeline
+ *                whose own large copies would hold small ones back).  The
+ *                library checks the batch shape, pointers and tables and
+ *                falls back to the full set-up when any differs. */
 typedef struct {
   double tol32;
   int32_t stag_window;
@@ -194,7 +203,7 @@ typedef struct {
   const double *x0;
   double eig_scale;
   int32_t chunk_rows;
-  int32_t reserved;
+  int32_t setup_cached;
 } qd_lobpcg_opts;
 
 int qd_lobpcg_workspace_size(int32_t n_dots, int64_t n_rows_total, int64_t nnz_total, int b,

@@ -94,7 +94,7 @@ assert DST_PREC_DTYPE.itemsize == 40
 LOBPCG_OPTS_DTYPE = _np.dtype([("tol32", _np.float64), ("stag_window", _np.int32),
                                ("graphs", _np.int32), ("x0", _np.uint64),
                                ("eig_scale", _np.float64), ("chunk_rows", _np.int32),
-                               ("reserved", _np.int32)], align=True)
+                               ("setup_cached", _np.int32)], align=True)
 assert LOBPCG_OPTS_DTYPE.itemsize == 40
 
 # struct qd_cap_info (include/qdsim_b200.h)

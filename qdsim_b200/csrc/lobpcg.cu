@@ -162,10 +162,24 @@ __global__ void hm_exponent_kernel(int32_t nnz, const double *__restrict__ H,
   }
 }
 
-// FP32 (H 2^-eh, M 2^-em) pairs of the FP32 phase's SpMMs.
+// The binary exponents of the FP32 pairs' scales (INT_MIN, from an all-zero
+// matrix, counts as 0).
+__device__ inline int hm_scale_exp(const int *e2, int i) {
+  const int e = e2[i];
+  return e == INT_MIN ? 0 : e;
+}
+
+// e2 = {INT_MIN, INT_MIN} before hm_exponent_kernel's maxima.
+__global__ void hm_exponent_init_kernel(int *e2) {
+  if (threadIdx.x < 2) e2[threadIdx.x] = INT_MIN;
+}
+
+// FP32 (H 2^-eh, M 2^-em) pairs of the FP32 phase's SpMMs, with the exponents
+// read from the device (the host never waits for them).
 __global__ void pack_hm32_kernel(int32_t nnz, const double *__restrict__ H,
-                                 const double *__restrict__ M, int eh, int em,
+                                 const double *__restrict__ M, const int *__restrict__ e2,
                                  float2 *__restrict__ hm) {
+  const int eh = hm_scale_exp(e2, 0), em = hm_scale_exp(e2, 1);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x)
     hm[p] = make_float2(float(scalbn(H[p], -eh)), float(scalbn(M[p], -em)));
 }
@@ -468,7 +482,7 @@ __global__ void __launch_bounds__(32 * B, B <= 12 ? 2 : 1)
 spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restrict__ rowptr,
                const int32_t *__restrict__ col32, const uint16_t *__restrict__ pos16,
                const SubPlan *__restrict__ plan, int spc, const float2 *__restrict__ hm32,
-               const float *__restrict__ rs32, double sh, double smv,
+               const float *__restrict__ rs32, const int *__restrict__ hm_e,
                const double *__restrict__ theta, const float *__restrict__ X,
                const float *__restrict__ P, float *__restrict__ HX, float *__restrict__ MX,
                float *__restrict__ HP, float *__restrict__ MP, float *__restrict__ W,
@@ -503,6 +517,8 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
   const int sub = tid / G2, gg = tid % G2;
   const bool isx = gg < G;
   const int g = isx ? gg : gg - G;
+  // scales 2^e of the FP32 (H, M) pairs
+  const float fsh = ldexpf(1.f, hm_scale_exp(hm_e, 0)), fsm = ldexpf(1.f, hm_scale_exp(hm_e, 1));
   // FP64 sums of squares of this thread's rows (problems posed in SI units
   // have squared residuals far below FP32's range): r^2, (Mx)^2 per column
   double red[8];
@@ -635,7 +651,6 @@ spmm32s_kernel(const Chunk *chunks, const DotState *st, const int32_t *__restric
         h[3] = fmaf(rs, xi.w, h[3]);
         const size_t o = size_t(r) * B + 4 * g;
         // back to the matrices' own scale (powers of two: exact)
-        const float fsh = float(sh), fsm = float(smv);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           h[c] *= fsh;
@@ -2333,8 +2348,7 @@ struct Layout {
   SubPlan *planw;
   int spcw;
   float *rs32;           // row sums of the FP32 H values, summed in FP64 (mixed only)
-  int *hm_exp;           // largest binary exponents of |H| and |M|
-  double hm_sh, hm_sm;   // 2^exponent: scale of the FP32 pairs
+  int *hm_exp;           // largest binary exponents of |H| and |M| (scales 2^e of the pairs)
 };
 
 size_t rr_smem_bytes(int B) {
@@ -2373,7 +2387,6 @@ int carve(qd::Arena &ar, int n_dots, int64_t n_rows, int64_t nnz, int B, int nch
   L.pos16w = mixed ? ar.take<uint16_t>(size_t(nnz) + 16) : nullptr;
   L.planw = mixed ? ar.take<SubPlan>(size_t(nchunks) * L.spcw) : nullptr;
   L.hm_exp = ar.take<int>(2);
-  L.hm_sh = L.hm_sm = 1.0;
   L.dinv = jacobi ? ar.take<double>(size_t(n_rows)) : nullptr;
   L.njac = 0;
   L.nchunks = nchunks;
@@ -2412,18 +2425,6 @@ int count_chunks(int n_dots, const int32_t *row_off, int chunk_rows) {
   return int(c);
 }
 
-// Matrix values seen by the SpMMs of a phase: interleaved FP32 (H, M) pairs
-// while the vectors are FP32, the caller's FP64 arrays in the FP64 phase.
-template <typename TV> struct MatFor;
-template <> struct MatFor<double> {
-  static qd::MatF64 make(const Layout &, const double *H, const double *M) { return {H, M}; }
-};
-template <> struct MatFor<float> {
-  static qd::MatF32 make(const Layout &L, const double *, const double *) {
-    return {L.hm32, L.hm_sh, L.hm_sm};
-  }
-};
-
 template <typename TV>
 struct Bufs {
   TV *X, *W, *P, *HX, *HW, *HP, *MX, *MW, *MP;
@@ -2441,8 +2442,8 @@ int spmm32_w(const Layout &L, const int32_t *rowptr, const float *W, float *HW, 
   constexpr size_t bytes = SpmmStage<B, 1, 128>::BYTES;
   if (smem_attr<spmm32s_kernel<B, false>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
   spmm32s_kernel<B, false><<<L.nchunks, 32 * B, bytes, s>>>(
-      L.chunks, L.st, rowptr, L.col32, L.pos16w, L.planw, L.spcw, L.hm32, L.rs32, L.hm_sh,
-      L.hm_sm, L.theta, W, nullptr, HW, MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, ph);
+      L.chunks, L.st, rowptr, L.col32, L.pos16w, L.planw, L.spcw, L.hm32, L.rs32, L.hm_exp,
+      L.theta, W, nullptr, HW, MW, nullptr, nullptr, nullptr, nullptr, L.wait_err, ph);
   return QD_OK;
 }
 
@@ -2455,13 +2456,13 @@ int phase_sequence(const Layout &L, const Bufs<TV> &b, int n_dots, const int32_t
   constexpr int PH = sizeof(TV) == 8 ? 1 : 0;
   using GC = GramCfg<TV, B>;
   qd::prof_begin(qd::PK_SPMM, s);
-  const auto A = MatFor<TV>::make(L, H, M);
+  const qd::MatF64 A{H, M};   // the FP64 form's values (the FP32 form stages its pairs)
   if constexpr (sizeof(TV) == 4) {
     constexpr size_t bytes = SpmmStage<B, 2, 64>::BYTES;
     if (smem_attr<spmm32s_kernel<B, true>>(bytes) != cudaSuccess) return QD_ERR_CUDA;
     spmm32s_kernel<B, true><<<L.nchunks, 32 * B, bytes, s>>>(
-        L.chunks, L.st, rowptr, L.col32, L.pos16, L.plan, L.spc, L.hm32, L.rs32, L.hm_sh,
-        L.hm_sm, L.theta, b.X, b.P, b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err, 0);
+        L.chunks, L.st, rowptr, L.col32, L.pos16, L.plan, L.spc, L.hm32, L.rs32, L.hm_exp,
+        L.theta, b.X, b.P, b.HX, b.MX, b.HP, b.MP, b.W, L.norms, L.wait_err, 0);
   } else {
     spmm_xp_kernel<TV, TV, B><<<L.nchunks, 128 * G, 0, s>>>(L.chunks, L.st, rowptr, col, A,
                                                             L.theta, b.X, b.P, b.HX, b.MX,
@@ -2777,6 +2778,71 @@ int run_solver(const Layout &L, bool mixed, int n_dots, const int32_t *rowptr, c
   return QD_OK;
 }
 
+// Host-side record of the last set-up made in a workspace (at most
+// kSetupCaches workspaces, most recent first): the tables copied to it and
+// the count of nonzeros.  Read and written under g_setup_mutex.
+struct SetupCache {
+  const void *work = nullptr;
+  size_t work_bytes = 0;
+  const int32_t *rowptr = nullptr, *col = nullptr;
+  int B = 0, prec = 0, chunk_rows = 0, jacobi = 0;
+  int64_t ntx = 0, nty = 0;
+  int32_t nnz = 0;
+  std::vector<int32_t> row_off;
+  std::vector<Chunk> chunks;
+  std::vector<qd::GemmTile> tiles_x, tiles_y;
+  std::vector<qd_dst_prec> desc;
+};
+constexpr int kSetupCaches = 8;
+std::mutex g_setup_mutex;
+std::vector<SetupCache> g_setup_caches;
+
+SetupCache &setup_cache_for(const void *work) {
+  for (size_t i = 0; i < g_setup_caches.size(); ++i)
+    if (g_setup_caches[i].work == work) {
+      if (i) std::swap(g_setup_caches[0], g_setup_caches[i]);
+      return g_setup_caches[0];
+    }
+  if (int(g_setup_caches.size()) >= kSetupCaches) g_setup_caches.pop_back();
+  g_setup_caches.insert(g_setup_caches.begin(), SetupCache{});
+  return g_setup_caches[0];
+}
+
+template <typename T>
+bool pod_equal(const std::vector<T> &a, const std::vector<T> &b) {
+  return a.size() == b.size() && (a.empty() || std::memcmp(a.data(), b.data(), a.size() * sizeof(T)) == 0);
+}
+
+// Per-dot state at the start of a solve.  reset: rebuilt here from the chunk
+// range the state already holds (the previous solve's, same chunk table);
+// otherwise the host's copy is kept.  Theta, the residual norms and the wait
+// flag are zeroed either way.
+__global__ void state_reset_kernel(DotState *st, int n_dots, int reset, int phase0, int B,
+                                   double *theta, double *relres, int *wait_err) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d == 0) *wait_err = 0;
+  if (d >= n_dots) return;
+  if (reset) {
+    DotState y{};
+    y.chunk0 = st[d].chunk0;
+    y.chunk1 = st[d].chunk1;
+    y.active = 1;
+    y.phase = phase0;
+    y.run[phase0] = 1;
+    y.best = 1e300;
+    if (y.chunk1 == y.chunk0) {
+      y.active = 0;
+      y.run[0] = y.run[1] = 0;
+      y.status = 2;
+    }
+    st[d] = y;
+  }
+  for (int j = 0; j < B; ++j) {
+    theta[size_t(d) * B + j] = 0.0;
+    relres[size_t(d) * B + j] = 0.0;
+  }
+}
+
 template <int B>
 int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
             const int32_t *d_col, const double *d_H, const double *d_M,
@@ -2800,9 +2866,31 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     }
     qd::dst_tiles(n_dots, h_prec, B, nullptr, &ntx, nullptr, &nty);
   }
+  // With opts->setup_cached the caller asserts that the workspace and the
+  // CSR pattern are untouched since the previous call with this workspace: the
+  // count of nonzeros is then not read back, and tables byte-identical to
+  // that call's are not copied again (a host->device copy queued behind the
+  // caller's own large copies would hold the set-up back).
+  SetupCache cache;   // the previous set-up in this workspace (a copy)
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    cache = setup_cache_for(d_work);
+  }
+  const bool cached = opts && opts->setup_cached && cache.work == d_work &&
+                      cache.work_bytes == work_bytes && cache.rowptr == d_rowptr &&
+                      cache.col == d_col && cache.B == B && cache.prec == prec_mode &&
+                      cache.chunk_rows == chunk_rows &&
+                      cache.jacobi == int(needs_jacobi(n_dots, h_prec)) && cache.ntx == ntx &&
+                      cache.nty == nty && cache.row_off.size() == size_t(n_dots) + 1 &&
+                      std::equal(cache.row_off.begin(), cache.row_off.end(), h_row_off);
   int32_t nnz = 0;   // the CSR's own count of nonzeros
-  QD_CUDA_TRY(cudaMemcpyAsync(&nnz, d_rowptr + n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  QD_CUDA_TRY(cudaStreamSynchronize(s));
+  if (cached) {
+    nnz = cache.nnz;
+  } else {
+    QD_CUDA_TRY(cudaMemcpyAsync(&nnz, d_rowptr + n_rows, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, s));
+    QD_CUDA_TRY(cudaStreamSynchronize(s));
+  }
   if (nnz <= 0) return QD_ERR_INVALID;
   const bool mixed_mode = prec_mode == QD_PREC_MIXED;
   const bool jacobi = needs_jacobi(n_dots, h_prec);
@@ -2817,37 +2905,40 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
   Layout L;
   carve(ar, n_dots, n_rows, nnz, B, nchunks, chunk_rows, ntx, nty, mixed_mode, jacobi, L);
   if (mixed_mode) {
-    const int init[2] = {INT_MIN, INT_MIN};
-    int e2[2];
-    QD_CUDA_TRY(cudaMemcpyAsync(L.hm_exp, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    // FP32 (H, M) pairs scaled by 2^-e, the exponents kept on the device
+    hm_exponent_init_kernel<<<1, 32, 0, s>>>(L.hm_exp);
+    QD_CHECK_LAUNCH();
     hm_exponent_kernel<<<1184, 256, 0, s>>>(nnz, d_H, d_M, L.hm_exp);
     QD_CHECK_LAUNCH();
-    QD_CUDA_TRY(cudaMemcpyAsync(e2, L.hm_exp, sizeof(e2), cudaMemcpyDeviceToHost, s));
-    QD_CUDA_TRY(cudaStreamSynchronize(s));
-    for (int i = 0; i < 2; ++i)
-      if (e2[i] == INT_MIN) e2[i] = 0;   // all-zero matrix
-    L.hm_sh = std::ldexp(1.0, e2[0]);
-    L.hm_sm = std::ldexp(1.0, e2[1]);
-    pack_hm32_kernel<<<1184, 256, 0, s>>>(nnz, d_H, d_M, e2[0], e2[1], L.hm32);
+    pack_hm32_kernel<<<1184, 256, 0, s>>>(nnz, d_H, d_M, L.hm_exp, L.hm32);
     QD_CHECK_LAUNCH();
-    QD_CUDA_TRY(cudaMemcpyAsync(L.col32, d_col, size_t(nnz) * sizeof(int32_t),
-                                cudaMemcpyDeviceToDevice, s));
+    if (!cached)   // the pattern's column indices, with bulk-copy slack
+      QD_CUDA_TRY(cudaMemcpyAsync(L.col32, d_col, size_t(nnz) * sizeof(int32_t),
+                                  cudaMemcpyDeviceToDevice, s));
     rowsum32_kernel<<<1184, 256, 0, s>>>(n_rows, d_rowptr, L.hm32, L.rs32);
     QD_CHECK_LAUNCH();
   }
   std::vector<qd::GemmTile> htx, hty;
+  bool same_tiles = cached;
   if (ntx > 0) {
     if (reinterpret_cast<uintptr_t>(d_mats) % 16) return QD_ERR_INVALID;
     htx.resize(ntx);
     hty.resize(nty);
     qd::dst_tiles(n_dots, h_prec, B, htx.data(), &ntx, hty.data(), &nty, &L.rows_x, &L.rows_y);
     L.mats = d_mats;
-    QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_x, htx.data(), ntx * sizeof(qd::GemmTile),
-                                cudaMemcpyHostToDevice, s));
-    QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_y, hty.data(), nty * sizeof(qd::GemmTile),
-                                cudaMemcpyHostToDevice, s));
-    QD_CUDA_TRY(cudaMemcpyAsync(L.desc, h_prec, n_dots * sizeof(qd_dst_prec),
-                                cudaMemcpyHostToDevice, s));
+    same_tiles = same_tiles && pod_equal(cache.tiles_x, htx) && pod_equal(cache.tiles_y, hty) &&
+                 cache.desc.size() == size_t(n_dots) &&
+                 std::memcmp(cache.desc.data(), h_prec, n_dots * sizeof(qd_dst_prec)) == 0;
+    if (!same_tiles) {
+      QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_x, htx.data(), ntx * sizeof(qd::GemmTile),
+                                  cudaMemcpyHostToDevice, s));
+      QD_CUDA_TRY(cudaMemcpyAsync(L.tiles_y, hty.data(), nty * sizeof(qd::GemmTile),
+                                  cudaMemcpyHostToDevice, s));
+      QD_CUDA_TRY(cudaMemcpyAsync(L.desc, h_prec, n_dots * sizeof(qd_dst_prec),
+                                  cudaMemcpyHostToDevice, s));
+    }
+  } else {
+    same_tiles = same_tiles && cache.tiles_x.empty() && cache.tiles_y.empty();
   }
   // chunk table and per-dot state
   std::vector<Chunk> chunks;
@@ -2873,8 +2964,13 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
       x.status = 2;
     }
   }
-  QD_CUDA_TRY(cudaMemcpyAsync(L.chunks, chunks.data(), chunks.size() * sizeof(Chunk),
-                              cudaMemcpyHostToDevice, s));
+  const bool same_chunks = cached && same_tiles && pod_equal(cache.chunks, chunks);
+  if (!same_chunks) {
+    QD_CUDA_TRY(cudaMemcpyAsync(L.chunks, chunks.data(), chunks.size() * sizeof(Chunk),
+                                cudaMemcpyHostToDevice, s));
+    QD_CUDA_TRY(cudaMemcpyAsync(L.row_off, h_row_off, sizeof(int32_t) * (n_dots + 1),
+                                cudaMemcpyHostToDevice, s));
+  }
   if (mixed_mode) {
     const int64_t nsubs = int64_t(nchunks) * L.spc, nsubw = int64_t(nchunks) * L.spcw;
     stage_plan_kernel<64><<<int((nsubs + 7) / 8), 256, 0, s>>>(L.chunks, nchunks, L.spc,
@@ -2888,14 +2984,38 @@ int solve_b(int32_t n_dots, const int32_t *h_row_off, const int32_t *d_rowptr,
     jacobi_diag_kernel<<<int(chunks.size()), 256, 0, s>>>(L.chunks, d_rowptr, d_col, d_H, L.dinv);
     QD_CHECK_LAUNCH();
   }
-  QD_CUDA_TRY(cudaMemcpyAsync(L.st, st.data(), st.size() * sizeof(DotState),
-                              cudaMemcpyHostToDevice, s));
-  QD_CUDA_TRY(cudaMemcpyAsync(L.row_off, h_row_off, sizeof(int32_t) * (n_dots + 1),
-                              cudaMemcpyHostToDevice, s));
-  QD_CUDA_TRY(cudaMemsetAsync(L.theta, 0, sizeof(double) * size_t(n_dots) * B, s));
-  QD_CUDA_TRY(cudaMemsetAsync(L.wait_err, 0, sizeof(int), s));
-  QD_CUDA_TRY(cudaMemsetAsync(L.relres, 0, sizeof(double) * size_t(n_dots) * B, s));
-  QD_CUDA_TRY(cudaStreamSynchronize(s));   // host staging vectors die at return
+  // the per-dot state: from the host, or (same chunk table as the previous
+  // call, whose state still holds each dot's chunk range) reset on the device;
+  // Theta, the residual norms and the wait flag zeroed by a kernel
+  if (!same_chunks)
+    QD_CUDA_TRY(cudaMemcpyAsync(L.st, st.data(), st.size() * sizeof(DotState),
+                                cudaMemcpyHostToDevice, s));
+  state_reset_kernel<<<(n_dots + 127) / 128, 128, 0, s>>>(
+      L.st, n_dots, same_chunks ? 1 : 0, prec_mode == QD_PREC_MIXED ? 0 : 1, B, L.theta,
+      L.relres, L.wait_err);
+  QD_CHECK_LAUNCH();
+  // the host tables of this call, for the next call with this workspace
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    SetupCache &c = setup_cache_for(d_work);
+    c.work = d_work;
+    c.work_bytes = work_bytes;
+    c.rowptr = d_rowptr;
+    c.col = d_col;
+    c.B = B;
+    c.prec = prec_mode;
+    c.chunk_rows = chunk_rows;
+    c.jacobi = jacobi ? 1 : 0;
+    c.ntx = ntx;
+    c.nty = nty;
+    c.nnz = nnz;
+    c.row_off.assign(h_row_off, h_row_off + n_dots + 1);
+    c.chunks = chunks;
+    c.tiles_x = htx;
+    c.tiles_y = hty;
+    c.desc.clear();
+    if (h_prec) c.desc.assign(h_prec, h_prec + n_dots);
+  }
 
   const bool mixed = prec_mode == QD_PREC_MIXED;
   RRParams prm;

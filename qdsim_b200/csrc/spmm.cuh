@@ -35,25 +35,12 @@ template <> struct V4<double> {
   }
 };
 
-// Values of the two matrices at a nonzero: separate FP64 arrays, or one
-// interleaved FP32 (H, M) pair per nonzero (8 bytes instead of 16; used while
-// the vectors themselves are stored in FP32).  The FP32 pairs are scaled by
-// powers of two so that the largest magnitudes sit near 1: problems posed in
-// SI units have entries far below FP32's normal range.
+// Values of the two matrices at a nonzero: the caller's FP64 arrays.
 struct MatF64 {
   const double *H, *M;
   __device__ void get(int p, double &h, double &m) const {
     h = __ldg(H + p);
     m = __ldg(M + p);
-  }
-};
-struct MatF32 {
-  const float2 *HM;   // (H 2^-eh, M 2^-em): scaled into FP32's range
-  double sh, sm;      // 2^eh, 2^em (exact rescaling)
-  __device__ void get(int p, double &h, double &m) const {
-    const float2 v = __ldg(HM + p);
-    h = double(v.x) * sh;
-    m = double(v.y) * sm;
   }
 };
 

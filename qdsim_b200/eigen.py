@@ -141,7 +141,7 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
                   allow_not_converged=True, precond: DSTPreconditioner | None = None,
                   tol32: float | None = None, stag_window: int | None = None,
                   graphs: bool = True, x0=None, eig_scale: float = 0.0,
-                  chunk_rows: int | None = None):
+                  chunk_rows: int | None = None, setup_cached: bool = False):
     """Solve a packed block-diagonal batch; returns (E, X_all, res, iters, info, status).
 
     ``tol32`` / ``stag_window`` tune the FP32 -> FP64 hand-over of the mixed
@@ -150,7 +150,10 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
     warm-starts the first k block vectors; ``eig_scale`` (eV) measures
     eigenvalue errors relative to max(|E|, eig_scale) (levels near zero);
     ``chunk_rows`` sets the rows per CTA of the row-parallel kernels (a
-    multiple of 64 in [256, 8192]; ``None``: 1024)."""
+    multiple of 64 in [256, 8192]; ``None``: 1024); ``setup_cached`` asserts
+    that the workspace and the CSR pattern are those of the previous call with
+    this workspace (repeated solves of one batch: no read-back and no copy of
+    unchanged tables during the set-up)."""
     n_dots = len(row_off) - 1
     n_rows = int(row_off[-1])
     if b is None:
@@ -167,7 +170,8 @@ def lobpcg_packed(row_off, rowptr, col, H, M, k, b=None, precision="mixed", tol=
             raise ValueError("x0 must hold n_rows x k values")
     opts[0] = (float(tol32) if tol32 else 0.0, int(stag_window) if stag_window else 0,
                1 if graphs else 0, int(x0.data_ptr()) if x0 is not None else 0,
-               float(eig_scale), int(chunk_rows) if chunk_rows else 0, 0)
+               float(eig_scale), int(chunk_rows) if chunk_rows else 0,
+               1 if setup_cached else 0)
     nbytes = workspace_bytes(n_dots, n_rows, col.numel(), b, prec, h_prec, opts)
     ws = (workspace or Workspace(dev)).get(nbytes)
     X = torch.empty(n_rows * k, dtype=torch.float64, device=dev)
